@@ -1,0 +1,428 @@
+#!/usr/bin/env python
+"""Throughput of the CloverLeaf hydro step on B200: cell-steps/s and the
+fraction of the HBM roofline, FP64 plain form and FP32 form in the same run.
+
+Workload: the reference benchmark problem (InputDecks/clover_bm*.in physics:
+background rho=0.2 e=1.0, rectangle [0,5]x[0,2] rho=1.0 e=2.5 on [0,10]^2,
+gamma 1.4, reflective) on a 7680x7680 mesh.  One "step" is one hydro
+timestep of the reference driver (timestep, PdV predictor, accelerate, PdV
+corrector, flux_calc, advection, reset_field, and field_summary every 10
+steps), enqueued through the C ABI in the driver's call order, with the
+driver's per-step dt read-back.  Every field array is 472 MB, far above the
+126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun: the path does not shard (one mesh per GPU, no
+decomposition, as in the north star), so each rank advances its own replica
+and value is the sum over ranks (weak scaling).  --impl reference times the
+reference's own OpenMP build (oracle/_ref/omp) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "cell-steps/s and % HBM roofline: FP64 plain vs FP32 form at stated error"
+UNIT = "cell-steps/s"
+# Array touches per cell of each driver-level phase (the algorithmic byte count:
+# one read of each distinct full-grid input, one write of each output).
+PHASE_ARRAYS = {"ideal_gas": 4, "viscosity": 5, "calc_dt": 8, "pdv_predict": 11 + 4 + 4, "accelerate": 10,
+                "pdv_correct": 13, "flux_calc": 8, "advec_cell_s1": 8, "advec_mom_s1": 8, "advec_cell_s2": 7,
+                "advec_mom_s2": 7, "reset_field": 8, "field_summary": 10}
+STEP_ARRAYS = 105  # the step's phases, ideal_gas .. reset_field
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if self.p is None or not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            w = [x.strip() for x in line.split(",")]
+            if len(w) < 9:
+                continue
+            try:
+                sm.append(float(w[1]))
+                mx = float(w[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, w[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def bench_deck(cells, gamma=1.4):
+    from cloverleaf_b200 import benchmark_deck, nudged
+    d = benchmark_deck(cells, end_step=10 ** 9, end_time=1.0e30)
+    d.gamma = gamma
+    return nudged(d)
+
+
+class PhaseTimer:
+    """CUDA events on the chunk's own stream at every phase boundary."""
+
+    def __init__(self, chunk):
+        import torch
+        self.torch = torch
+        self.stream = torch.cuda.ExternalStream(chunk.stream())
+        self.marks = []
+
+    def __call__(self, name):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        self.marks.append((name, e))
+
+    def totals(self):
+        tot, cnt = {}, {}
+        for (n, a), (_, b) in zip(self.marks, self.marks[1:]):
+            if n == "end":
+                continue
+            tot[n] = tot.get(n, 0.0) + a.elapsed_time(b)
+            cnt[n] = cnt.get(n, 0) + 1
+        return tot, cnt
+
+
+def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1):
+    """Sets up a chunk, runs warmup steps, then times `steps` steps; returns
+    (ms, run, chunk, phase totals, launches in the timed region)."""
+    import torch
+    from cloverleaf_b200 import Chunk, HydroRun
+    dk = bench_deck(cells)
+    dev = torch.cuda.current_device()
+    c = Chunk(cells, cells, precision=precision, device=dev)
+    run = HydroRun(c, dk, forced_dt=forced_dt)
+    run.start()
+    for _ in range(warmup):
+        run.hydro_step()
+    ext = torch.cuda.ExternalStream(c.stream())
+    timer = PhaseTimer(c) if with_phases else None
+    run.probe = timer
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    n0 = c.launch_count()
+    t0.record(ext)
+    for _ in range(steps):
+        run.hydro_step()
+    t1.record(ext)
+    c.synchronize()
+    torch.cuda.synchronize()
+    n1 = c.launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    run.probe = None
+    ms = t0.elapsed_time(t1)
+    phases = timer.totals() if timer else None
+    return ms, run, c, phases, n1 - n0
+
+
+def rel_errors(a64, a32):
+    import numpy as np
+    d = np.abs(a32 - a64)
+    den = np.abs(a64)
+    floor = 1e-12 * den.max() if den.max() > 0 else 1e-300
+    return float(d.sum() / den.sum()) if den.sum() > 0 else float(d.sum()), float((d / np.maximum(den, floor)).max())
+
+
+def e2e_run(cells, warmup, steps):
+    """The same metric through the public C ABI with host buffers: the timed
+    region uploads the step-0 state (density0, energy0, xvel0, yvel0) from
+    pinned host memory, advances `steps` steps (dt read back every step, the
+    summaries every 10) and reads the final state back to pinned host memory."""
+    import numpy as np
+    import torch
+    from cloverleaf_b200 import Chunk, HydroRun
+    dk = bench_deck(cells)
+    c = Chunk(cells, cells, device=torch.cuda.current_device())
+    run = HydroRun(c, dk)
+    run.start()
+    names = ["density0", "energy0", "xvel0", "yvel0"]
+    host = {n: torch.empty(tuple(reversed(c.extent(n))), dtype=torch.float64, pin_memory=True).numpy() for n in names}
+    for n in names:
+        host[n][...] = c.read(n)
+    for _ in range(warmup):
+        run.hydro_step()
+    run2 = HydroRun(c, dk)
+    run2.summaries = []
+    ext = torch.cuda.ExternalStream(c.stream())
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c.synchronize()
+    torch.cuda.synchronize()
+    t0.record(ext)
+    for n in names:
+        c.write(n, host[n])
+    for _ in range(steps):
+        run2.hydro_step()
+    for n in names:
+        host[n][...] = c.read(n)
+    t1.record(ext)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    h2d = sum(host[n].nbytes for n in names)
+    d2h = sum(host[n].nbytes for n in names) + 8 * steps + 40 * len(run2.summaries)
+    c.close()
+    return ms, h2d, d2h
+
+
+def traffic_per_launch(kernel, cells):
+    """DRAM bytes per launch from the committed ncu summary, scaled to `cells`."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        e = t[kernel]
+        return e["dram_bytes_per_cell"] * cells * cells
+    except Exception:
+        return None
+
+
+def reference_exe():
+    return os.path.join(ROOT, "oracle", "_ref", "omp")
+
+
+def run_reference_omp(cells, steps, threads, timeout=900):
+    """Runs the reference OpenMP build on the benchmark deck for `steps` steps;
+    returns the per-step "Step time per cell" values the driver prints
+    (driver/hydro.cpp:209-220)."""
+    from cloverleaf_b200 import benchmark_deck, format_deck
+    exe = reference_exe()
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = os.path.join(tmp, "clover.in")
+        with open(deck, "w") as f:
+            f.write(format_deck(benchmark_deck(cells, end_step=steps, end_time=1.0e30)))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="true", OMP_PLACES="cores")
+        p = subprocess.run([exe, "--file", deck, "--out", os.path.join(tmp, "clover.out")], cwd=tmp, env=env,
+                           capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"reference OpenMP build exited {p.returncode}: {p.stdout[-500:]}")
+        return [float(x) for x in re.findall(r"Step time per cell\s+([0-9.eE+-]+)", p.stdout)]
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(cells):
+    """The reference OpenMP build on all host cores, bounded: 3 steps of the
+    same deck (the first step is dropped).  Falls back to the C oracle port
+    (one core, a 960^2 sample) if the reference build is absent."""
+    cores = cpu_cores()
+    if os.path.exists(reference_exe()):
+        per_cell = run_reference_omp(cells, 3, cores)
+        v = 1.0 / statistics.mean(per_cell[1:])
+        return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"reference OpenMP build (oracle/_ref/omp, g++ -O3), {cells}x{cells} benchmark deck, "
+                          f"steps 2-3 of a 3-step run, OMP_NUM_THREADS={cores}"}
+    import oracle
+    from cloverleaf_b200 import benchmark_deck, nudged
+    dk = nudged(benchmark_deck(960, end_step=3))
+    o = oracle.OracleChunk(960, 960)
+    t = time.time()
+    o.run(dk)
+    dt = time.time() - t
+    return {"value": 960 * 960 * 3 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "C oracle port, one core, 960x960 benchmark deck, 3 steps incl. setup"}
+
+
+def main_reference(args, rank, world):
+    if rank != 0:
+        return
+    cores = cpu_cores()
+    if not os.path.exists(reference_exe()):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/omp was not built (needs the reference sources)"}))
+        return
+    steps = min(args.steps, 50)
+    warm = max(1, min(args.warmup, 3))
+    per_cell = run_reference_omp(args.size, warm + steps, cores)
+    timed = per_cell[warm:warm + steps]
+    v = 1.0 / statistics.mean(timed)
+    ms = statistics.mean(timed) * args.size * args.size * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": len(timed),
+            "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic: the reference benchmark deck generated in-process",
+            "config": {"workload": f"clover_bm FP64 {args.size}x{args.size}, hydro steps", "cells": args.size * args.size,
+                       "l2": "inputs larger than L2 (host run)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"reference OpenMP build, {args.size}^2, steps {warm + 1}-{warm + len(timed)} of "
+                                       f"{warm + steps}, OMP_NUM_THREADS={cores}"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=7680)
+    ap.add_argument("--large", type=int, default=15360, help="second FP64 size timed (0 to skip)")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return main_reference(args, rank, world)
+    if args.warmup < 3:
+        raise SystemExit("bench.py: --warmup must be at least 3")
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    from cloverleaf_b200 import FP32, FP64
+
+    S = args.size
+    peak, peak_kind = peaks()
+    with ClockSampler(local) as clk:
+        ms64, run64, c64, phases, launches = run_form(FP64, S, args.warmup, args.steps, with_phases=True, rank=rank,
+                                                      world=world)
+    clocks = clk.summary()
+    if world > 1:
+        t = torch.tensor([ms64], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms64 = float(t.item())
+    value = S * S * args.steps * world / (ms64 / 1e3)
+
+    # FP32 form, replaying the FP64 run's dt sequence, errors against FP64 at the same time
+    dts = list(run64.dt_trace)
+    ms32, run32, c32, _, _ = run_form(FP32, S, args.warmup, args.steps, forced_dt=dts, world=world)
+    if world > 1:
+        t = torch.tensor([ms32], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms32 = float(t.item())
+    value32 = S * S * args.steps * world / (ms32 / 1e3)
+    errs = {}
+    for name in ("density0", "energy0", "pressure", "xvel0", "yvel0"):
+        a64 = c64.read(name)[2:-2, 2:-2]
+        a32 = c32.read(name)[2:-2, 2:-2]
+        l1, mx = rel_errors(a64, a32)
+        errs[name] = {"l1_rel": l1, "max_rel": mx}
+
+    def drift(run):
+        s0, s1 = run.summaries[0], run.summaries[-1]
+        return {"mass": (s1.mass - s0.mass) / s0.mass,
+                "total_energy": ((s1.ie + s1.ke) - (s0.ie + s0.ke)) / (s0.ie + s0.ke)}
+
+    fp32 = {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
+            "errors_vs_fp64": errs, "drift_fp64": drift(run64), "drift_fp32": drift(run32),
+            "dt_sequence": "the FP64 run's, replayed"}
+    c64.close()
+    c32.close()
+
+    large = None
+    if args.large:
+        try:
+            msl, _, cl, _, _ = run_form(FP64, args.large, 3, 20, world=world)
+            cl.close()
+            large = {"cells": f"{args.large}x{args.large}", "steps": 20, "value": args.large ** 2 * 20 * world / (msl / 1e3),
+                     "unit": UNIT}
+        except Exception as e:  # memory or other failure is reported, not hidden
+            large = {"error": str(e)}
+
+    ms_e2e, h2d, d2h = e2e_run(S, args.warmup, args.steps)
+    e2e = {"value": S * S * args.steps * world / (ms_e2e / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
+
+    # roofline of the dominant kernel (largest total time over the timed steps)
+    tot, cnt = phases
+    kern = {k: v for k, v in tot.items() if k in PHASE_ARRAYS and k != "calc_dt"}
+    dom = max(kern, key=kern.get)
+    avg_ms = tot[dom] / cnt[dom]
+    alg = PHASE_ARRAYS[dom] * 8 * S * S
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    traffic = traffic_per_launch(dom, S)
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6.65 TB/s", "traffic": traffic, "alg_bytes_per_launch": alg,
+            "step_frac": value / world * STEP_ARRAYS * 8 / 1e9 / peak,
+            "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(S)
+        except Exception as e:
+            cpu = {"error": str(e)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic: the reference benchmark deck generated in-process",
+                "config": {"workload": f"clover_bm FP64 {S}x{S} hydro steps (InputDecks/clover_bm64_300.in physics)",
+                           "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "halo": "folded into producers"},
+                "roofline": roof, "fp32": fp32, "large": large, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

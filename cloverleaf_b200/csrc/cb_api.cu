@@ -1,0 +1,620 @@
+// cb_api.cu -- the C ABI of libcloverb200 (declared in include/cloverb200.h).
+//
+// Host-side orchestration only: argument checks, allocation, the halo
+// freshness bookkeeping that turns update_halo into a no-op after a folded
+// producer, buffer swaps of the double-buffered phases, and the dispatch to
+// the FP64 / FP32 kernel instantiations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cloverb200.h"
+#include "cb_chunk.h"
+#include "cb_phase.cuh"
+
+namespace cb {
+template <typename T> struct Ops;
+}
+#include "cb_ops.cuh"
+
+extern template struct cb::Ops<double>;
+extern template struct cb::Ops<float>;
+
+struct cb_chunk : cb::Chunk {};
+
+using namespace cb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+  return fail(CB_ECUDA, std::string(where) + ": " + cudaGetErrorName(e) + ": " + cudaGetErrorString(e));
+}
+
+#define CB_CHECK_CHUNK(c)                                                                                                                    \
+  do {                                                                                                                                       \
+    if (!(c)) return fail(CB_EINVAL, std::string(__func__) + ": null chunk");                                                               \
+    cudaError_t _e = select_device(c);                                                                                                       \
+    if (_e != cudaSuccess) return cuda_fail(_e, __func__);                                                                                   \
+  } while (0)
+
+#define CB_CUDA(expr)                                                                                                                        \
+  do {                                                                                                                                       \
+    cudaError_t _e = (expr);                                                                                                                 \
+    if (_e != cudaSuccess) return cuda_fail(_e, __func__);                                                                                   \
+  } while (0)
+
+cudaError_t select_device(const cb_chunk *c) {
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return e;
+  if (cur != c->device) return cudaSetDevice(c->device);
+  return cudaSuccess;
+}
+
+// Dispatch to the instantiation of the chunk's precision.
+template <typename F> cudaError_t dispatch(cb_chunk *c, F &&f) {
+  if (c->precision == CB_FP64) return f(Ops<double>());
+  return f(Ops<float>());
+}
+
+void field_extent(const cb_chunk *c, int f, int &sx, int &sy) {
+  switch (kind_of(f)) {
+    case VERTEX: sx = c->nx + 5; sy = c->ny + 5; break;
+    case XFACE: sx = c->nx + 5; sy = c->ny + 4; break;
+    case YFACE: sx = c->nx + 4; sy = c->ny + 5; break;
+    default: sx = c->nx + 4; sy = c->ny + 4; break;
+  }
+}
+
+int geom_len(const cb_chunk *c, int g) {
+  switch (g) {
+    case CELLX: case CELLDX: return c->nx + 4;
+    case CELLY: case CELLDY: return c->ny + 4;
+    case VERTEXX: case VERTEXDX: return c->nx + 5;
+    default: return c->ny + 5;
+  }
+}
+
+bool is_state_field(int f) { return f >= 0 && f < 15; }
+
+int effective_fold(const cb_chunk *c, int depth) { return c->can_fold() ? depth : 0; }
+
+int check_depth(int d, bool allow0) {
+  if (d == 1 || d == 2 || (allow0 && d == 0)) return CB_OK;
+  return fail(CB_EINVAL, "halo depth must be " + std::string(allow0 ? "0, 1 or 2" : "1 or 2") + ", got " + std::to_string(d));
+}
+
+cudaError_t upload_geom(cb_chunk *c) {
+  for (int g = 0; g < NUM_GEOM; ++g) {
+    cudaError_t e = cudaMemcpyAsync(c->geom_d[g], c->geom_h[g], sizeof(double) * c->geom_len, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+    if (c->precision == CB_FP32) {
+      std::vector<float> tmp(c->geom_len);
+      for (int k = 0; k < c->geom_len; ++k) tmp[k] = (float)c->geom_h[g][k];
+      e = cudaMemcpyAsync(c->geom_t[g], tmp.data(), sizeof(float) * c->geom_len, cudaMemcpyHostToDevice, c->stream);
+      if (e != cudaSuccess) return e;
+      e = cudaStreamSynchronize(c->stream); // tmp dies here
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+void release(cb_chunk *c) {
+  for (auto &p : c->field_mem)
+    if (p) cudaFree(p), p = nullptr;
+  for (auto &p : c->spare_mem)
+    if (p) cudaFree(p), p = nullptr;
+  for (int g = 0; g < NUM_GEOM; ++g) {
+    if (c->geom_d[g]) cudaFree(c->geom_d[g]);
+    if (c->precision == CB_FP32 && c->geom_t[g]) cudaFree(c->geom_t[g]);
+    delete[] c->geom_h[g];
+    c->geom_d[g] = nullptr;
+    c->geom_t[g] = nullptr;
+    c->geom_h[g] = nullptr;
+  }
+  if (c->d_dt_bits) cudaFree(c->d_dt_bits);
+  if (c->d_partials) cudaFree(c->d_partials);
+  if (c->d_counter) cudaFree(c->d_counter);
+  if (c->d_sums) cudaFree(c->d_sums);
+  if (c->h_scalars) cudaFreeHost(c->h_scalars);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->d_dt_bits = nullptr;
+  c->d_partials = nullptr;
+  c->d_counter = nullptr;
+  c->d_sums = nullptr;
+  c->h_scalars = nullptr;
+  c->stream = nullptr;
+}
+
+} // namespace
+
+extern "C" {
+
+int cb_version(void) { return 1; }
+
+const char *cb_last_error(void) { return g_err.c_str(); }
+
+int cb_device_count(int *count) {
+  if (!count) return fail(CB_EINVAL, "cb_device_count: null count");
+  *count = 0;
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return cuda_fail(e, "cb_device_count");
+  }
+  return CB_OK;
+}
+
+int cb_device_name(int device, char *name, size_t len) {
+  if (!name || len == 0) return fail(CB_EINVAL, "cb_device_name: null buffer");
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return cuda_fail(e, "cb_device_name");
+  std::snprintf(name, len, "%s (sm_%d%d, %d SMs, %.1f GB)", prop.name, prop.major, prop.minor, prop.multiProcessorCount,
+                prop.totalGlobalMem / 1e9);
+  return CB_OK;
+}
+
+int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
+  if (!out) return fail(CB_EINVAL, "cb_create: null out");
+  *out = nullptr;
+  if (nx < 1 || ny < 1) return fail(CB_EINVAL, "cb_create: mesh must have at least one cell in each direction");
+  if (nx > (1 << 20) || ny > (1 << 20)) return fail(CB_EINVAL, "cb_create: mesh side above 1048576 cells");
+  if (precision != CB_FP64 && precision != CB_FP32) return fail(CB_EINVAL, "cb_create: precision must be CB_FP64 or CB_FP32");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_fail(e, "cb_create");
+  if (device < 0 || device >= ndev) return fail(CB_EINVAL, "cb_create: no CUDA device " + std::to_string(device));
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_fail(e, "cb_create");
+  cb_chunk *c = new (std::nothrow) cb_chunk();
+  if (!c) return fail(CB_ENOMEM, "cb_create: out of host memory");
+  c->nx = nx;
+  c->ny = ny;
+  c->precision = precision;
+  c->device = device;
+  c->esize = precision == CB_FP64 ? 8 : 4;
+  const long long align = 256 / (long long)c->esize;
+  c->off = (size_t)(align - 2);
+  c->pitch = ((long long)nx + 5 + align - 1) / align * align;
+  c->alloc_elems = c->off + (size_t)c->pitch * (size_t)(ny + 5) + (size_t)align;
+  const size_t bytes = c->alloc_elems * c->esize;
+  auto bail = [&](cudaError_t err, const char *what) {
+    release(c);
+    delete c;
+    if (err == cudaErrorMemoryAllocation) return fail(CB_ENOMEM, std::string("cb_create: out of device memory allocating ") + what);
+    return cuda_fail(err, "cb_create");
+  };
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+  for (int f = 0; f < 15; ++f)
+    if ((e = cudaMalloc(&c->field_mem[f], bytes)) != cudaSuccess) return bail(e, "fields");
+  for (int s = 0; s < NUM_SPARE; ++s)
+    if ((e = cudaMalloc(&c->spare_mem[s], bytes)) != cudaSuccess) return bail(e, "spare buffers");
+  c->geom_len = std::max(nx, ny) + 6;
+  for (int g = 0; g < NUM_GEOM; ++g) {
+    c->geom_h[g] = new (std::nothrow) double[c->geom_len]();
+    if (!c->geom_h[g]) return bail(cudaErrorMemoryAllocation, "geometry");
+    if ((e = cudaMalloc(&c->geom_d[g], sizeof(double) * c->geom_len)) != cudaSuccess) return bail(e, "geometry");
+    if (precision == CB_FP32) {
+      if ((e = cudaMalloc(&c->geom_t[g], sizeof(float) * c->geom_len)) != cudaSuccess) return bail(e, "geometry");
+    } else {
+      c->geom_t[g] = c->geom_d[g];
+    }
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  c->summary_grid = sms * 8;
+  if ((e = cudaMalloc(&c->d_dt_bits, sizeof(unsigned long long))) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMalloc(&c->d_partials, sizeof(double) * 5 * (size_t)c->summary_grid)) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMalloc(&c->d_counter, sizeof(unsigned int))) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMalloc(&c->d_sums, sizeof(double) * 5)) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMallocHost(&c->h_scalars, sizeof(double) * 8)) != cudaSuccess) return bail(e, "pinned scratch");
+  if ((e = cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), c->stream)) != cudaSuccess) return bail(e, "scratch");
+  for (int f = 0; f < 15; ++f)
+    if ((e = cudaMemsetAsync(c->field_mem[f], 0, bytes, c->stream)) != cudaSuccess) return bail(e, "fields");
+  for (int s = 0; s < NUM_SPARE; ++s)
+    if ((e = cudaMemsetAsync(c->spare_mem[s], 0, bytes, c->stream)) != cudaSuccess) return bail(e, "spare buffers");
+  if ((e = upload_geom(c)) != cudaSuccess) return bail(e, "geometry");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "setup");
+  *out = c;
+  return CB_OK;
+}
+
+int cb_destroy(cb_chunk *c) {
+  if (!c) return CB_OK;
+  select_device(c);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  release(c);
+  delete c;
+  return CB_OK;
+}
+
+int cb_set_gamma(cb_chunk *c, double gamma) {
+  CB_CHECK_CHUNK(c);
+  if (!(gamma > 1.0) || !std::isfinite(gamma)) return fail(CB_EINVAL, "cb_set_gamma: gamma must be a finite value above 1");
+  c->gamma = gamma;
+  return CB_OK;
+}
+
+int cb_set_option(cb_chunk *c, int option, int value) {
+  CB_CHECK_CHUNK(c);
+  if (option == CB_OPT_FOLD_HALO) {
+    c->fold_enabled = value != 0;
+    std::fill(std::begin(c->halo_fresh), std::end(c->halo_fresh), 0);
+  } else if (option == CB_OPT_RESET_BY_SWAP) {
+    c->reset_by_swap = value != 0;
+  } else {
+    return fail(CB_EINVAL, "cb_set_option: unknown option " + std::to_string(option));
+  }
+  return CB_OK;
+}
+
+int cb_get_extent(const cb_chunk *c, int field, int *sx, int *sy) {
+  if (!c || !sx || !sy) return fail(CB_EINVAL, "cb_get_extent: null argument");
+  if (field < 0 || field >= NUM_FIELDS) return fail(CB_EINVAL, "cb_get_extent: bad field id " + std::to_string(field));
+  field_extent(c, field, *sx, *sy);
+  return CB_OK;
+}
+
+int cb_read_field(cb_chunk *c, int field, double *host, size_t n, int layout) {
+  CB_CHECK_CHUNK(c);
+  if (!host) return fail(CB_EINVAL, "cb_read_field: null host buffer");
+  if (field < 0 || field >= NUM_FIELDS) return fail(CB_EINVAL, "cb_read_field: bad field id " + std::to_string(field));
+  if (layout != CB_LAYOUT_XFAST && layout != CB_LAYOUT_YFAST) return fail(CB_EINVAL, "cb_read_field: bad layout");
+  int sx, sy;
+  field_extent(c, field, sx, sy);
+  if (n != (size_t)sx * (size_t)sy)
+    return fail(CB_EINVAL, "cb_read_field: buffer holds " + std::to_string(n) + " values, field has " + std::to_string((size_t)sx * sy));
+  if (c->precision == CB_FP64 && layout == CB_LAYOUT_XFAST && is_state_field(field)) {
+    // straight pitched copy into the caller's buffer (fast when it is pinned)
+    CB_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * sx, c->base(field), sizeof(double) * c->pitch, sizeof(double) * sx, sy,
+                              cudaMemcpyDeviceToHost, c->stream));
+    CB_CUDA(cudaStreamSynchronize(c->stream));
+    return CB_OK;
+  }
+  std::vector<double> xf((size_t)sx * sy);
+  if (field >= WORK1 && field <= WORK7) {
+    // work arrays are intra-phase scratch the kernels keep on chip
+    std::fill(xf.begin(), xf.end(), 0.0);
+  } else if (field == VOLUME || field == XAREA || field == YAREA) {
+    // derived from the 1-D widths exactly as src/serial/initialise_chunk.cpp:78-84 forms them
+    const double dx = c->geom_h[CELLDX][0], dy = c->geom_h[CELLDY][0];
+    for (int j = 0; j < sy; ++j)
+      for (int i = 0; i < sx; ++i) {
+        double v = 0.0;
+        const bool in_cells = i < c->nx + 4 && j < c->ny + 4;
+        if (field == VOLUME) v = in_cells ? dx * dy : 0.0;
+        else if (field == XAREA) v = in_cells ? c->geom_h[CELLDY][j] : 0.0;
+        else v = in_cells ? c->geom_h[CELLDX][i] : 0.0;
+        xf[(size_t)j * sx + i] = v;
+      }
+  } else {
+    CB_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->precision == CB_FP64) {
+      CB_CUDA(cudaMemcpy2D(xf.data(), sizeof(double) * sx, c->base(field), sizeof(double) * c->pitch, sizeof(double) * sx, sy,
+                           cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> tmp((size_t)sx * sy);
+      CB_CUDA(cudaMemcpy2D(tmp.data(), sizeof(float) * sx, c->base(field), sizeof(float) * c->pitch, sizeof(float) * sx, sy,
+                           cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < tmp.size(); ++k) xf[k] = tmp[k];
+    }
+  }
+  if (layout == CB_LAYOUT_XFAST) {
+    std::memcpy(host, xf.data(), sizeof(double) * xf.size());
+  } else {
+    for (int i = 0; i < sx; ++i)
+      for (int j = 0; j < sy; ++j) host[(size_t)i * sy + j] = xf[(size_t)j * sx + i];
+  }
+  return CB_OK;
+}
+
+int cb_write_field(cb_chunk *c, int field, const double *host, size_t n, int layout) {
+  CB_CHECK_CHUNK(c);
+  if (!host) return fail(CB_EINVAL, "cb_write_field: null host buffer");
+  if (!is_state_field(field))
+    return fail(CB_EINVAL, "cb_write_field: field " + std::to_string(field) +
+                               " is derived (geometry comes from the 1-D widths, work arrays are on-chip scratch)");
+  if (layout != CB_LAYOUT_XFAST && layout != CB_LAYOUT_YFAST) return fail(CB_EINVAL, "cb_write_field: bad layout");
+  int sx, sy;
+  field_extent(c, field, sx, sy);
+  if (n != (size_t)sx * (size_t)sy)
+    return fail(CB_EINVAL, "cb_write_field: buffer holds " + std::to_string(n) + " values, field has " + std::to_string((size_t)sx * sy));
+  if (c->precision == CB_FP64 && layout == CB_LAYOUT_XFAST) {
+    CB_CUDA(cudaMemcpy2DAsync(c->base(field), sizeof(double) * c->pitch, host, sizeof(double) * sx, sizeof(double) * sx, sy,
+                              cudaMemcpyHostToDevice, c->stream));
+    CB_CUDA(cudaStreamSynchronize(c->stream));
+    c->halo_fresh[field] = 0;
+    return CB_OK;
+  }
+  std::vector<double> xf((size_t)sx * sy);
+  if (layout == CB_LAYOUT_XFAST) {
+    std::memcpy(xf.data(), host, sizeof(double) * xf.size());
+  } else {
+    for (int i = 0; i < sx; ++i)
+      for (int j = 0; j < sy; ++j) xf[(size_t)j * sx + i] = host[(size_t)i * sy + j];
+  }
+  CB_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->precision == CB_FP64) {
+    CB_CUDA(cudaMemcpy2D(c->base(field), sizeof(double) * c->pitch, xf.data(), sizeof(double) * sx, sizeof(double) * sx, sy,
+                         cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> tmp(xf.size());
+    for (size_t k = 0; k < tmp.size(); ++k) tmp[k] = (float)xf[k];
+    CB_CUDA(cudaMemcpy2D(c->base(field), sizeof(float) * c->pitch, tmp.data(), sizeof(float) * sx, sizeof(float) * sx, sy,
+                         cudaMemcpyHostToDevice));
+  }
+  c->halo_fresh[field] = 0;
+  return CB_OK;
+}
+
+int cb_read_geom(cb_chunk *c, int geom, double *host, size_t n) {
+  CB_CHECK_CHUNK(c);
+  if (!host) return fail(CB_EINVAL, "cb_read_geom: null host buffer");
+  if (geom < 0 || geom >= NUM_GEOM) return fail(CB_EINVAL, "cb_read_geom: bad geometry id");
+  if (n != (size_t)geom_len(c, geom)) return fail(CB_EINVAL, "cb_read_geom: length mismatch");
+  std::memcpy(host, c->geom_h[geom], sizeof(double) * n);
+  return CB_OK;
+}
+
+int cb_write_geom(cb_chunk *c, int geom, const double *host, size_t n) {
+  CB_CHECK_CHUNK(c);
+  if (!host) return fail(CB_EINVAL, "cb_write_geom: null host buffer");
+  if (geom < 0 || geom >= NUM_GEOM) return fail(CB_EINVAL, "cb_write_geom: bad geometry id");
+  if (n != (size_t)geom_len(c, geom)) return fail(CB_EINVAL, "cb_write_geom: length mismatch");
+  std::memcpy(c->geom_h[geom], host, sizeof(double) * n);
+  CB_CUDA(upload_geom(c));
+  return CB_OK;
+}
+
+// src/serial/build_field.cpp:29-180: every array to zero.
+int cb_build_field(cb_chunk *c) {
+  CB_CHECK_CHUNK(c);
+  const size_t bytes = c->alloc_elems * c->esize;
+  for (int f = 0; f < 15; ++f) CB_CUDA(cudaMemsetAsync(c->field_mem[f], 0, bytes, c->stream));
+  for (int s = 0; s < NUM_SPARE; ++s) CB_CUDA(cudaMemsetAsync(c->spare_mem[s], 0, bytes, c->stream));
+  for (int g = 0; g < NUM_GEOM; ++g) std::fill(c->geom_h[g], c->geom_h[g] + c->geom_len, 0.0);
+  CB_CUDA(upload_geom(c));
+  std::fill(std::begin(c->halo_fresh), std::end(c->halo_fresh), 0);
+  return CB_OK;
+}
+
+// src/serial/initialise_chunk.cpp:30-85 (single tile: t_left = t_bottom = 1).
+int cb_initialise_chunk(cb_chunk *c, double gxmin, double gymin, double gxmax, double gymax) {
+  CB_CHECK_CHUNK(c);
+  if (!(gxmax > gxmin) || !(gymax > gymin)) return fail(CB_EINVAL, "cb_initialise_chunk: empty domain");
+  const int x_min = 1, y_min = 1, x_max = c->nx, y_max = c->ny;
+  double dx = (gxmax - gxmin) / (double)(c->nx);
+  double dy = (gymax - gymin) / (double)(c->ny);
+  double xmin = gxmin + dx * (double)(1 - 1);
+  double ymin = gymin + dy * (double)(1 - 1);
+  double **g = c->geom_h;
+  const int xrange = (x_max + 3) - (x_min - 2) + 1, yrange = (y_max + 3) - (y_min - 2) + 1;
+  for (int j = 0; j < xrange; j++) {
+    g[VERTEXX][j] = xmin + dx * (j - 1 - x_min);
+    g[VERTEXDX][j] = dx;
+  }
+  for (int k = 0; k < yrange; k++) {
+    g[VERTEXY][k] = ymin + dy * (k - 1 - y_min);
+    g[VERTEXDY][k] = dy;
+  }
+  const int xrange1 = (x_max + 2) - (x_min - 2) + 1, yrange1 = (y_max + 2) - (y_min - 2) + 1;
+  for (int j = 0; j < xrange1; j++) {
+    g[CELLX][j] = 0.5 * (g[VERTEXX][j] + g[VERTEXX][j + 1]);
+    g[CELLDX][j] = dx;
+  }
+  for (int k = 0; k < yrange1; k++) {
+    g[CELLY][k] = 0.5 * (g[VERTEXY][k] + g[VERTEXY][k + 1]);
+    g[CELLDY][k] = dy;
+  }
+  CB_CUDA(upload_geom(c));
+  return CB_OK;
+}
+
+int cb_generate_chunk(cb_chunk *c, int nstates, const cb_state *states) {
+  CB_CHECK_CHUNK(c);
+  if (nstates < 1 || !states) return fail(CB_EINVAL, "cb_generate_chunk: need at least the background state");
+  static_assert(sizeof(cb_state) == sizeof(DevState), "cb_state layout");
+  DevState *d = nullptr;
+  CB_CUDA(cudaMalloc(&d, sizeof(DevState) * nstates));
+  cudaError_t e = cudaMemcpyAsync(d, states, sizeof(DevState) * nstates, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = dispatch(c, [&](auto ops) { return ops.generate_chunk(*c, d, nstates); });
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "cb_generate_chunk");
+  c->halo_fresh[DENSITY0] = c->halo_fresh[ENERGY0] = c->halo_fresh[XVEL0] = c->halo_fresh[YVEL0] = 0;
+  return CB_OK;
+}
+
+int cb_ideal_gas(cb_chunk *c, int predict, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.ideal_gas(*c, predict ? 1 : 0, fold); }));
+  c->halo_fresh[PRESSURE] = fold;
+  c->halo_fresh[SOUNDSPEED] = 0;
+  return CB_OK;
+}
+
+int cb_viscosity(cb_chunk *c, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.viscosity(*c, fold); }));
+  c->halo_fresh[VISCOSITY] = fold;
+  return CB_OK;
+}
+
+int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *control, int *jldt, int *kldt, int *small) {
+  CB_CHECK_CHUNK(c);
+  if (!p || !dt_min_val) return fail(CB_EINVAL, "cb_calc_dt: null argument");
+  DtConsts k{p->dtc_safe, p->dtu_safe, p->dtv_safe, p->dtdiv_safe};
+  c->h_scalars[0] = g_big;
+  CB_CUDA(cudaMemcpyAsync(c->d_dt_bits, &c->h_scalars[0], sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.calc_dt(*c, k); }));
+  CB_CUDA(cudaMemcpyAsync(&c->h_scalars[1], c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CB_CUDA(cudaStreamSynchronize(c->stream));
+  const double dt = c->h_scalars[1];
+  *dt_min_val = dt;
+  // src/serial/calc_dt.cpp:73-79: control is always "sound" (jk_control = 1.1)
+  double jk_control = 1.1;
+  const int l_control = (int)(10.01 * (jk_control - (int)(jk_control)));
+  jk_control = jk_control - (jk_control - (int)(jk_control));
+  if (control) *control = l_control;
+  if (jldt) *jldt = ((int)jk_control) % c->nx;
+  if (kldt) *kldt = (int)(1.f + (jk_control / c->nx));
+  if (small) *small = dt < p->dtmin ? 1 : 0;
+  return CB_OK;
+}
+
+int cb_pdv(cb_chunk *c, int predict, double dt, int full, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  if (full && !predict) return fail(CB_EINVAL, "cb_pdv: full = 1 is the predictor step; use predict = 1");
+  const int fold = effective_fold(c, halo_depth);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.pdv(*c, predict ? 1 : 0, dt, full ? 1 : 0, fold); }));
+  if (full && halo_depth > 0 && fold == 0) {
+    // the predictor's own update_halo(pressure) (src/serial/PdV.cpp:118-124) on a mesh too small to fold
+    HaloJob job{};
+    job.nfields = 1;
+    job.field[0] = PRESSURE;
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.update_halo(*c, job, halo_depth); }));
+  }
+  if (full) {
+    c->halo_fresh[PRESSURE] = fold;
+    c->halo_fresh[SOUNDSPEED] = 0;
+    c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = 0;
+  } else {
+    c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = fold;
+  }
+  return CB_OK;
+}
+
+int cb_revert(cb_chunk *c) {
+  CB_CHECK_CHUNK(c);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.revert(*c); }));
+  c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = 0;
+  return CB_OK;
+}
+
+int cb_accelerate(cb_chunk *c, double dt, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.accelerate(*c, dt, fold); }));
+  c->halo_fresh[XVEL1] = c->halo_fresh[YVEL1] = fold;
+  return CB_OK;
+}
+
+int cb_flux_calc(cb_chunk *c, double dt, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.flux_calc(*c, dt, fold); }));
+  c->halo_fresh[VOL_FLUX_X] = c->halo_fresh[VOL_FLUX_Y] = fold;
+  return CB_OK;
+}
+
+int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (sweep_number != 1 && sweep_number != 2) return fail(CB_EINVAL, "cb_advec_cell: sweep_number must be 1 or 2");
+  if (direction != 1 && direction != 2) return fail(CB_EINVAL, "cb_advec_cell: direction must be 1 (x) or 2 (y)");
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  void *dd = c->spare_base(0), *de = c->spare_base(1);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.advec_cell(*c, sweep_number, direction, fold, dd, de); }));
+  std::swap(c->field_mem[DENSITY1], c->spare_mem[0]);
+  std::swap(c->field_mem[ENERGY1], c->spare_mem[1]);
+  c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = fold;
+  c->halo_fresh[direction == 1 ? MASS_FLUX_X : MASS_FLUX_Y] = fold;
+  return CB_OK;
+}
+
+int cb_advec_mom(cb_chunk *c, int which_vel, int sweep_number, int direction, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (which_vel < 1 || which_vel > 3) return fail(CB_EINVAL, "cb_advec_mom: which_vel must be 1, 2 or 3");
+  if (sweep_number != 1 && sweep_number != 2) return fail(CB_EINVAL, "cb_advec_mom: sweep_number must be 1 or 2");
+  if (direction != 1 && direction != 2) return fail(CB_EINVAL, "cb_advec_mom: direction must be 1 (x) or 2 (y)");
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  void *du = c->spare_base(2), *dv = c->spare_base(3);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.advec_mom(*c, which_vel, sweep_number, direction, fold, du, dv); }));
+  if (which_vel & 1) {
+    std::swap(c->field_mem[XVEL1], c->spare_mem[2]);
+    c->halo_fresh[XVEL1] = fold;
+  }
+  if (which_vel & 2) {
+    std::swap(c->field_mem[YVEL1], c->spare_mem[3]);
+    c->halo_fresh[YVEL1] = fold;
+  }
+  return CB_OK;
+}
+
+int cb_reset_field(cb_chunk *c, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.reset_field(*c, fold); }));
+  c->halo_fresh[DENSITY0] = c->halo_fresh[ENERGY0] = c->halo_fresh[XVEL0] = c->halo_fresh[YVEL0] = fold;
+  return CB_OK;
+}
+
+int cb_update_halo(cb_chunk *c, const int fields[15], int depth) {
+  CB_CHECK_CHUNK(c);
+  if (!fields) return fail(CB_EINVAL, "cb_update_halo: null field list");
+  if (int r = check_depth(depth, false)) return r;
+  HaloJob job{};
+  for (int f = 0; f < 15; ++f) {
+    if (fields[f] != 1) continue;
+    if (c->can_fold() && c->halo_fresh[f] >= depth) continue; // a folded producer already wrote it
+    job.field[job.nfields++] = f;
+  }
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.update_halo(*c, job, depth); }));
+  for (int k = 0; k < job.nfields; ++k) c->halo_fresh[job.field[k]] = std::max(c->halo_fresh[job.field[k]], depth);
+  return CB_OK;
+}
+
+int cb_field_summary(cb_chunk *c, double out[5]) {
+  CB_CHECK_CHUNK(c);
+  if (!out) return fail(CB_EINVAL, "cb_field_summary: null out");
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.field_summary(*c); }));
+  CB_CUDA(cudaMemcpyAsync(&c->h_scalars[2], c->d_sums, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream));
+  CB_CUDA(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < 5; ++q) out[q] = c->h_scalars[2 + q];
+  c->halo_fresh[PRESSURE] = 0;
+  c->halo_fresh[SOUNDSPEED] = 0;
+  return CB_OK;
+}
+
+int cb_synchronize(cb_chunk *c) {
+  CB_CHECK_CHUNK(c);
+  CB_CUDA(cudaStreamSynchronize(c->stream));
+  return CB_OK;
+}
+
+int cb_get_stream(cb_chunk *c, void **stream) {
+  if (!c || !stream) return fail(CB_EINVAL, "cb_get_stream: null argument");
+  *stream = (void *)c->stream;
+  return CB_OK;
+}
+
+int cb_launch_count(const cb_chunk *c, long long *count) {
+  if (!c || !count) return fail(CB_EINVAL, "cb_launch_count: null argument");
+  *count = c->launches;
+  return CB_OK;
+}
+
+} // extern "C"

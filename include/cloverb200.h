@@ -1,0 +1,149 @@
+/*
+ * cloverb200.h -- C ABI of the B200 CloverLeaf hydro library (libcloverb200.so).
+ *
+ * One opaque cb_chunk holds one mesh chunk resident in the memory of one
+ * B200: every 2-D field of the reference's field_type
+ * (driver/definitions.h:130-170), the 1-D geometry, a CUDA stream and the
+ * scratch of the on-device reductions.  Each entry point below replaces one
+ * routine of the reference's per-model interface (the driver/NAME.h
+ * declarations every src/<model>/ implements); the comment names it.
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a nonzero CB_E* code on
+ *    failure; cb_last_error() then describes the failure (per thread).
+ *  - Indices follow the reference: interior cell (j, k) of the Fortran
+ *    original is (i, j) = (j + 1, k + 1); arrays carry a 2-deep halo.
+ *    Field extents are the reference's (driver/definitions.cpp:4-41):
+ *    cell (nx+4)x(ny+4), vertex (nx+5)x(ny+5), x face (nx+5)x(ny+4),
+ *    y face (nx+4)x(ny+5).
+ *  - Calls are enqueued on the chunk's stream and return without waiting,
+ *    except those that hand a value to the host (cb_calc_dt,
+ *    cb_field_summary, cb_read_*), which wait for it.
+ *  - halo_depth arguments (0, 1 or 2): besides its outputs, the phase also
+ *    writes their reflective halo exactly as a following
+ *    cb_update_halo(..., halo_depth) would, and the library remembers it, so
+ *    that cb_update_halo skips those fields.  0 writes no halo.  Meshes
+ *    smaller than 8 cells in either direction ignore halo_depth (there the
+ *    reference's fill reads halo cells and is not idempotent, so every
+ *    cb_update_halo runs as called), except cb_pdv(full = 1), whose halo
+ *    update is part of the routine it replaces.
+ *  - Host buffers are plain double arrays; in the FP32 form values are
+ *    converted on the way in and out.
+ */
+#ifndef CLOVERB200_H
+#define CLOVERB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cb_chunk cb_chunk;
+
+/* Field ids; 0..14 are driver/definitions.h:61-77 (field_parameter). */
+enum {
+  CB_DENSITY0 = 0, CB_DENSITY1 = 1, CB_ENERGY0 = 2, CB_ENERGY1 = 3, CB_PRESSURE = 4, CB_VISCOSITY = 5,
+  CB_SOUNDSPEED = 6, CB_XVEL0 = 7, CB_XVEL1 = 8, CB_YVEL0 = 9, CB_YVEL1 = 10, CB_VOL_FLUX_X = 11,
+  CB_VOL_FLUX_Y = 12, CB_MASS_FLUX_X = 13, CB_MASS_FLUX_Y = 14,
+  CB_WORK_ARRAY1 = 15, CB_WORK_ARRAY7 = 21, CB_VOLUME = 22, CB_XAREA = 23, CB_YAREA = 24,
+  CB_NUM_FIELDS = 25
+};
+/* 1-D geometry ids (driver/definitions.h:156-163). */
+enum { CB_CELLX = 0, CB_CELLY, CB_CELLDX, CB_CELLDY, CB_VERTEXX, CB_VERTEXY, CB_VERTEXDX, CB_VERTEXDY, CB_NUM_GEOM };
+enum { CB_FP64 = 0, CB_FP32 = 1 };
+/* Host layouts for cb_read_field / cb_write_field: row-major with x fastest,
+ * or the reference Buffer2D order data[j + i * sizeY] (src/serial/context.h:73). */
+enum { CB_LAYOUT_XFAST = 0, CB_LAYOUT_YFAST = 1 };
+/* Options for cb_set_option. */
+enum { CB_OPT_FOLD_HALO = 1, CB_OPT_RESET_BY_SWAP = 2 };
+/* Error codes. */
+enum { CB_OK = 0, CB_EINVAL = 1, CB_ECUDA = 2, CB_ENOMEM = 3, CB_ESTATE = 4 };
+
+/* A deck state (driver/definitions.h:79-95); geometry 1 rectangle, 2 circle, 3 point.
+ * Pass the extents already nudged as driver/read_input.cpp:268-276 does. */
+typedef struct {
+  double density, energy, xvel, yvel;
+  int geometry;
+  double xmin, ymin, xmax, ymax, radius;
+} cb_state;
+
+/* Safety factors of calc_dt (driver/definitions.h:240-247). */
+typedef struct {
+  double dtmin, dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;
+} cb_dt_params;
+
+/* Library version and last error of the calling thread. */
+int cb_version(void);
+const char *cb_last_error(void);
+
+/* Device discovery for the model's create_context / report_context
+ * (driver/initialise.h:160-162; the CUDA model's src/cuda/initialise.cpp:25-45). */
+int cb_device_count(int *count);
+int cb_device_name(int device, char *name, size_t len);
+
+/* Lifecycle.  Replaces the allocation in field_type's constructor
+ * (driver/definitions.cpp:4-41) and src/cuda/finalise.cpp:22-58's release.
+ * precision is CB_FP64 or CB_FP32; device is a CUDA device ordinal. */
+int cb_create(int nx, int ny, int precision, int device, cb_chunk **out);
+int cb_destroy(cb_chunk *c);
+/* gamma of the ideal-gas law; the reference hard-codes 1.4 (src/serial/ideal_gas.cpp:41-42). */
+int cb_set_gamma(cb_chunk *c, double gamma);
+int cb_set_option(cb_chunk *c, int option, int value);
+int cb_get_extent(const cb_chunk *c, int field, int *size_x, int *size_y);
+
+/* Host <-> device copies of whole fields (the model's Buffer2D::mirrored(),
+ * src/serial/context.h:82-86).  n must equal size_x * size_y of the field. */
+int cb_read_field(cb_chunk *c, int field, double *host, size_t n, int layout);
+int cb_write_field(cb_chunk *c, int field, const double *host, size_t n, int layout);
+/* 1-D geometry arrays; n = its reference length (nx+4/ny+4 cell, nx+5/ny+5 vertex). */
+int cb_read_geom(cb_chunk *c, int geom, double *host, size_t n);
+int cb_write_geom(cb_chunk *c, int geom, const double *host, size_t n);
+
+/* Setup: driver/build_field.h:24, driver/initialise_chunk.h:24, driver/generate_chunk.h:24. */
+int cb_build_field(cb_chunk *c);
+int cb_initialise_chunk(cb_chunk *c, double xmin, double ymin, double xmax, double ymax);
+int cb_generate_chunk(cb_chunk *c, int nstates, const cb_state *states);
+
+/* Hydro phases. */
+/* driver/ideal_gas.h:24 -- pressure, soundspeed from level 0 (or level 1 if predict). */
+int cb_ideal_gas(cb_chunk *c, int predict, int halo_depth);
+/* driver/viscosity.h:24. */
+int cb_viscosity(cb_chunk *c, int halo_depth);
+/* driver/calc_dt.h:26-27 -- the minimum over cells, on the device; returns the
+ * kernel's dt_min_val and control/jldt/kldt/small as src/serial/calc_dt.cpp:73-79 forms them. */
+int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *control, int *jldt, int *kldt, int *small);
+/* driver/PdV.h:24.  full = 0: the PdV kernel alone (src/serial/PdV.cpp:36-87);
+ * full = 1 with predict = 1: the model's whole predictor step (:92-133:
+ * kernel, ideal_gas on level 1, depth-1 pressure halo, revert) in one pass. */
+int cb_pdv(cb_chunk *c, int predict, double dt, int full, int halo_depth);
+/* driver/revert.h:24. */
+int cb_revert(cb_chunk *c);
+/* driver/accelerate.h:24. */
+int cb_accelerate(cb_chunk *c, double dt, int halo_depth);
+/* driver/flux_calc.h:24. */
+int cb_flux_calc(cb_chunk *c, double dt, int halo_depth);
+/* driver/advec_cell.h:24 -- dir 1 = x, 2 = y. */
+int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth);
+/* driver/advec_mom.h:24 -- which_vel 1 (x velocity), 2 (y velocity) or 3
+ * (both in one pass, as the pair of calls at driver/advection.cpp:56-57 does). */
+int cb_advec_mom(cb_chunk *c, int which_vel, int sweep_number, int direction, int halo_depth);
+/* driver/reset_field.h:24. */
+int cb_reset_field(cb_chunk *c, int halo_depth);
+/* driver/update_halo.h:24 -- fields[15] flags (field_parameter order), depth 1 or 2. */
+int cb_update_halo(cb_chunk *c, const int fields[15], int depth);
+/* driver/field_summary.h:25 -- ideal_gas then volume, mass, internal energy,
+ * kinetic energy, pressure*volume sums, reduced on the device. */
+int cb_field_summary(cb_chunk *c, double out[5]);
+/* Waits for everything enqueued on the chunk. */
+int cb_synchronize(cb_chunk *c);
+/* The CUDA stream (a cudaStream_t) the chunk's work is enqueued on, for
+ * callers that time it with their own events or order their own work after it. */
+int cb_get_stream(cb_chunk *c, void **stream);
+/* Number of kernels the library has launched for this chunk so far. */
+int cb_launch_count(const cb_chunk *c, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,79 @@
+"""Regenerates the golden fixtures in this directory from the reference itself.
+
+Runs the reference driver + serial model (built from the reference sources by
+`make -C oracle ref`, with the capture hooks of oracle/ref_hooks/) on a set
+of decks and stores, per deck:
+  <name>.in            the deck
+  <name>.summary.txt   every field_summary at full precision (step time vol mass ie ke press)
+  <name>.fields.bin    the final interior fields (CLVF format, small decks only)
+  <name>.stdout.txt    the lines of the reference's stdout that carry the verdict
+
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref/serial-capture)
+"""
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle  # noqa: E402
+from cloverleaf_b200 import deck as D  # noqa: E402
+
+# The built-in deck of driver/clover_leaf.cpp:156-171 (test_problem 1).
+DEFAULT_DECK = """*clover
+ state 1 density=0.2 energy=1.0
+ state 2 density=1.0 energy=2.5 geometry=rectangle xmin=0.0 xmax=5.0 ymin=0.0 ymax=2.0
+ x_cells=10
+ y_cells=2
+ xmin=0.0
+ ymin=0.0
+ xmax=10.0
+ ymax=2.0
+ initial_timestep=0.04
+ timestep_rise=1.5
+ max_timestep=0.04
+ end_time=3.0
+ test_problem 1
+*endclover
+"""
+
+
+def decks():
+    out = {"default10x2": (DEFAULT_DECK, True)}
+    out["bm32x87"] = (D.format_deck(D.benchmark_deck(32, 87)), True)
+    out["bm40x24x120"] = (D.format_deck(D.benchmark_deck(40, 120, ny=24)), True)
+    c = D.benchmark_deck(24, 70, ny=20)
+    c.states.append(D.State(density=2.0, energy=3.0, xvel=0.5, yvel=-0.25, geometry=D.GEOM_CIRC, xmin=6.0, ymin=6.0,
+                            radius=2.0, defined=True))
+    c.states.append(D.State(density=0.5, energy=1.5, xvel=-0.3, yvel=0.2, geometry=D.GEOM_RECT, xmin=6.0, xmax=9.0,
+                            ymin=1.0, ymax=3.0, defined=True))
+    out["circ24x20x70"] = (D.format_deck(c), True)
+    # the reference benchmark at 960^2, 87 steps (test_problem 2): summaries only
+    out["bm960x87"] = (D.format_deck(D.benchmark_deck(960, 87, test_problem=2)), False)
+    return out
+
+
+def main():
+    for name, (text, keep_fields) in decks().items():
+        res = oracle.run_reference(text)
+        if res["returncode"] != 0:
+            raise SystemExit(f"{name}: reference exited {res['returncode']}")
+        with open(os.path.join(HERE, name + ".in"), "w") as f:
+            f.write(text)
+        with open(os.path.join(HERE, name + ".summary.txt"), "w") as f:
+            for r in res["summaries"]:
+                f.write("%d %.17e %.17e %.17e %.17e %.17e %.17e\n" % r)
+        keep = [l for l in res["stdout"].splitlines() if "within" in l or "PASSED" in l or "Outcome" in l]
+        with open(os.path.join(HERE, name + ".stdout.txt"), "w") as f:
+            f.write("\n".join(keep) + "\n")
+        if keep_fields:
+            fl = res["fields"]
+            d = D.parse_deck(text)
+            oracle.write_fields(os.path.join(HERE, name + ".fields.bin"), d.x_cells, d.y_cells, fl)
+        print(name, len(res["summaries"]), "summaries", "fields" if keep_fields else "")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,79 @@
+"""The drop-in: the reference's unchanged C++ driver linked against the b200
+model (cloverleaf_b200/bin/clover_leaf) runs the decks and passes the
+driver's own expected-solution check; its full-precision captures equal the
+reference serial build's (fields bit for bit, summaries to 1e-12)."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle
+from cloverleaf_b200 import deck as D
+from golden_util import CAPTURED, SMALL_DECKS, deck_text, fields, rel, summaries
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "cloverleaf_b200", "bin", "clover_leaf")
+
+
+def run_driver(text, env_extra=None, args=()):
+    assert os.path.exists(EXE), "driver binary not built (make -C cloverleaf_b200/model)"
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = os.path.join(tmp, "clover.in")
+        open(deck, "w").write(text)
+        env = dict(os.environ)
+        env["CLOVER_CAPTURE_SUMMARY"] = os.path.join(tmp, "s.txt")
+        env["CLOVER_CAPTURE_FIELDS"] = os.path.join(tmp, "f.bin")
+        env.update(env_extra or {})
+        p = subprocess.run([EXE, "--file", deck, *args], cwd=tmp, env=env, capture_output=True, text=True, timeout=600)
+        summ = []
+        if os.path.exists(env["CLOVER_CAPTURE_SUMMARY"]):
+            for line in open(env["CLOVER_CAPTURE_SUMMARY"]):
+                w = line.split()
+                summ.append((int(w[0]),) + tuple(float(x) for x in w[1:]))
+        flds = oracle.read_fields(env["CLOVER_CAPTURE_FIELDS"]) if os.path.exists(env["CLOVER_CAPTURE_FIELDS"]) else {}
+        return p, summ, flds
+
+
+@pytest.mark.parametrize("name", SMALL_DECKS)
+def test_driver_matches_reference(name):
+    p, summ, flds = run_driver(deck_text(name))
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    gold = summaries(name)
+    assert len(summ) == len(gold)
+    for s, g in zip(summ, gold):
+        assert s[0] == g[0] and s[1] == g[1]
+        for a, b in zip(s[2:], g[2:]):
+            assert rel(a, b) <= 1e-12
+    gf = fields(name)
+    for fid, _ in CAPTURED:
+        assert np.array_equal(flds[fid], gf[fid]), fid
+
+
+def test_driver_default_deck_passes():
+    p, _, _ = run_driver(deck_text("default10x2"))
+    assert p.returncode == 0
+    assert "This test is considered PASSED" in p.stdout
+
+
+def test_driver_unfolded_and_profiled():
+    p, summ, flds = run_driver(deck_text("bm32x87"), {"CLOVER_B200_FOLD": "0"}, ["--profile"])
+    assert p.returncode == 0, p.stdout[-2000:]
+    assert "Profiler Output" in p.stdout
+    gf = fields("bm32x87")
+    for fid, _ in CAPTURED:
+        assert np.array_equal(flds[fid], gf[fid]), fid
+
+
+@pytest.mark.slow
+def test_driver_config1_960_passes():
+    p, summ, _ = run_driver(deck_text("bm960x87"))
+    assert p.returncode == 0, p.stdout[-3000:]
+    assert "Test problem 2 is within" in p.stdout and "This test is considered PASSED" in p.stdout
+    gold = summaries("bm960x87")
+    for s, g in zip(summ, gold):
+        for a, b in zip(s[2:], g[2:]):
+            assert rel(a, b) <= 5e-11
