@@ -16,15 +16,7 @@
 
 #include "../../include/cloverb200.h"
 #include "cb_chunk.h"
-#include "cb_phase.cuh"
-
-namespace cb {
-template <typename T> struct Ops;
-}
-#include "cb_ops.cuh"
-
-extern template struct cb::Ops<double>;
-extern template struct cb::Ops<float>;
+#include "cb_ops.h"
 
 struct cb_chunk : cb::Chunk {};
 

@@ -1,5 +1,5 @@
 // cb_fp32.cu -- FP32 instantiation of the phase kernels (the FP32 storage
 // form; FP64 where the kernels say `double`).  Multiply-adds may contract.
-#include "cb_ops.cuh"
+#include "cb_ops_impl.cuh"
 
 template struct cb::Ops<float>;

@@ -1,0 +1,48 @@
+// cb_ops.h -- declarations of the phase-kernel launchers.  The definitions
+// (cb_ops_impl.cuh) are compiled only in cb_fp64.cu (with -fmad=false, for
+// bit parity with the reference) and cb_fp32.cu; the C-ABI translation unit
+// sees these declarations alone, so no kernel is ever compiled with the
+// wrong contraction setting.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "cb_chunk.h"
+
+namespace cb {
+
+struct DevState {
+  double density, energy, xvel, yvel;
+  int geometry;
+  double xmin, ymin, xmax, ymax, radius;
+};
+
+struct DtConsts {
+  double dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;
+};
+
+struct HaloJob {
+  int nfields;
+  int field[15];
+};
+
+template <typename T> struct Ops {
+  static cudaError_t generate_chunk(Chunk &c, const DevState *d_states, int nstates);
+  static cudaError_t ideal_gas(Chunk &c, int predict, int fold);
+  static cudaError_t viscosity(Chunk &c, int fold);
+  static cudaError_t calc_dt(Chunk &c, const DtConsts &k);
+  static cudaError_t pdv(Chunk &c, int predict, double dt, int mode, int fold);
+  static cudaError_t revert(Chunk &c);
+  static cudaError_t accelerate(Chunk &c, double dt, int fold);
+  static cudaError_t flux_calc(Chunk &c, double dt, int fold);
+  static cudaError_t advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de);
+  static cudaError_t advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv);
+  static cudaError_t reset_field(Chunk &c, int fold);
+  static cudaError_t update_halo(Chunk &c, const HaloJob &job, int depth);
+  static cudaError_t field_summary(Chunk &c);
+};
+
+extern template struct Ops<double>;
+extern template struct Ops<float>;
+
+} // namespace cb

@@ -1,0 +1,178 @@
+// cb_ops_impl.cuh -- definitions of the phase-kernel launchers (declared in
+// cb_ops.h).  Included only by cb_fp64.cu and cb_fp32.cu, which instantiate
+// Ops<double> and Ops<float>.
+#pragma once
+
+#include <algorithm>
+
+#include "cb_ops.h"
+#include "cb_phase.cuh"
+
+namespace cb {
+
+namespace detail {
+
+template <typename T> Fields<T> fields(const Chunk &c) {
+  Fields<T> F;
+  for (int f = 0; f < NUM_FIELDS; ++f) F.f[f] = (T *)c.base(f);
+  return F;
+}
+
+template <typename T> Mesh<T> mesh(const Chunk &c) {
+  Mesh<T> m;
+  m.nx = c.nx;
+  m.ny = c.ny;
+  m.pitch = c.pitch;
+  m.celldx = c.geom_d[CELLDX];
+  m.celldy = c.geom_d[CELLDY];
+  m.vertexdx = c.geom_d[VERTEXDX];
+  m.vertexdy = c.geom_d[VERTEXDY];
+  m.celldx_t = (const T *)c.geom_t[CELLDX];
+  m.celldy_t = (const T *)c.geom_t[CELLDY];
+  return m;
+}
+
+inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+
+// Counts one kernel launch and returns its launch status.
+inline cudaError_t launched(Chunk &c) {
+  ++c.launches;
+  return cudaGetLastError();
+}
+
+template <typename T> T gm1(const Chunk &c) { return (T)(c.gamma - 1.0); }
+
+inline int reduce_grid(const Chunk &c, int ntiles) { return std::min(ntiles, c.summary_grid); }
+
+// Copies the ring around the updated rectangle [ilo, ihi] x [jlo, jhi] from
+// src to dst (double-buffered phases whose halo is not folded).
+template <typename T>
+cudaError_t copy_ring(Chunk &c, const void *src, void *dst, int ilo, int ihi, int jlo, int jhi, int ex, int ey) {
+  const int n = ex * ey;
+  k_copy_ring<T><<<(n + 255) / 256, 256, 0, c.stream>>>((const T *)src, (T *)dst, mesh<T>(c), ilo, ihi, jlo, jhi, ex, ey);
+  return launched(c);
+}
+
+} // namespace detail
+
+using namespace detail;
+
+template <typename T> cudaError_t Ops<T>::generate_chunk(Chunk &c, const DevState *d_states, int nstates) {
+  dim3 b(32, 8);
+  k_generate_chunk<T><<<grid2(c.nx + 5, c.ny + 5, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), d_states, nstates, c.geom_d[CELLX],
+                                                                        c.geom_d[CELLY], c.geom_d[VERTEXX], c.geom_d[VERTEXY]);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::ideal_gas(Chunk &c, int predict, int fold) {
+  dim3 b(32, 8);
+  k_ideal_gas<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), predict, gm1<T>(c), fold);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::viscosity(Chunk &c, int fold) {
+  dim3 b(32, 8);
+  k_viscosity<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), fold);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::calc_dt(Chunk &c, const DtConsts &k) {
+  dim3 b(32, 8);
+  const int tx = (c.nx + 31) / 32, ty = (c.ny + 7) / 8;
+  const int nt = tx * ty;
+  k_calc_dt<T><<<reduce_grid(c, nt), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), k, c.d_dt_bits, tx, nt);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::pdv(Chunk &c, int predict, double dt, int mode, int fold) {
+  dim3 b(32, 8);
+  k_pdv<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), predict, (T)dt, mode, gm1<T>(c), fold);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::revert(Chunk &c) {
+  dim3 b(32, 8);
+  k_revert<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c));
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::accelerate(Chunk &c, double dt, int fold) {
+  dim3 b(32, 8);
+  k_accelerate<T><<<grid2(c.nx + 1, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), (T)dt, fold);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fold) {
+  dim3 b(32, 8);
+  k_flux_calc<T><<<grid2(c.nx + 1, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), (T)dt, fold);
+  return launched(c);
+}
+
+// dir 1 = x, 2 = y.  The updated density/energy go to (dd, de); the caller swaps buffers.
+template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de) {
+  const T *sd = (const T *)c.base(DENSITY1), *se = (const T *)c.base(ENERGY1);
+  cudaError_t e;
+  if (fold != 2) { // keep the halo ring exactly as the in-place reference leaves it
+    if ((e = copy_ring<T>(c, sd, dd, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
+    if ((e = copy_ring<T>(c, se, de, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
+  }
+  if (dir == 1) {
+    using K = CellSweep<1>;
+    dim3 g((c.nx + K::NA - 1) / K::NA, (c.ny + K::NL - 1) / K::NL);
+    k_advec_cell<T, 1><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), sweep, sd, se, (T *)dd, (T *)de, fold);
+  } else {
+    using K = CellSweep<2>;
+    dim3 g((c.nx + K::NL - 1) / K::NL, (c.ny + K::NA - 1) / K::NA);
+    k_advec_cell<T, 2><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), sweep, sd, se, (T *)dd, (T *)de, fold);
+  }
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv) {
+  const T *su = (const T *)c.base(XVEL1), *sv = (const T *)c.base(YVEL1);
+  cudaError_t e;
+  if (fold != 2) {
+    if ((vel_mask & 1) && (e = copy_ring<T>(c, su, du, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
+    if ((vel_mask & 2) && (e = copy_ring<T>(c, sv, dv, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
+  }
+  // nodes [2, n+2] along both axes: n+1 of them
+  if (dir == 1) {
+    using K = MomSweep<1>;
+    dim3 g((c.nx + 1 + K::NA - 1) / K::NA, (c.ny + 1 + K::NL - 1) / K::NL);
+    k_advec_mom<T, 1><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), vel_mask, sweep, su, sv, (T *)du, (T *)dv, fold);
+  } else {
+    using K = MomSweep<2>;
+    dim3 g((c.nx + 1 + K::NL - 1) / K::NL, (c.ny + 1 + K::NA - 1) / K::NA);
+    k_advec_mom<T, 2><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), vel_mask, sweep, su, sv, (T *)du, (T *)dv, fold);
+  }
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::reset_field(Chunk &c, int fold) {
+  dim3 b(32, 8);
+  k_reset_field<T><<<grid2(c.nx + 1, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), fold);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::update_halo(Chunk &c, const HaloJob &job, int depth) {
+  if (job.nfields == 0) return cudaSuccess;
+  const int len = std::max(c.nx, c.ny) + 5 + 2 * depth;
+  dim3 g((len + 127) / 128, job.nfields);
+  for (int pass = 0; pass < 2; ++pass) {
+    k_update_halo<T><<<g, 128, 0, c.stream>>>(fields<T>(c), mesh<T>(c), job, depth, pass);
+    cudaError_t e = launched(c);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <typename T> cudaError_t Ops<T>::field_summary(Chunk &c) {
+  dim3 b(32, 8);
+  const int tx = (c.nx + 31) / 32, ty = (c.ny + 7) / 8;
+  const int nt = tx * ty;
+  k_field_summary<T><<<reduce_grid(c, nt), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), gm1<T>(c), c.d_partials, c.d_counter, c.d_sums,
+                                                             tx, nt);
+  return launched(c);
+}
+
+} // namespace cb

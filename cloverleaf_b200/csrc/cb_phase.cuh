@@ -15,6 +15,7 @@
 #pragma once
 
 #include "cb_mesh.cuh"
+#include "cb_ops.h"
 
 namespace cb {
 
@@ -27,12 +28,6 @@ template <typename T> struct Fields {
 // generate_chunk: src/serial/generate_chunk.cpp:31-131.  Later states
 // overwrite earlier ones; a node takes the velocity of the last state that
 // paints any of the (up to four) cells whose loop iteration writes it.
-struct DevState {
-  double density, energy, xvel, yvel;
-  int geometry;
-  double xmin, ymin, xmax, ymax, radius;
-};
-
 template <typename T>
 __device__ __forceinline__ bool state_hits(const DevState &s, const Mesh<T> &m, const double *cellx, const double *celly,
                                            const double *vertexx, const double *vertexy, int i, int j) {
@@ -166,10 +161,6 @@ __global__ void k_viscosity(Fields<T> F, Mesh<T> m, int fold) {
 // in T; the minimum is taken in FP64 on the device: a warp/block min, then
 // one atomicMin per block on the bit pattern (all candidates are >= 0 and
 // NaN candidates lose, as std::fmin ignores them).
-struct DtConsts {
-  double dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;
-};
-
 template <typename T>
 __device__ __forceinline__ T dt_candidate(const Fields<T> &F, const Mesh<T> &m, const DtConsts &k, int i, int j) {
   const T dsx = m.celldx_t[i], dsy = m.celldy_t[j];
@@ -381,9 +372,9 @@ __global__ void k_flux_calc(Fields<T> F, Mesh<T> m, T dt, int fold) {
 // advec_cell: src/serial/advec_cell.cpp:28-220, the three loops of one sweep
 // fused into one pass.  Reads density1/energy1 from (sd, se), writes the
 // update to (dd, de) -- the host swaps the buffers afterwards -- and writes
-// the mass flux of the sweep direction.  pre_vol/ener_flux stay on chip.
-// Each thread owns one cell; a block row computes the fluxes of its faces
-// (one more face than cells) into shared memory first.
+// the mass flux of the sweep direction.  pre_vol/ener_flux stay on chip:
+// a block first computes the fluxes of its faces (one more face than cells
+// per line) into shared memory, then updates its cells.
 template <typename T>
 __device__ __forceinline__ T cell_limiter(T sigma, T sigma3, T sigma4, T diffuw, T diffdw) {
   const T one_by_six = T(1.0 / 6.0);
@@ -407,18 +398,28 @@ __device__ __forceinline__ T cell_pre_vol(const T *vfx, const T *vfy, const Mesh
   return vol + vfy[m.at(i, j + 1)] - vfy[m.at(i, j)];
 }
 
-// Mass and energy flux through face f (x face f = left face of cell f when
-// dir == 1, bottom face when dir == 2) of line `line`.
-// Returns mass flux; energy flux in *ef.  `mf_t` is the type mass fluxes
-// are kept in (FP64 in both forms).
-template <typename T>
-__device__ __forceinline__ double cell_face_flux(const T *d1, const T *e1, const T *vfx, const T *vfy, const Mesh<T> &m,
-                                                 int sweep, int dir, int f, int line, double *ef) {
-  const int nmax = dir == 1 ? m.nx : m.ny;
-  const T *vf = dir == 1 ? vfx : vfy;
-  const double *vdx = dir == 1 ? m.vertexdx : m.vertexdy;
-  auto at = [&](int a) { return dir == 1 ? m.at(a, line) : m.at(line, a); };
-  auto pv = [&](int a) { return dir == 1 ? cell_pre_vol(vfx, vfy, m, sweep, dir, a, line) : cell_pre_vol(vfx, vfy, m, sweep, dir, line, a); };
+// Block shapes of the cell sweeps.  threadIdx.x always runs along x so every
+// warp reads consecutive addresses; in the x sweep the TA = 32 x-threads cover
+// NA = 64 cells and the 8 y-threads 8 rows, in the y sweep the 8 y-threads
+// cover NA = 32 cells along y and the 32 x-threads 32 columns.
+template <int DIR> struct CellSweep;
+template <> struct CellSweep<1> { static constexpr int TX = 32, TY = 8, TA = 32, NA = 64, NL = 8; };
+template <> struct CellSweep<2> { static constexpr int TX = 32, TY = 8, TA = 8, NA = 32, NL = 32; };
+
+// Mass and energy flux through face f of line `line` (an x face, the left
+// face of cell f, when DIR == 1; a y face when DIR == 2): the flux loop body
+// of advec_cell.cpp:68-113 / :160-205.  Returns the mass flux; the energy
+// flux is formed in FP64 (the FP32 form keeps that accumulation in FP64).
+template <typename T, int DIR>
+__device__ __forceinline__ double cell_face_flux(const T *d1, const T *e1, const T *vfx, const T *vfy, const Mesh<T> &m, int sweep,
+                                                 int f, int line, double *ef) {
+  const int nmax = DIR == 1 ? m.nx : m.ny;
+  const T *vf = DIR == 1 ? vfx : vfy;
+  const double *vdx = DIR == 1 ? m.vertexdx : m.vertexdy;
+  auto at = [&](int a) { return DIR == 1 ? m.at(a, line) : m.at(line, a); };
+  auto pv = [&](int a) {
+    return DIR == 1 ? cell_pre_vol(vfx, vfy, m, sweep, DIR, a, line) : cell_pre_vol(vfx, vfy, m, sweep, DIR, line, a);
+  };
   const T flux = vf[at(f)];
   int upwind, donor, downwind, dif;
   if (flux > T(0.0)) {
@@ -442,55 +443,59 @@ __device__ __forceinline__ double cell_face_flux(const T *d1, const T *e1, const
   return (double)mass_flux;
 }
 
-template <typename T, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY) k_advec_cell(Fields<T> F, Mesh<T> m, int sweep, int dir, const T *sd, const T *se, T *dd,
-                                                       T *de, int fold) {
-  // dir 1: threads tile cells along x; dir 2: along y (the sweep axis is
-  // always the "a" axis below, the other is the "line").
-  __shared__ double s_mf[BY][BX + 1];
-  __shared__ double s_ef[BY][BX + 1];
-  const int na = dir == 1 ? m.nx : m.ny, nl = dir == 1 ? m.ny : m.nx;
-  const int a0 = 2 + blockIdx.x * BX;
-  const int a = a0 + threadIdx.x;
-  const int line = 2 + blockIdx.y * BY + threadIdx.y;
-  T *mf = F.f[dir == 1 ? MASS_FLUX_X : MASS_FLUX_Y];
-  const T *vfx = F.f[VOL_FLUX_X], *vfy = F.f[VOL_FLUX_Y];
-  auto at = [&](int aa, int ll) { return dir == 1 ? m.at(aa, ll) : m.at(ll, aa); };
+template <typename T, int DIR>
+__global__ void __launch_bounds__(256) k_advec_cell(Fields<T> F, Mesh<T> m, int sweep, const T *sd, const T *se, T *dd, T *de,
+                                                    int fold) {
+  using K = CellSweep<DIR>;
+  constexpr int NA = K::NA, NL = K::NL, TA = K::TA;
+  __shared__ double s_mf[(NA + 1) * NL];
+  __shared__ double s_ef[(NA + 1) * NL];
+  // shared layout keeps the warp's fastest thread index contiguous
+  auto sidx = [](int p, int l) { return DIR == 1 ? l * (NA + 1) + p : p * NL + l; };
+  const int ta = DIR == 1 ? threadIdx.x : threadIdx.y;
+  const int tl = DIR == 1 ? threadIdx.y : threadIdx.x;
+  const int na = DIR == 1 ? m.nx : m.ny, nl = DIR == 1 ? m.ny : m.nx;
+  const int a0 = 2 + (DIR == 1 ? blockIdx.x : blockIdx.y) * NA;
+  const int line = 2 + (DIR == 1 ? blockIdx.y : blockIdx.x) * NL + tl;
   const bool line_ok = line < nl + 2;
-  // faces a0 .. a0 + BX (faces run to na + 3 inclusive)
-  for (int t = threadIdx.x; t <= BX; t += BX) {
-    const int f = a0 + t;
-    if (line_ok && f <= na + 3) {
-      double ef;
-      double mfv = cell_face_flux(sd, se, vfx, vfy, m, sweep, dir, f, line, &ef);
-      s_mf[threadIdx.y][t] = mfv;
-      s_ef[threadIdx.y][t] = ef;
-      const bool halo_face = fold && f == na + 3; // overwritten by the fold of face na+1
-      if (!halo_face) mf[at(f, line)] = (T)mfv;
-      if (fold && f < na + 3) {
-        if (dir == 1) fold_halo(mf, m, halo_rule(MASS_FLUX_X), fold, f, line, (T)mfv);
-        else fold_halo(mf, m, halo_rule(MASS_FLUX_Y), fold, line, f, (T)mfv);
-      }
+  T *mf = F.f[DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y];
+  const T *vfx = F.f[VOL_FLUX_X], *vfy = F.f[VOL_FLUX_Y];
+  auto at = [&](int aa, int ll) { return DIR == 1 ? m.at(aa, ll) : m.at(ll, aa); };
+  // faces a0 .. a0 + NA (faces run to na + 3)
+  for (int p = ta; p <= NA; p += TA) {
+    const int f = a0 + p;
+    if (!line_ok || f > na + 3) continue;
+    double ef;
+    const double mfv = cell_face_flux<T, DIR>(sd, se, vfx, vfy, m, sweep, f, line, &ef);
+    s_mf[sidx(p, tl)] = mfv;
+    s_ef[sidx(p, tl)] = ef;
+    if (!(fold && f == na + 3)) mf[at(f, line)] = (T)mfv; // with a fold, face na+3 takes its halo value
+    if (fold && f < na + 3) {
+      if (DIR == 1) fold_halo(mf, m, halo_rule(MASS_FLUX_X), fold, f, line, (T)mfv);
+      else fold_halo(mf, m, halo_rule(MASS_FLUX_Y), fold, line, f, (T)mfv);
     }
   }
   __syncthreads();
-  if (!line_ok || a >= na + 2) return;
-  const long long id = at(a, line);
-  const T pre_vol = cell_pre_vol(vfx, vfy, m, sweep, dir, dir == 1 ? a : line, dir == 1 ? line : a);
-  const T *vf = dir == 1 ? vfx : vfy;
-  // cell-advection mass/energy accumulation in FP64 (the FP32 form keeps it too)
-  double pre_mass_s = (double)sd[id] * (double)pre_vol;
-  double post_mass_s = pre_mass_s + s_mf[threadIdx.y][threadIdx.x] - s_mf[threadIdx.y][threadIdx.x + 1];
-  double post_ener_s = ((double)se[id] * pre_mass_s + s_ef[threadIdx.y][threadIdx.x] - s_ef[threadIdx.y][threadIdx.x + 1]) / post_mass_s;
-  double advec_vol_s = (double)pre_vol + (double)vf[id] - (double)vf[at(a + 1, line)];
-  T dnew = (T)(post_mass_s / advec_vol_s);
-  T enew = (T)post_ener_s;
-  dd[id] = dnew;
-  de[id] = enew;
-  if (fold) {
-    const int i = dir == 1 ? a : line, j = dir == 1 ? line : a;
-    fold_halo(dd, m, halo_rule(DENSITY1), fold, i, j, dnew);
-    fold_halo(de, m, halo_rule(ENERGY1), fold, i, j, enew);
+  const T *vf = DIR == 1 ? vfx : vfy;
+  for (int p = ta; p < NA; p += TA) {
+    const int a = a0 + p;
+    if (!line_ok || a >= na + 2) continue;
+    const long long id = at(a, line);
+    const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+    const T pre_vol = cell_pre_vol(vfx, vfy, m, sweep, DIR, i, j);
+    // advec_cell.cpp:122-128: the mass/energy accumulation, in FP64 in both forms
+    double pre_mass_s = (double)sd[id] * (double)pre_vol;
+    double post_mass_s = pre_mass_s + s_mf[sidx(p, tl)] - s_mf[sidx(p + 1, tl)];
+    double post_ener_s = ((double)se[id] * pre_mass_s + s_ef[sidx(p, tl)] - s_ef[sidx(p + 1, tl)]) / post_mass_s;
+    double advec_vol_s = (double)pre_vol + (double)vf[id] - (double)vf[at(a + 1, line)];
+    T dnew = (T)(post_mass_s / advec_vol_s);
+    T enew = (T)post_ener_s;
+    dd[id] = dnew;
+    de[id] = enew;
+    if (fold) {
+      fold_halo(dd, m, halo_rule(DENSITY1), fold, i, j, dnew);
+      fold_halo(de, m, halo_rule(ENERGY1), fold, i, j, enew);
+    }
   }
 }
 
@@ -499,9 +504,7 @@ __global__ void __launch_bounds__(BX *BY) k_advec_cell(Fields<T> F, Mesh<T> m, i
 // one pass when vel_mask == 3 (the which_vel == 1 call computes node flux
 // and node masses that the which_vel == 2 call reuses, :81-103).  Reads
 // velocities from (su, sv), writes to (du, dv); the host swaps buffers.
-// Block layout: threads along the sweep axis cover nodes [a0 - 2, a0 - 2 + BX),
-// of which [a0, a0 + BX - 4) are updated; the two outer nodes on each side
-// only feed node_flux / node_mass_pre / mom_flux of the inner ones.
+// node_flux, node masses and mom_flux stay in shared memory.
 template <typename T>
 __device__ __forceinline__ T mom_limited(T vdiffuw, T vdiffdw, T sigma, T width, T dx_dif) {
   T limiter = T(0.0);
@@ -525,82 +528,107 @@ __device__ __forceinline__ T mom_post_vol(const T *vfx, const T *vfy, const Mesh
   return vol;
 }
 
-template <typename T, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY) k_advec_mom(Fields<T> F, Mesh<T> m, int vel_mask, int sweep, int dir, const T *su, const T *sv,
-                                                      T *du, T *dv, int fold) {
-  __shared__ T s_nf[BY][BX];   // node_flux
-  __shared__ T s_nmpre[BY][BX]; // node_mass_pre
-  __shared__ T s_mfu[BY][BX];  // mom_flux of u
-  __shared__ T s_mfv[BY][BX];  // mom_flux of v
-  const int mom_sweep = dir + 2 * (sweep - 1);
-  const int na = dir == 1 ? m.nx : m.ny, nl = dir == 1 ? m.ny : m.nx;
-  const int a0 = 2 + blockIdx.x * (BX - 4);
-  const int a = a0 - 2 + threadIdx.x;             // node index along the sweep axis
-  const int line = 2 + blockIdx.y * BY + threadIdx.y; // node index across
+// Block shapes of the momentum sweeps: NA nodes along the sweep axis per
+// block (plus two on each side that only feed the fluxes of the inner ones),
+// NL lines across; threadIdx.x runs along x in both directions.
+template <int DIR> struct MomSweep;
+template <> struct MomSweep<1> { static constexpr int TX = 32, TY = 8, TA = 32, NA = 64, NL = 8; };
+template <> struct MomSweep<2> { static constexpr int TX = 32, TY = 8, TA = 8, NA = 32, NL = 32; };
+
+template <typename T, int DIR>
+__global__ void __launch_bounds__(256) k_advec_mom(Fields<T> F, Mesh<T> m, int vel_mask, int sweep, const T *su, const T *sv, T *du,
+                                                   T *dv, int fold) {
+  using K = MomSweep<DIR>;
+  constexpr int NA = K::NA, NL = K::NL, TA = K::TA, NP = NA + 4;
+  __shared__ T s_nf[NP * NL];     // node_flux
+  __shared__ T s_nmpre[NP * NL];  // node_mass_pre
+  __shared__ T s_nmpost[NP * NL]; // node_mass_post
+  __shared__ T s_mfu[NP * NL];    // mom_flux of the x velocity
+  __shared__ T s_mfv[NP * NL];    // mom_flux of the y velocity
+  auto sidx = [](int p, int l) { return DIR == 1 ? l * NP + p : p * NL + l; };
+  const int mom_sweep = DIR + 2 * (sweep - 1);
+  const int ta = DIR == 1 ? threadIdx.x : threadIdx.y;
+  const int tl = DIR == 1 ? threadIdx.y : threadIdx.x;
+  const int na = DIR == 1 ? m.nx : m.ny, nl = DIR == 1 ? m.ny : m.nx;
+  const int a0 = 2 + (DIR == 1 ? blockIdx.x : blockIdx.y) * NA; // first updated node; position p <-> node a0 - 2 + p
+  const int line = 2 + (DIR == 1 ? blockIdx.y : blockIdx.x) * NL + tl;
   const bool line_ok = line < nl + 3;
-  auto at = [&](int aa, int ll) { return dir == 1 ? m.at(aa, ll) : m.at(ll, aa); };
+  auto at = [&](int aa, int ll) { return DIR == 1 ? m.at(aa, ll) : m.at(ll, aa); };
   const T *vfx = F.f[VOL_FLUX_X], *vfy = F.f[VOL_FLUX_Y];
   const T *d1 = F.f[DENSITY1];
-  const T *mflux = F.f[dir == 1 ? MASS_FLUX_X : MASS_FLUX_Y];
-  // node_flux(a) over a in [0, na+3]; node_mass_post/pre(a) over [1, na+3]
-  T nf = T(0.0), nmpost = T(1.0), nmpre = T(1.0);
-  const bool a_ok = a >= 0 && a <= na + 3;
-  if (line_ok && a_ok) {
-    if (dir == 1) {
-      nf = T(0.25) * (mflux[m.at(a, line - 1)] + mflux[m.at(a, line)] + mflux[m.at(a + 1, line - 1)] + mflux[m.at(a + 1, line)]);
-    } else {
-      nf = T(0.25) * (mflux[m.at(line - 1, a)] + mflux[m.at(line, a)] + mflux[m.at(line - 1, a + 1)] + mflux[m.at(line, a + 1)]);
+  const T *mflux = F.f[DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y];
+  // node_flux over nodes [0, na+3] (advec_mom.cpp:84-88 / :156-160)
+  for (int p = ta; p < NP; p += TA) {
+    const int a = a0 - 2 + p;
+    T nf = T(0.0);
+    if (line_ok && a >= 0 && a <= na + 3) {
+      if (DIR == 1)
+        nf = T(0.25) * (mflux[m.at(a, line - 1)] + mflux[m.at(a, line)] + mflux[m.at(a + 1, line - 1)] + mflux[m.at(a + 1, line)]);
+      else
+        nf = T(0.25) * (mflux[m.at(line - 1, a)] + mflux[m.at(line, a)] + mflux[m.at(line - 1, a + 1)] + mflux[m.at(line, a + 1)]);
     }
+    s_nf[sidx(p, tl)] = nf;
   }
-  s_nf[threadIdx.y][threadIdx.x] = nf;
   __syncthreads();
-  if (line_ok && a >= 1 && a <= na + 3) {
-    // node (i, j) mass from cells (i-1..i, j-1..j)
-    const int i = dir == 1 ? a : line, j = dir == 1 ? line : a;
-    nmpost = T(0.25) * (d1[m.at(i, j - 1)] * mom_post_vol(vfx, vfy, m, mom_sweep, i, j - 1) +
-                        d1[m.at(i, j)] * mom_post_vol(vfx, vfy, m, mom_sweep, i, j) +
-                        d1[m.at(i - 1, j - 1)] * mom_post_vol(vfx, vfy, m, mom_sweep, i - 1, j - 1) +
-                        d1[m.at(i - 1, j)] * mom_post_vol(vfx, vfy, m, mom_sweep, i - 1, j));
-    const T nf_prev = threadIdx.x > 0 ? s_nf[threadIdx.y][threadIdx.x - 1] : T(0.0);
-    nmpre = nmpost - nf_prev + nf;
+  // node_mass_post / node_mass_pre over nodes [1, na+3] (:93-102 / :165-174)
+  for (int p = ta; p < NP; p += TA) {
+    const int a = a0 - 2 + p;
+    T nmpost = T(1.0), nmpre = T(1.0);
+    if (line_ok && p >= 1 && a >= 1 && a <= na + 3) {
+      const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+      nmpost = T(0.25) * (d1[m.at(i, j - 1)] * mom_post_vol(vfx, vfy, m, mom_sweep, i, j - 1) +
+                          d1[m.at(i, j)] * mom_post_vol(vfx, vfy, m, mom_sweep, i, j) +
+                          d1[m.at(i - 1, j - 1)] * mom_post_vol(vfx, vfy, m, mom_sweep, i - 1, j - 1) +
+                          d1[m.at(i - 1, j)] * mom_post_vol(vfx, vfy, m, mom_sweep, i - 1, j));
+      nmpre = nmpost - s_nf[sidx(p - 1, tl)] + s_nf[sidx(p, tl)];
+    }
+    s_nmpost[sidx(p, tl)] = nmpost;
+    s_nmpre[sidx(p, tl)] = nmpre;
   }
-  s_nmpre[threadIdx.y][threadIdx.x] = nmpre;
   __syncthreads();
-  // mom_flux(a) for a in [1, na+2]: needs node_mass_pre(donor), vel at a-1..a+2
-  const T *celld = dir == 1 ? m.celldx_t : m.celldy_t;
-  if (line_ok && a >= 1 && a <= na + 2 && threadIdx.x >= 1 && threadIdx.x <= BX - 2) {
+  // mom_flux over nodes [1, na+2] (:108-133 / :180-205): positions [1, NA+1]
+  const T *celld = DIR == 1 ? m.celldx_t : m.celldy_t;
+  for (int p = 1 + ta; p <= NA + 1; p += TA) {
+    const int a = a0 - 2 + p;
+    if (!line_ok || a < 1 || a > na + 2) continue;
+    const T nf = s_nf[sidx(p, tl)];
     int upwind, donor, downwind, dif;
     if (nf < T(0.0)) {
       upwind = a + 2; donor = a + 1; downwind = a; dif = donor;
     } else {
       upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
     }
-    const T sigma = fabs(nf) / s_nmpre[threadIdx.y][threadIdx.x + (donor - a)];
+    const T sigma = fabs(nf) / s_nmpre[sidx(p + (donor - a), tl)];
     const T width = celld[a];
     if (vel_mask & 1) {
       const T vd = su[at(donor, line)];
       T lim = mom_limited(vd - su[at(upwind, line)], su[at(downwind, line)] - vd, sigma, width, celld[dif]);
-      s_mfu[threadIdx.y][threadIdx.x] = (vd + (T(1.0) - sigma) * lim) * nf;
+      s_mfu[sidx(p, tl)] = (vd + (T(1.0) - sigma) * lim) * nf;
     }
     if (vel_mask & 2) {
       const T vd = sv[at(donor, line)];
       T lim = mom_limited(vd - sv[at(upwind, line)], sv[at(downwind, line)] - vd, sigma, width, celld[dif]);
-      s_mfv[threadIdx.y][threadIdx.x] = (vd + (T(1.0) - sigma) * lim) * nf;
+      s_mfv[sidx(p, tl)] = (vd + (T(1.0) - sigma) * lim) * nf;
     }
   }
   __syncthreads();
-  if (!line_ok || a < a0 || a >= a0 + BX - 4 || a > na + 2) return;
-  const long long id = at(a, line);
-  const int i = dir == 1 ? a : line, j = dir == 1 ? line : a;
-  if (vel_mask & 1) {
-    T v = (su[id] * nmpre + s_mfu[threadIdx.y][threadIdx.x - 1] - s_mfu[threadIdx.y][threadIdx.x]) / nmpost;
-    du[id] = v;
-    if (fold) fold_halo(du, m, halo_rule(XVEL1), fold, i, j, v);
-  }
-  if (vel_mask & 2) {
-    T v = (sv[id] * nmpre + s_mfv[threadIdx.y][threadIdx.x - 1] - s_mfv[threadIdx.y][threadIdx.x]) / nmpost;
-    dv[id] = v;
-    if (fold) fold_halo(dv, m, halo_rule(YVEL1), fold, i, j, v);
+  // velocity update over nodes [2, na+2] (:139-144 / :211-216): positions [2, NA+2)
+  for (int p = 2 + ta; p < NA + 2; p += TA) {
+    const int a = a0 - 2 + p;
+    if (!line_ok || a > na + 2) continue;
+    const long long id = at(a, line);
+    const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+    const T nmpre = s_nmpre[sidx(p, tl)], nmpost = s_nmpost[sidx(p, tl)];
+    if (vel_mask & 1) {
+      T v = (su[id] * nmpre + s_mfu[sidx(p - 1, tl)] - s_mfu[sidx(p, tl)]) / nmpost;
+      du[id] = v;
+      if (fold) fold_halo(du, m, halo_rule(XVEL1), fold, i, j, v);
+    }
+    if (vel_mask & 2) {
+      T v = (sv[id] * nmpre + s_mfv[sidx(p - 1, tl)] - s_mfv[sidx(p, tl)]) / nmpost;
+      dv[id] = v;
+      if (fold) fold_halo(dv, m, halo_rule(YVEL1), fold, i, j, v);
+    }
   }
 }
 
@@ -648,11 +676,6 @@ __global__ void k_copy_ring(const T *src, T *dst, Mesh<T> m, int ilo, int ihi, i
 // update_halo: src/serial/update_halo.cpp:33-684 in two launches: pass 0 does
 // bottom then top for every column, pass 1 left then right for every row, so
 // corner and tiny-mesh semantics are the reference's exactly.
-struct HaloJob {
-  int nfields;
-  int field[15];
-};
-
 template <typename T>
 __global__ void k_update_halo(Fields<T> F, Mesh<T> m, HaloJob job, int depth, int pass) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
