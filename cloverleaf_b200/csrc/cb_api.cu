@@ -17,6 +17,7 @@
 #include "../../include/cloverb200.h"
 #include "cb_chunk.h"
 #include "cb_ops.h"
+#include "cb_tma.cuh"
 
 struct cb_chunk : cb::Chunk {};
 
@@ -106,9 +107,7 @@ cudaError_t upload_geom(cb_chunk *c) {
 }
 
 void release(cb_chunk *c) {
-  for (auto &p : c->field_mem)
-    if (p) cudaFree(p), p = nullptr;
-  for (auto &p : c->spare_mem)
+  for (auto &p : c->buf)
     if (p) cudaFree(p), p = nullptr;
   for (int g = 0; g < NUM_GEOM; ++g) {
     if (c->geom_d[g]) cudaFree(c->geom_d[g]);
@@ -122,14 +121,61 @@ void release(cb_chunk *c) {
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_counter) cudaFree(c->d_counter);
   if (c->d_sums) cudaFree(c->d_sums);
+  if (c->d_err) cudaFree(c->d_err);
   if (c->h_scalars) cudaFreeHost(c->h_scalars);
   if (c->stream) cudaStreamDestroy(c->stream);
   c->d_dt_bits = nullptr;
   c->d_partials = nullptr;
   c->d_counter = nullptr;
   c->d_sums = nullptr;
+  c->d_err = nullptr;
   c->h_scalars = nullptr;
   c->stream = nullptr;
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
+                                 const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// One 2-D tensor map per buffer and staged box height: the whole allocation
+// as a (pitch x ny+6) array, boxes of BOX_X x h elements (cb_tma.cuh).
+bool encode_maps(cb_chunk *c) {
+  static EncodeTiled encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn) {
+      g_err = "cuTensorMapEncodeTiled is not available from the driver";
+      return false;
+    }
+    encode = (EncodeTiled)fn;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)c->pitch, (cuuint64_t)(c->ny + 6)};
+  const cuuint64_t strides[1] = {(cuuint64_t)(c->pitch * c->esize)};
+  const cuuint32_t estr[2] = {1, 1};
+  for (int b = 0; b < NUM_BUF; ++b)
+    for (int h = 0; h < NUM_BOX_H; ++h) {
+      const cuuint32_t box[2] = {(cuuint32_t)BOX_X, (cuuint32_t)BOX_HEIGHTS[h]};
+      CUresult r = encode(&c->tmap[b][h], c->precision == CB_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                          c->buf[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        g_err = "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r);
+        return false;
+      }
+    }
+  c->tmap_ok = true;
+  return true;
+}
+
+// A staging wait that gave up in some kernel leaves a flag on the device;
+// the host reports it at the next point that synchronises.
+int check_device_error(cb_chunk *c, const char *where) {
+  int err = 0;
+  cudaError_t e = cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, where);
+  if (err) return fail(CB_ECUDA, std::string(where) + ": a kernel's tile staging did not complete (TMA wait limit reached)");
+  return CB_OK;
 }
 
 } // namespace
@@ -179,10 +225,18 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
   c->precision = precision;
   c->device = device;
   c->esize = precision == CB_FP64 ? 8 : 4;
+  // Row layout: element (i, j) at allocation + off + j * pitch + i.  off puts
+  // the first interior column (i = 2) on a 256-byte boundary and makes the
+  // tiles' TMA boxes (starting at i = 2 + 64k - 4) 16-byte aligned; pitch
+  // covers off + nx + 5 so the tensor-map rows hold whole mesh rows.
   const long long align = 256 / (long long)c->esize;
   c->off = (size_t)(align - 2);
-  c->pitch = ((long long)nx + 5 + align - 1) / align * align;
-  c->alloc_elems = c->off + (size_t)c->pitch * (size_t)(ny + 5) + (size_t)align;
+  c->pitch = ((long long)c->off + nx + 5 + align - 1) / align * align;
+  c->alloc_elems = c->off + (size_t)c->pitch * (size_t)(ny + 6) + (size_t)align;
+  if (c->alloc_elems >= (size_t)1 << 31) {
+    delete c;
+    return fail(CB_EINVAL, "cb_create: mesh too large (a field must hold fewer than 2^31 elements)");
+  }
   const size_t bytes = c->alloc_elems * c->esize;
   auto bail = [&](cudaError_t err, const char *what) {
     release(c);
@@ -191,10 +245,15 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
     return cuda_fail(err, "cb_create");
   };
   if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
-  for (int f = 0; f < 15; ++f)
-    if ((e = cudaMalloc(&c->field_mem[f], bytes)) != cudaSuccess) return bail(e, "fields");
-  for (int s = 0; s < NUM_SPARE; ++s)
-    if ((e = cudaMalloc(&c->spare_mem[s], bytes)) != cudaSuccess) return bail(e, "spare buffers");
+  for (int b = 0; b < NUM_BUF; ++b)
+    if ((e = cudaMalloc(&c->buf[b], bytes)) != cudaSuccess) return bail(e, "fields");
+  for (int f = 0; f < 15; ++f) c->fbuf[f] = f;
+  for (int s = 0; s < NUM_SPARE; ++s) c->sbuf[s] = 15 + s;
+  if (!encode_maps(c)) {
+    release(c);
+    delete c;
+    return fail(CB_ECUDA, "cb_create: " + g_err);
+  }
   c->geom_len = std::max(nx, ny) + 6;
   for (int g = 0; g < NUM_GEOM; ++g) {
     c->geom_h[g] = new (std::nothrow) double[c->geom_len]();
@@ -206,19 +265,18 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
       c->geom_t[g] = c->geom_d[g];
     }
   }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  c->summary_grid = sms * 8;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  c->summary_grid = c->sms * 8;
   if ((e = cudaMalloc(&c->d_dt_bits, sizeof(unsigned long long))) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&c->d_partials, sizeof(double) * 5 * (size_t)c->summary_grid)) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&c->d_counter, sizeof(unsigned int))) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&c->d_sums, sizeof(double) * 5)) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream)) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMallocHost(&c->h_scalars, sizeof(double) * 8)) != cudaSuccess) return bail(e, "pinned scratch");
   if ((e = cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), c->stream)) != cudaSuccess) return bail(e, "scratch");
-  for (int f = 0; f < 15; ++f)
-    if ((e = cudaMemsetAsync(c->field_mem[f], 0, bytes, c->stream)) != cudaSuccess) return bail(e, "fields");
-  for (int s = 0; s < NUM_SPARE; ++s)
-    if ((e = cudaMemsetAsync(c->spare_mem[s], 0, bytes, c->stream)) != cudaSuccess) return bail(e, "spare buffers");
+  for (int b = 0; b < NUM_BUF; ++b)
+    if ((e = cudaMemsetAsync(c->buf[b], 0, bytes, c->stream)) != cudaSuccess) return bail(e, "fields");
   if ((e = upload_geom(c)) != cudaSuccess) return bail(e, "geometry");
   if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "setup");
   *out = c;
@@ -376,8 +434,7 @@ int cb_write_geom(cb_chunk *c, int geom, const double *host, size_t n) {
 int cb_build_field(cb_chunk *c) {
   CB_CHECK_CHUNK(c);
   const size_t bytes = c->alloc_elems * c->esize;
-  for (int f = 0; f < 15; ++f) CB_CUDA(cudaMemsetAsync(c->field_mem[f], 0, bytes, c->stream));
-  for (int s = 0; s < NUM_SPARE; ++s) CB_CUDA(cudaMemsetAsync(c->spare_mem[s], 0, bytes, c->stream));
+  for (int b = 0; b < NUM_BUF; ++b) CB_CUDA(cudaMemsetAsync(c->buf[b], 0, bytes, c->stream));
   for (int g = 0; g < NUM_GEOM; ++g) std::fill(c->geom_h[g], c->geom_h[g] + c->geom_len, 0.0);
   CB_CUDA(upload_geom(c));
   std::fill(std::begin(c->halo_fresh), std::end(c->halo_fresh), 0);
@@ -459,6 +516,7 @@ int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *cont
   CB_CUDA(dispatch(c, [&](auto ops) { return ops.calc_dt(*c, k); }));
   CB_CUDA(cudaMemcpyAsync(&c->h_scalars[1], c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CB_CUDA(cudaStreamSynchronize(c->stream));
+  if (int r = check_device_error(c, "cb_calc_dt")) return r;
   const double dt = c->h_scalars[1];
   *dt_min_val = dt;
   // src/serial/calc_dt.cpp:73-79: control is always "sound" (jk_control = 1.1)
@@ -528,8 +586,8 @@ int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth) 
   const int fold = effective_fold(c, halo_depth);
   void *dd = c->spare_base(0), *de = c->spare_base(1);
   CB_CUDA(dispatch(c, [&](auto ops) { return ops.advec_cell(*c, sweep_number, direction, fold, dd, de); }));
-  std::swap(c->field_mem[DENSITY1], c->spare_mem[0]);
-  std::swap(c->field_mem[ENERGY1], c->spare_mem[1]);
+  std::swap(c->fbuf[DENSITY1], c->sbuf[0]);
+  std::swap(c->fbuf[ENERGY1], c->sbuf[1]);
   c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = fold;
   c->halo_fresh[direction == 1 ? MASS_FLUX_X : MASS_FLUX_Y] = fold;
   return CB_OK;
@@ -545,11 +603,11 @@ int cb_advec_mom(cb_chunk *c, int which_vel, int sweep_number, int direction, in
   void *du = c->spare_base(2), *dv = c->spare_base(3);
   CB_CUDA(dispatch(c, [&](auto ops) { return ops.advec_mom(*c, which_vel, sweep_number, direction, fold, du, dv); }));
   if (which_vel & 1) {
-    std::swap(c->field_mem[XVEL1], c->spare_mem[2]);
+    std::swap(c->fbuf[XVEL1], c->sbuf[2]);
     c->halo_fresh[XVEL1] = fold;
   }
   if (which_vel & 2) {
-    std::swap(c->field_mem[YVEL1], c->spare_mem[3]);
+    std::swap(c->fbuf[YVEL1], c->sbuf[3]);
     c->halo_fresh[YVEL1] = fold;
   }
   return CB_OK;
@@ -585,6 +643,7 @@ int cb_field_summary(cb_chunk *c, double out[5]) {
   CB_CUDA(dispatch(c, [&](auto ops) { return ops.field_summary(*c); }));
   CB_CUDA(cudaMemcpyAsync(&c->h_scalars[2], c->d_sums, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream));
   CB_CUDA(cudaStreamSynchronize(c->stream));
+  if (int r = check_device_error(c, "cb_field_summary")) return r;
   for (int q = 0; q < 5; ++q) out[q] = c->h_scalars[2 + q];
   c->halo_fresh[PRESSURE] = 0;
   c->halo_fresh[SOUNDSPEED] = 0;
@@ -594,7 +653,7 @@ int cb_field_summary(cb_chunk *c, double out[5]) {
 int cb_synchronize(cb_chunk *c) {
   CB_CHECK_CHUNK(c);
   CB_CUDA(cudaStreamSynchronize(c->stream));
-  return CB_OK;
+  return check_device_error(c, "cb_synchronize");
 }
 
 int cb_get_stream(cb_chunk *c, void **stream) {

@@ -1,16 +1,21 @@
 // cb_chunk.h -- host-side state of one mesh chunk owned by the C-ABI library.
 #pragma once
 
+#include <cuda.h>
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
-#include <cuda_runtime.h>
 #include <string>
 
 #include "cb_mesh.cuh"
 
 namespace cb {
 
-constexpr int NUM_SPARE = 4; // second buffers for the double-buffered in-place phases
+constexpr int NUM_SPARE = 4;            // second buffers of the double-buffered phases
+constexpr int NUM_BUF = 15 + NUM_SPARE; // device buffers of the 15 state fields + spares
+constexpr int NUM_BOX_H = 2;            // staged box heights: 16 and 24 rows
+constexpr int BOX_HEIGHTS[NUM_BOX_H] = {16, 24};
 
 struct Chunk {
   int nx = 0, ny = 0;
@@ -22,8 +27,15 @@ struct Chunk {
   size_t alloc_elems = 0; // elements per allocation
   double gamma = 1.4;
 
-  void *field_mem[NUM_FIELDS] = {};  // allocation backing each field (nullptr = not allocated)
-  void *spare_mem[NUM_SPARE] = {};
+  // Buffers: buf[b] is a raw allocation; field f currently lives in buffer
+  // fbuf[f], spare s in sbuf[s].  Double-buffered phases swap indices.
+  void *buf[NUM_BUF] = {};
+  int fbuf[15] = {};
+  int sbuf[NUM_SPARE] = {};
+  // One TMA tensor map per buffer and staged box height (cb_tma.cuh).
+  CUtensorMap tmap[NUM_BUF][NUM_BOX_H];
+  bool tmap_ok = false;
+
   // geometry: FP64 on device for every precision, plus a copy in the storage type
   double *geom_d[NUM_GEOM] = {};
   void *geom_t[NUM_GEOM] = {};
@@ -35,8 +47,10 @@ struct Chunk {
   double *d_partials = nullptr;
   unsigned int *d_counter = nullptr;
   double *d_sums = nullptr;
-  double *h_scalars = nullptr; // pinned: [0] dt, [1..5] sums
+  int *d_err = nullptr;        // set by a kernel whose staging wait gave up
+  double *h_scalars = nullptr; // pinned: [0] dt init, [1] dt, [2..6] sums
   int summary_grid = 0;
+  int sms = 148;
 
   int halo_fresh[15] = {};     // depth to which each field's halo matches update_halo
   bool fold_enabled = true;    // fold halos into producers when the mesh allows it
@@ -45,8 +59,10 @@ struct Chunk {
   long long launches = 0; // kernels launched for this chunk
 
   bool can_fold() const { return fold_enabled && nx >= 8 && ny >= 8; }
-  void *base(int f) const { return field_mem[f] ? (char *)field_mem[f] + off * esize : nullptr; }
-  void *spare_base(int s) const { return (char *)spare_mem[s] + off * esize; }
+  void *base(int f) const { return (char *)buf[fbuf[f]] + off * esize; }
+  void *spare_base(int s) const { return (char *)buf[sbuf[s]] + off * esize; }
+  const CUtensorMap *map(int f, int box_h) const { return &tmap[fbuf[f]][box_h == 16 ? 0 : 1]; }
+  const CUtensorMap *spare_map(int s, int box_h) const { return &tmap[sbuf[s]][box_h == 16 ? 0 : 1]; }
 };
 
 } // namespace cb

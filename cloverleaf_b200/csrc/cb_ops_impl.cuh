@@ -4,9 +4,11 @@
 #pragma once
 
 #include <algorithm>
+#include <initializer_list>
 
 #include "cb_ops.h"
 #include "cb_phase.cuh"
+#include "cb_tile.cuh"
 
 namespace cb {
 
@@ -53,6 +55,19 @@ cudaError_t copy_ring(Chunk &c, const void *src, void *dst, int ilo, int ihi, in
   return launched(c);
 }
 
+// Tensor maps of the listed fields for staged boxes of height box_h.
+inline Maps maps_of(const Chunk &c, std::initializer_list<int> fields, int box_h) {
+  Maps mp;
+  int k = 0;
+  for (int f : fields) mp.m[k++] = *c.map(f, box_h);
+  return mp;
+}
+
+// Raises a kernel's dynamic shared-memory limit (a cheap host-side call).
+template <typename K> cudaError_t allow_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 } // namespace detail
 
 using namespace detail;
@@ -71,22 +86,37 @@ template <typename T> cudaError_t Ops<T>::ideal_gas(Chunk &c, int predict, int f
 }
 
 template <typename T> cudaError_t Ops<T>::viscosity(Chunk &c, int fold) {
-  dim3 b(32, 8);
-  k_viscosity<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), fold);
+  constexpr int TY = 16;
+  const size_t smem = 4 * Tile<TY>::BOX * sizeof(T);
+  cudaError_t e = allow_smem(kt_viscosity<T>, smem);
+  if (e != cudaSuccess) return e;
+  dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
+  kt_viscosity<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of(c, {PRESSURE, DENSITY0, XVEL0, YVEL0}, Tile<TY>::BH),
+                                                      (T *)c.base(VISCOSITY), mesh<T>(c), (int)c.off, fold, c.d_err);
   return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::calc_dt(Chunk &c, const DtConsts &k) {
-  dim3 b(32, 8);
-  const int tx = (c.nx + 31) / 32, ty = (c.ny + 7) / 8;
-  const int nt = tx * ty;
-  k_calc_dt<T><<<reduce_grid(c, nt), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), k, c.d_dt_bits, tx, nt);
+  constexpr int TY = 16;
+  const size_t smem = 5 * Tile<TY>::BOX * sizeof(T);
+  cudaError_t e = allow_smem(kt_calc_dt<T>, smem);
+  if (e != cudaSuccess) return e;
+  const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
+  const int grid = std::min(nt, c.sms * 3);
+  kt_calc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of(c, {SOUNDSPEED, VISCOSITY, DENSITY0, XVEL0, YVEL0}, Tile<TY>::BH),
+                                                       mesh<T>(c), (int)c.off, k, tx, nt, c.d_dt_bits, c.d_err);
   return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::pdv(Chunk &c, int predict, double dt, int mode, int fold) {
-  dim3 b(32, 8);
-  k_pdv<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), predict, (T)dt, mode, gm1<T>(c), fold);
+  constexpr int TY = 8;
+  const size_t smem = 8 * Tile<TY>::BOX * sizeof(T);
+  cudaError_t e = allow_smem(kt_pdv<T>, smem);
+  if (e != cudaSuccess) return e;
+  dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
+  PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
+  Maps mp = maps_of(c, {DENSITY0, ENERGY0, PRESSURE, VISCOSITY, XVEL0, YVEL0, XVEL1, YVEL1}, Tile<TY>::BH);
+  kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, predict, (T)dt, mode, gm1<T>(c), fold, c.d_err);
   return launched(c);
 }
 
@@ -97,14 +127,25 @@ template <typename T> cudaError_t Ops<T>::revert(Chunk &c) {
 }
 
 template <typename T> cudaError_t Ops<T>::accelerate(Chunk &c, double dt, int fold) {
-  dim3 b(32, 8);
-  k_accelerate<T><<<grid2(c.nx + 1, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), (T)dt, fold);
+  constexpr int TY = 16;
+  const size_t smem = 5 * Tile<TY>::BOX * sizeof(T);
+  cudaError_t e = allow_smem(kt_accelerate<T>, smem);
+  if (e != cudaSuccess) return e;
+  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
+  kt_accelerate<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of(c, {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0}, Tile<TY>::BH),
+                                                       (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, (T)dt, fold,
+                                                       c.d_err);
   return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fold) {
-  dim3 b(32, 8);
-  k_flux_calc<T><<<grid2(c.nx + 1, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), (T)dt, fold);
+  constexpr int TY = 16;
+  const size_t smem = 4 * Tile<TY>::BOX * sizeof(T);
+  cudaError_t e = allow_smem(kt_flux_calc<T>, smem);
+  if (e != cudaSuccess) return e;
+  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
+  kt_flux_calc<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of(c, {XVEL0, YVEL0, XVEL1, YVEL1}, Tile<TY>::BH), (T *)c.base(VOL_FLUX_X),
+                                                      (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off, (T)dt, fold, c.d_err);
   return launched(c);
 }
 
@@ -116,14 +157,19 @@ template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int di
     if ((e = copy_ring<T>(c, sd, dd, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
     if ((e = copy_ring<T>(c, se, de, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
   }
+  constexpr int TY = CellShared<1>::TY;
+  const int box_h = Tile<TY>::BH;
+  CellOut out{dd, de, c.base(dir == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
+  Maps mp = maps_of(c, {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y}, box_h);
+  dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
   if (dir == 1) {
-    using K = CellSweep<1>;
-    dim3 g((c.nx + K::NA - 1) / K::NA, (c.ny + K::NL - 1) / K::NL);
-    k_advec_cell<T, 1><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), sweep, sd, se, (T *)dd, (T *)de, fold);
+    const size_t smem = cell_smem_bytes<T, 1>();
+    if ((e = allow_smem(kt_advec_cell<T, 1>, smem)) != cudaSuccess) return e;
+    kt_advec_cell<T, 1><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, sweep, fold, c.d_err);
   } else {
-    using K = CellSweep<2>;
-    dim3 g((c.nx + K::NL - 1) / K::NL, (c.ny + K::NA - 1) / K::NA);
-    k_advec_cell<T, 2><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), sweep, sd, se, (T *)dd, (T *)de, fold);
+    const size_t smem = cell_smem_bytes<T, 2>();
+    if ((e = allow_smem(kt_advec_cell<T, 2>, smem)) != cudaSuccess) return e;
+    kt_advec_cell<T, 2><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, sweep, fold, c.d_err);
   }
   return launched(c);
 }
@@ -136,14 +182,22 @@ template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int 
     if ((vel_mask & 2) && (e = copy_ring<T>(c, sv, dv, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
   }
   // nodes [2, n+2] along both axes: n+1 of them
+  constexpr int TY = MomShared<1>::TY;
+  const int box_h = Tile<TY>::BH;
+  const int mom_sweep = dir + 2 * (sweep - 1);
+  MomOut out{du, dv};
+  Maps mp = mom_sweep == 1 ? maps_of(c, {DENSITY1, MASS_FLUX_X, XVEL1, YVEL1, VOL_FLUX_Y}, box_h)
+            : mom_sweep == 2 ? maps_of(c, {DENSITY1, MASS_FLUX_Y, XVEL1, YVEL1, VOL_FLUX_X}, box_h)
+                             : maps_of(c, {DENSITY1, dir == 1 ? MASS_FLUX_X : MASS_FLUX_Y, XVEL1, YVEL1}, box_h);
+  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
   if (dir == 1) {
-    using K = MomSweep<1>;
-    dim3 g((c.nx + 1 + K::NA - 1) / K::NA, (c.ny + 1 + K::NL - 1) / K::NL);
-    k_advec_mom<T, 1><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), vel_mask, sweep, su, sv, (T *)du, (T *)dv, fold);
+    const size_t smem = mom_smem_bytes<T, 1>();
+    if ((e = allow_smem(kt_advec_mom<T, 1>, smem)) != cudaSuccess) return e;
+    kt_advec_mom<T, 1><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, vel_mask, sweep, fold, c.d_err);
   } else {
-    using K = MomSweep<2>;
-    dim3 g((c.nx + 1 + K::NL - 1) / K::NL, (c.ny + 1 + K::NA - 1) / K::NA);
-    k_advec_mom<T, 2><<<g, dim3(K::TX, K::TY), 0, c.stream>>>(fields<T>(c), mesh<T>(c), vel_mask, sweep, su, sv, (T *)du, (T *)dv, fold);
+    const size_t smem = mom_smem_bytes<T, 2>();
+    if ((e = allow_smem(kt_advec_mom<T, 2>, smem)) != cudaSuccess) return e;
+    kt_advec_mom<T, 2><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, vel_mask, sweep, fold, c.d_err);
   }
   return launched(c);
 }

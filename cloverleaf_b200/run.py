@@ -1,0 +1,49 @@
+"""Run a clover.in deck (or the benchmark problem at any size) on a B200
+through the C ABI, in the reference driver's call order, and print the
+field summaries.
+
+  python -m cloverleaf_b200.run --deck clover.in
+  python -m cloverleaf_b200.run --bm 4608 --steps 2 [--precision fp32] [--no-fold]
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+
+from . import FP32, FP64, Chunk, HydroRun
+from .deck import benchmark_deck, nudged, read_deck
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    g = ap.add_mutually_exclusive_group(required=True)
+    g.add_argument("--deck", help="clover.in deck file")
+    g.add_argument("--bm", type=int, help="benchmark problem on an N x N mesh")
+    ap.add_argument("--steps", type=int, default=None, help="stop after this many steps (default: the deck's end)")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--no-fold", action="store_true", help="run every update_halo as its own pass")
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+
+    dk = read_deck(args.deck) if args.deck else nudged(benchmark_deck(args.bm, end_step=args.steps or 87))
+    c = Chunk(dk.x_cells, dk.y_cells, precision=FP32 if args.precision == "fp32" else FP64, device=args.device)
+    run = HydroRun(c, dk, fold=not args.no_fold)
+    t = time.time()
+    run.run(max_steps=args.steps)
+    c.synchronize()
+    wall = time.time() - t
+    for s in run.summaries:
+        print(f" step {s.step:6d} time {s.time:.6e} vol {s.vol:.15e} mass {s.mass:.15e} ie {s.ie:.15e} "
+              f"ke {s.ke:.15e} press {s.press:.15e}")
+    print(f" {run.step} steps of {dk.x_cells}x{dk.y_cells} in {wall:.3f} s "
+          f"({dk.x_cells * dk.y_cells * run.step / wall:.4e} cell-steps/s incl. setup); {c.launch_count()} kernel launches")
+    if dk.test_problem == 2 and run.step == 87:
+        qa = abs(100.0 * (run.summaries[-1].ke / 1.19316898756307) - 100.0)
+        print(f" Test problem 2 is within {qa}% of the expected solution: {'PASSED' if qa < 0.001 else 'NOT PASSED'}")
+    c.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
