@@ -92,7 +92,7 @@ __global__ void k_generate_chunk(Fields<T> F, Mesh<T> m, const DevState *st, int
 // reference's hard-coded gamma = 1.4).
 template <typename T>
 __device__ __forceinline__ void eos(T density, T energy, T gm1, T &pressure, T &soundspeed) {
-  T v = T(1.0) / density;
+  T v = (T(1.0)) / (density);
   pressure = gm1 * density * energy;
   T pressurebyenergy = gm1 * density;
   T pressurebyvolume = -density * pressure;

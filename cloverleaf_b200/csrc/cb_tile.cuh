@@ -62,13 +62,12 @@ __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, 
   T ugrad = (u10 + u11) - (u00 + u01);
   T vgrad = (v01 + v11) - (v00 + v10);
   T div = (cdx * (ugrad) + cdy * (vgrad));
-  T strain2 = T(0.5) * (u01 + u11 - u00 - u10) / cdy + T(0.5) * (v10 + v11 - v00 - v01) / cdx;
+  T strain2 = (T(0.5) * (u01 + u11 - u00 - u10)) / (cdy) + (T(0.5) * (v10 + v11 - v00 - v01)) / (cdx);
   T pgradx = (p_r - p_l) / (cdx + cdx1);
   T pgrady = (p_t - p_b) / (cdy + cdy2);
   T pgradx2 = pgradx * pgradx;
   T pgrady2 = pgrady * pgrady;
-  T limiter = ((T(0.5) * (ugrad) / cdx) * pgradx2 + (T(0.5) * (vgrad) / cdy) * pgrady2 + strain2 * pgradx * pgrady) /
-              fmax(pgradx2 + pgrady2, T(g_small));
+  T limiter = (((T(0.5) * (ugrad)) / (cdx)) * pgradx2 + ((T(0.5) * (vgrad)) / (cdy)) * pgrady2 + strain2 * pgradx * pgrady) / (fmax(pgradx2 + pgrady2, T(g_small)));
   if ((limiter > T(0.0)) || (div >= T(0.0))) return T(0.0);
   T dirx = T(1.0);
   if (pgradx < T(0.0)) dirx = T(-1.0);
@@ -77,8 +76,8 @@ __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, 
   if (pgradx < T(0.0)) diry = T(-1.0);
   pgrady = diry * fmax(T(g_small), fabs(pgrady));
   T pgrad = sqrt(pgradx * pgradx + pgrady * pgrady);
-  T xgrad = fabs(cdx * pgrad / pgradx);
-  T ygrad = fabs(cdy * pgrad / pgrady);
+  T xgrad = fabs((cdx * pgrad) / (pgradx));
+  T ygrad = fabs((cdy * pgrad) / (pgrady));
   T grad = fmin(xgrad, ygrad);
   T grad2 = grad * grad;
   return T(2.0) * density0 * grad2 * limiter * limiter;
@@ -124,22 +123,22 @@ __device__ __forceinline__ T dt_value(T ss, T q, T d0, T u00, T u10, T u01, T u1
   const T xa0 = dsy, xa1 = dsy;   // xarea(i, j), xarea(i+1, j) = celldy[j]
   const T ya0 = dsx, ya1 = dsx;   // yarea(i, j), yarea(i, j+1) = celldx[i]
   T cc = ss * ss;
-  cc = cc + T(2.0) * q / d0;
+  cc = cc + (T(2.0) * q) / (d0);
   cc = fmax(sqrt(cc), T(g_small));
-  T dtct = T(k.dtc_safe) * fmin(dsx, dsy) / cc;
+  T dtct = (T(k.dtc_safe) * fmin(dsx, dsy)) / (cc);
   T div = T(0.0);
   T dv1 = (u00 + u01) * xa0;
   T dv2 = (u10 + u11) * xa1;
   div = div + dv2 - dv1;
-  T dtut = T(k.dtu_safe) * T(2.0) * vol / fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol);
+  T dtut = (T(k.dtu_safe) * T(2.0) * vol) / (fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol));
   dv1 = (v00 + v10) * ya0;
   dv2 = (v01 + v11) * ya1;
   div = div + dv2 - dv1;
-  T dtvt = T(k.dtv_safe) * T(2.0) * vol / fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol);
-  div = div / (T(2.0) * vol);
+  T dtvt = (T(k.dtv_safe) * T(2.0) * vol) / (fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol));
+  div = (div) / (T(2.0) * vol);
   T dtdivt;
   if (div < T(-g_small)) {
-    dtdivt = T(k.dtdiv_safe) * (T(-1.0) / div);
+    dtdivt = T(k.dtdiv_safe) * ((T(-1.0)) / (div));
   } else {
     dtdivt = T(g_big);
   }
@@ -199,16 +198,16 @@ __device__ __forceinline__ void pdv_value(bool predict, T dt, T xa, T ya, T vol,
     top_flux = (ya_t * (v01 + v11 + z01 + z11)) * T(0.25) * dt;
   }
   T total_flux = right_flux - left_flux + top_flux - bottom_flux;
-  T volume_change_s = vol / (vol + total_flux);
-  T recip_volume = T(1.0) / vol;
-  T energy_change = (p / d0 + q / d0) * total_flux * recip_volume;
+  T volume_change_s = (vol) / (vol + total_flux);
+  T recip_volume = (T(1.0)) / (vol);
+  T energy_change = ((p) / (d0) + (q) / (d0)) * total_flux * recip_volume;
   energy1 = e0 - energy_change;
   density1 = d0 * volume_change_s;
 }
 
 template <typename T>
 __device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressure, T &soundspeed) {
-  T v = T(1.0) / density;
+  T v = (T(1.0)) / (density);
   pressure = gm1 * density * energy;
   T pressurebyenergy = gm1 * density;
   T pressurebyvolume = -density * pressure;
@@ -301,7 +300,7 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
     const T cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
     const T vol_mm = cdxm * cdym, vol_m0 = cdxm * cdy, vol_00 = cdx * cdy, vol_0m = cdx * cdym;
     const int c00 = b, cm0 = b - 1, c0m = b - BOX_X, cmm = b - BOX_X - 1;
-    T stepbymass_s = halfdt / ((D0[cmm] * vol_mm + D0[cm0] * vol_m0 + D0[c00] * vol_00 + D0[c0m] * vol_0m) * T(0.25));
+    T stepbymass_s = (halfdt) / (((D0[cmm] * vol_mm + D0[cm0] * vol_m0 + D0[c00] * vol_00 + D0[c0m] * vol_0m) * T(0.25)));
     const T xa = cdy, xa_m = cdym; // xarea(i, j), xarea(i, j-1)
     const T ya = cdx, ya_m = cdxm; // yarea(i, j), yarea(i-1, j)
     T u = U0[c00] - stepbymass_s * (xa * (P[c00] - P[cm0]) + xa_m * (P[c0m] - P[cmm]));
@@ -447,14 +446,14 @@ __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Map
       }
       const int bd = b + (donor - f) * step, bu = b + (upwind - f) * step, bw = b + (downwind - f) * step;
       const T pre_vol_d = DIR == 1 ? s_pv[fy * L::PV_W + (donor - (x0 - 2))] : s_pv[(donor - (y0 - 2)) * L::PV_W + fx];
-      T sigmat = fabs(flux) / pre_vol_d;
-      T sigma3 = (T(1.0) + sigmat) * (T)(vdx[f] / vdx[dif]);
+      T sigmat = (fabs(flux)) / (pre_vol_d);
+      T sigma3 = (T(1.0) + sigmat) * (T)((vdx[f]) / (vdx[dif]));
       T sigma4 = T(2.0) - sigmat;
       T sigmav = sigmat;
       const T dd = D1[bd], du = D1[bu], dw = D1[bw];
       T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
       T mass_flux = flux * (dd + limiter);
-      T sigmam = fabs(mass_flux) / (dd * pre_vol_d);
+      T sigmam = (fabs(mass_flux)) / ((dd * pre_vol_d));
       const T ed = E1[bd], eu = E1[bu], ew = E1[bw];
       limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
       s_mf[fy * L::F_W + fx] = (double)mass_flux;
@@ -485,9 +484,9 @@ __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Map
     const T vf_hi = DIR == 1 ? VFX[b + 1] : VFY[b + BOX_X];
     double pre_mass_s = (double)D1[b] * (double)pre_vol;
     double post_mass_s = pre_mass_s + mf_lo - mf_hi;
-    double post_ener_s = ((double)E1[b] * pre_mass_s + ef_lo - ef_hi) / post_mass_s;
+    double post_ener_s = ((double)E1[b] * pre_mass_s + ef_lo - ef_hi) / (post_mass_s);
     double advec_vol_s = (double)pre_vol + (double)vf_lo - (double)vf_hi;
-    const T dnew = (T)(post_mass_s / advec_vol_s);
+    const T dnew = (T)((post_mass_s) / (advec_vol_s));
     const T enew = (T)post_ener_s;
     const int g = gidx(pitch, i, j);
     ((T *)out.density1)[g] = dnew;
@@ -518,7 +517,7 @@ __device__ __forceinline__ T mom_limiter_value(T vdiffuw, T vdiffdw, T sigma, T 
     T adw = fabs(vdiffdw);
     T wind = T(1.0);
     if (vdiffdw <= T(0.0)) wind = T(-1.0);
-    limiter = wind * fmin(fmin(width * ((T(2.0) - sigma) * adw / width + (T(1.0) + sigma) * auw / dx_dif) / T(6.0), auw), adw);
+    limiter = wind * fmin(fmin((width * (((T(2.0) - sigma) * adw) / (width) + ((T(1.0) + sigma) * auw) / (dx_dif))) / (T(6.0)), auw), adw);
   }
   return limiter;
 }
@@ -618,7 +617,7 @@ __global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps
       } else {
         upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
       }
-      const T sigma = fabs(nf) / s_nmpre[sidx(p + (donor - a), l)];
+      const T sigma = (fabs(nf)) / (s_nmpre[sidx(p + (donor - a), l)]);
       const T width = celld[a];
       const int b = box_of(a, line);
       const int bd = b + (donor - a) * ST, bu = b + (upwind - a) * ST, bw = b + (downwind - a) * ST;
@@ -647,12 +646,12 @@ __global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps
       const T nmpre = s_nmpre[sidx(p, l)], nmpost = s_nmpost[sidx(p, l)];
       const int g = gidx(pitch, i, j);
       if (vel_mask & 1) {
-        T v = (U1[b] * nmpre + s_mfu[sidx(p - 1, l)] - s_mfu[sidx(p, l)]) / nmpost;
+        T v = (U1[b] * nmpre + s_mfu[sidx(p - 1, l)] - s_mfu[sidx(p, l)]) / (nmpost);
         ((T *)out.xvel1)[g] = v;
         if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
       }
       if (vel_mask & 2) {
-        T v = (V1[b] * nmpre + s_mfv[sidx(p - 1, l)] - s_mfv[sidx(p, l)]) / nmpost;
+        T v = (V1[b] * nmpre + s_mfv[sidx(p - 1, l)] - s_mfv[sidx(p, l)]) / (nmpost);
         ((T *)out.yvel1)[g] = v;
         if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
       }
