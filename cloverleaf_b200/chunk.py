@@ -31,7 +31,7 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk",
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
-           "cb_synchronize", "cb_get_stream", "cb_launch_count"]
+           "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_field_summary_noalloc"]
 
 
 class CloverError(RuntimeError):
@@ -82,6 +82,7 @@ def library() -> ctypes.CDLL:
         "cb_reset_field": ([P, i], i), "cb_update_halo": ([P, ip, i], i), "cb_field_summary": ([P, dp], i),
         "cb_synchronize": ([P], i), "cb_get_stream": ([P, ctypes.POINTER(P)], i),
         "cb_launch_count": ([P, ctypes.POINTER(ctypes.c_longlong)], i),
+        "cb_field_summary_noalloc": ([i, i, ctypes.c_longlong] + [P] * 8 + [d, P, P], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

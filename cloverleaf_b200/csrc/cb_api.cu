@@ -180,6 +180,10 @@ int check_device_error(cb_chunk *c, const char *where) {
 
 } // namespace
 
+namespace cb {
+int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+} // namespace cb
+
 extern "C" {
 
 int cb_version(void) { return 1; }

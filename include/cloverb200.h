@@ -143,6 +143,25 @@ int cb_get_stream(cb_chunk *c, void **stream);
 /* Number of kernels the library has launched for this chunk so far. */
 int cb_launch_count(const cb_chunk *c, long long *count);
 
+/* The field summary of cb_field_summary (ideal_gas, then the five sums) over
+ * FP64 device arrays the caller owns, allocating no memory: for callers that
+ * must not allocate device memory where they need the summary (their device
+ * memory comes from their own pool, or the call sits inside a loop that must
+ * stay allocation-free).  No counterpart in the reference.  Arrays are device
+ * pointers to element (0, 0) of each field, rows `pitch` elements apart, in
+ * the reference's index convention; celldx/celldy hold nx+4 / ny+4 widths.
+ * pressure and soundspeed receive the interior ideal-gas values; sums (device,
+ * 5 doubles) receives volume, mass, internal energy, kinetic energy and
+ * pressure*volume.  The work is enqueued on `stream` (a cudaStream_t; NULL for
+ * the default stream) and the call returns without waiting.  The reduction
+ * scratch is one fixed device array inside the library (meshes of at most
+ * 4,194,304 interior cells; larger ones are rejected), shared by all calls on
+ * a device: the first call on each device looks up its address, so make it
+ * before any stream capture, and do not let calls overlap on the GPU. */
+int cb_field_summary_noalloc(int nx, int ny, long long pitch, const double *density0, const double *energy0, const double *xvel0,
+                             const double *yvel0, const double *celldx, const double *celldy, double *pressure, double *soundspeed,
+                             double gamma, double *sums, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
