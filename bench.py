@@ -291,7 +291,7 @@ def main_reference(args, rank, world):
     if not os.path.exists(reference_exe()):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/omp was not built (needs the reference sources)"}))
         return
-    steps = min(args.steps, 50)
+    steps = min(args.steps, 20)
     warm = max(1, min(args.warmup, 3))
     per_cell = run_reference_omp(args.size, warm + steps, cores)
     timed = per_cell[warm:warm + steps]
