@@ -14,8 +14,15 @@ namespace cb {
 
 constexpr int NUM_SPARE = 4;            // second buffers of the double-buffered phases
 constexpr int NUM_BUF = 15 + NUM_SPARE; // device buffers of the 15 state fields + spares
-constexpr int NUM_BOX_H = 2;            // staged box heights: 16 and 24 rows
-constexpr int BOX_HEIGHTS[NUM_BOX_H] = {16, 24};
+constexpr int NUM_BOX_H = 6;            // staged box heights (rows) with a tensor map each
+constexpr int BOX_HEIGHTS[NUM_BOX_H] = {10, 12, 16, 18, 20, 24};
+
+// Slot of box height H in BOX_HEIGHTS; a height without a map does not compile.
+template <int H> constexpr int box_slot() {
+  constexpr int s = H == 10 ? 0 : H == 12 ? 1 : H == 16 ? 2 : H == 18 ? 3 : H == 20 ? 4 : H == 24 ? 5 : -1;
+  static_assert(s >= 0, "no tensor map for this box height");
+  return s;
+}
 
 struct Chunk {
   int nx = 0, ny = 0;
@@ -61,8 +68,7 @@ struct Chunk {
   bool can_fold() const { return fold_enabled && nx >= 8 && ny >= 8; }
   void *base(int f) const { return (char *)buf[fbuf[f]] + off * esize; }
   void *spare_base(int s) const { return (char *)buf[sbuf[s]] + off * esize; }
-  const CUtensorMap *map(int f, int box_h) const { return &tmap[fbuf[f]][box_h == 16 ? 0 : 1]; }
-  const CUtensorMap *spare_map(int s, int box_h) const { return &tmap[sbuf[s]][box_h == 16 ? 0 : 1]; }
+  template <int H> const CUtensorMap *map(int f) const { return &tmap[fbuf[f]][box_slot<H>()]; }
 };
 
 } // namespace cb

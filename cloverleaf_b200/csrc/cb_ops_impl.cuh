@@ -47,19 +47,22 @@ template <typename T> T gm1(const Chunk &c) { return (T)(c.gamma - 1.0); }
 inline int reduce_grid(const Chunk &c, int ntiles) { return std::min(ntiles, c.summary_grid); }
 
 // Copies the ring around the updated rectangle [ilo, ihi] x [jlo, jhi] from
-// src to dst (double-buffered phases whose halo is not folded).
+// src to dst for each of the n (1 or 2) pairs (double-buffered phases whose
+// halo is not folded).
 template <typename T>
-cudaError_t copy_ring(Chunk &c, const void *src, void *dst, int ilo, int ihi, int jlo, int jhi, int ex, int ey) {
-  const int n = ex * ey;
-  k_copy_ring<T><<<(n + 255) / 256, 256, 0, c.stream>>>((const T *)src, (T *)dst, mesh<T>(c), ilo, ihi, jlo, jhi, ex, ey);
+cudaError_t copy_ring(Chunk &c, const RingPair &rp, int n, int ilo, int ihi, int jlo, int jhi, int ex, int ey) {
+  if (n == 0) return cudaSuccess;
+  const long long ring = (long long)ex * ey - (long long)(ihi - ilo + 1) * (jhi - jlo + 1);
+  dim3 g((unsigned)((ring + 255) / 256), n);
+  k_copy_ring<T><<<g, 256, 0, c.stream>>>(rp, mesh<T>(c), ilo, ihi, jlo, jhi, ex, ey);
   return launched(c);
 }
 
-// Tensor maps of the listed fields for staged boxes of height box_h.
-inline Maps maps_of(const Chunk &c, std::initializer_list<int> fields, int box_h) {
+// Tensor maps of the listed fields for staged boxes of H rows.
+template <int H> Maps maps_of(const Chunk &c, std::initializer_list<int> fields) {
   Maps mp;
   int k = 0;
-  for (int f : fields) mp.m[k++] = *c.map(f, box_h);
+  for (int f : fields) mp.m[k++] = *c.map<H>(f);
   return mp;
 }
 
@@ -91,7 +94,7 @@ template <typename T> cudaError_t Ops<T>::viscosity(Chunk &c, int fold) {
   cudaError_t e = allow_smem(kt_viscosity<T>, smem);
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
-  kt_viscosity<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of(c, {PRESSURE, DENSITY0, XVEL0, YVEL0}, Tile<TY>::BH),
+  kt_viscosity<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {PRESSURE, DENSITY0, XVEL0, YVEL0}),
                                                       (T *)c.base(VISCOSITY), mesh<T>(c), (int)c.off, fold, c.d_err);
   return launched(c);
 }
@@ -103,7 +106,7 @@ template <typename T> cudaError_t Ops<T>::calc_dt(Chunk &c, const DtConsts &k) {
   if (e != cudaSuccess) return e;
   const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
   const int grid = std::min(nt, c.sms * 3);
-  kt_calc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of(c, {SOUNDSPEED, VISCOSITY, DENSITY0, XVEL0, YVEL0}, Tile<TY>::BH),
+  kt_calc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {SOUNDSPEED, VISCOSITY, DENSITY0, XVEL0, YVEL0}),
                                                        mesh<T>(c), (int)c.off, k, tx, nt, c.d_dt_bits, c.d_err);
   return launched(c);
 }
@@ -115,7 +118,7 @@ template <typename T> cudaError_t Ops<T>::pdv(Chunk &c, int predict, double dt, 
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
   PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
-  Maps mp = maps_of(c, {DENSITY0, ENERGY0, PRESSURE, VISCOSITY, XVEL0, YVEL0, XVEL1, YVEL1}, Tile<TY>::BH);
+  Maps mp = maps_of<Tile<TY>::BH>(c, {DENSITY0, ENERGY0, PRESSURE, VISCOSITY, XVEL0, YVEL0, XVEL1, YVEL1});
   kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, predict, (T)dt, mode, gm1<T>(c), fold, c.d_err);
   return launched(c);
 }
@@ -132,7 +135,7 @@ template <typename T> cudaError_t Ops<T>::accelerate(Chunk &c, double dt, int fo
   cudaError_t e = allow_smem(kt_accelerate<T>, smem);
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  kt_accelerate<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of(c, {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0}, Tile<TY>::BH),
+  kt_accelerate<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0}),
                                                        (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, (T)dt, fold,
                                                        c.d_err);
   return launched(c);
@@ -144,8 +147,26 @@ template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fol
   cudaError_t e = allow_smem(kt_flux_calc<T>, smem);
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  kt_flux_calc<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of(c, {XVEL0, YVEL0, XVEL1, YVEL1}, Tile<TY>::BH), (T *)c.base(VOL_FLUX_X),
+  kt_flux_calc<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1}), (T *)c.base(VOL_FLUX_X),
                                                       (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off, (T)dt, fold, c.d_err);
+  return launched(c);
+}
+
+#ifndef CB_CELL_TY_X
+#define CB_CELL_TY_X 8 // rows per x-sweep tile of advec_cell
+#endif
+#ifndef CB_CELL_TY_Y
+#define CB_CELL_TY_Y 8 // rows per y-sweep tile of advec_cell
+#endif
+
+template <typename T, int DIR, int TY> cudaError_t launch_advec_cell(Chunk &c, int sweep, int fold, void *dd, void *de) {
+  using L = CellLayout<T, DIR, TY>;
+  CellOut out{dd, de, c.base(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
+  Maps mp = maps_of<L::BH>(c, {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y});
+  cudaError_t e = allow_smem(kt_advec_cell<T, DIR, TY>, L::SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
+  kt_advec_cell<T, DIR, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, sweep, fold, c.d_err);
   return launched(c);
 }
 
@@ -154,23 +175,34 @@ template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int di
   const T *sd = (const T *)c.base(DENSITY1), *se = (const T *)c.base(ENERGY1);
   cudaError_t e;
   if (fold != 2) { // keep the halo ring exactly as the in-place reference leaves it
-    if ((e = copy_ring<T>(c, sd, dd, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
-    if ((e = copy_ring<T>(c, se, de, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
+    RingPair rp{{sd, se}, {dd, de}};
+    if ((e = copy_ring<T>(c, rp, 2, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
   }
-  constexpr int TY = CellShared<1>::TY;
-  const int box_h = Tile<TY>::BH;
-  CellOut out{dd, de, c.base(dir == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
-  Maps mp = maps_of(c, {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y}, box_h);
-  dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
-  if (dir == 1) {
-    const size_t smem = cell_smem_bytes<T, 1>();
-    if ((e = allow_smem(kt_advec_cell<T, 1>, smem)) != cudaSuccess) return e;
-    kt_advec_cell<T, 1><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, sweep, fold, c.d_err);
-  } else {
-    const size_t smem = cell_smem_bytes<T, 2>();
-    if ((e = allow_smem(kt_advec_cell<T, 2>, smem)) != cudaSuccess) return e;
-    kt_advec_cell<T, 2><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, sweep, fold, c.d_err);
-  }
+  return dir == 1 ? launch_advec_cell<T, 1, CB_CELL_TY_X>(c, sweep, fold, dd, de)
+                  : launch_advec_cell<T, 2, CB_CELL_TY_Y>(c, sweep, fold, dd, de);
+}
+
+#ifndef CB_MOM_TY_X
+#define CB_MOM_TY_X 8 // rows per x-sweep tile of advec_mom
+#endif
+#ifndef CB_MOM_TY_Y
+#define CB_MOM_TY_Y 8 // rows per y-sweep tile of advec_mom
+#endif
+
+template <typename T, int DIR, int TY>
+cudaError_t launch_advec_mom(Chunk &c, int vel_mask, int sweep, int fold, void *du, void *dv) {
+  using L = MomLayout<T, DIR, TY>;
+  const int mom_sweep = DIR + 2 * (sweep - 1);
+  const int mf = DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y;
+  Maps mp = mom_sweep == 1   ? maps_of<L::BH>(c, {XVEL1, YVEL1, DENSITY1, mf, VOL_FLUX_Y})
+            : mom_sweep == 2 ? maps_of<L::BH>(c, {XVEL1, YVEL1, DENSITY1, mf, VOL_FLUX_X})
+                             : maps_of<L::BH>(c, {XVEL1, YVEL1, DENSITY1, mf});
+  cudaError_t e = allow_smem(kt_advec_mom<T, DIR, TY>, L::SMEM);
+  if (e != cudaSuccess) return e;
+  // nodes [2, n+2] along both axes: n+1 of them
+  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
+  kt_advec_mom<T, DIR, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(mp, MomOut{du, dv}, mesh<T>(c), (int)c.off, vel_mask, sweep, fold,
+                                                                  c.d_err);
   return launched(c);
 }
 
@@ -178,28 +210,14 @@ template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int 
   const T *su = (const T *)c.base(XVEL1), *sv = (const T *)c.base(YVEL1);
   cudaError_t e;
   if (fold != 2) {
-    if ((vel_mask & 1) && (e = copy_ring<T>(c, su, du, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
-    if ((vel_mask & 2) && (e = copy_ring<T>(c, sv, dv, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
+    RingPair rp{};
+    int n = 0;
+    if (vel_mask & 1) rp.src[n] = su, rp.dst[n++] = du;
+    if (vel_mask & 2) rp.src[n] = sv, rp.dst[n++] = dv;
+    if ((e = copy_ring<T>(c, rp, n, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
   }
-  // nodes [2, n+2] along both axes: n+1 of them
-  constexpr int TY = MomShared<1>::TY;
-  const int box_h = Tile<TY>::BH;
-  const int mom_sweep = dir + 2 * (sweep - 1);
-  MomOut out{du, dv};
-  Maps mp = mom_sweep == 1 ? maps_of(c, {DENSITY1, MASS_FLUX_X, XVEL1, YVEL1, VOL_FLUX_Y}, box_h)
-            : mom_sweep == 2 ? maps_of(c, {DENSITY1, MASS_FLUX_Y, XVEL1, YVEL1, VOL_FLUX_X}, box_h)
-                             : maps_of(c, {DENSITY1, dir == 1 ? MASS_FLUX_X : MASS_FLUX_Y, XVEL1, YVEL1}, box_h);
-  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  if (dir == 1) {
-    const size_t smem = mom_smem_bytes<T, 1>();
-    if ((e = allow_smem(kt_advec_mom<T, 1>, smem)) != cudaSuccess) return e;
-    kt_advec_mom<T, 1><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, vel_mask, sweep, fold, c.d_err);
-  } else {
-    const size_t smem = mom_smem_bytes<T, 2>();
-    if ((e = allow_smem(kt_advec_mom<T, 2>, smem)) != cudaSuccess) return e;
-    kt_advec_mom<T, 2><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, vel_mask, sweep, fold, c.d_err);
-  }
-  return launched(c);
+  return dir == 1 ? launch_advec_mom<T, 1, CB_MOM_TY_X>(c, vel_mask, sweep, fold, du, dv)
+                  : launch_advec_mom<T, 2, CB_MOM_TY_Y>(c, vel_mask, sweep, fold, du, dv);
 }
 
 template <typename T> cudaError_t Ops<T>::reset_field(Chunk &c, int fold) {

@@ -179,13 +179,37 @@ __global__ void k_reset_field(Fields<T> F, Mesh<T> m, int fold) {
 // Copies the elements of `src` outside the rectangle [ilo, ihi] x [jlo, jhi]
 // (the ring of width 2 or 3 around it) into `dst`, so a double-buffered
 // update leaves dst's halo exactly as the in-place reference leaves it.
+// Threads enumerate the ring only: the rows below jlo, the rows above jhi,
+// then the left and right pieces of the rows in between.  blockIdx.y picks
+// one of up to two (src, dst) pairs.
+struct RingPair {
+  const void *src[2];
+  void *dst[2];
+};
+
 template <typename T>
-__global__ void k_copy_ring(const T *src, T *dst, Mesh<T> m, int ilo, int ihi, int jlo, int jhi, int ext_x, int ext_y) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_copy_ring(RingPair rp, Mesh<T> m, int ilo, int ihi, int jlo, int jhi, int ext_x, int ext_y) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int w = ext_x, h = ext_y;
-  if (t >= w * h) return;
-  const int i = t % w, j = t / w;
-  if (i >= ilo && i <= ihi && j >= jlo && j <= jhi) return;
+  const long long nb = (long long)jlo * w, nt = (long long)(h - 1 - jhi) * w;
+  const int side = ilo + (w - 1 - ihi); // ring elements per middle row
+  const long long nm = (long long)(jhi - jlo + 1) * side;
+  int i, j;
+  if (t < nb) {
+    i = (int)(t % w), j = (int)(t / w);
+  } else if (t < nb + nt) {
+    const long long u = t - nb;
+    i = (int)(u % w), j = jhi + 1 + (int)(u / w);
+  } else if (t < nb + nt + nm) {
+    const long long u = t - nb - nt;
+    const int c = (int)(u % side);
+    j = jlo + (int)(u / side);
+    i = c < ilo ? c : ihi + 1 + (c - ilo);
+  } else {
+    return;
+  }
+  const T *src = (const T *)rp.src[blockIdx.y];
+  T *dst = (T *)rp.dst[blockIdx.y];
   dst[m.at(i, j)] = src[m.at(i, j)];
 }
 

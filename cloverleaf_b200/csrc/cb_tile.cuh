@@ -365,8 +365,8 @@ __global__ void __launch_bounds__(256) kt_flux_calc(const __grid_constant__ Maps
 // ---------------------------------------------------------------------------
 // advec_cell: src/serial/advec_cell.cpp:28-220, one sweep in one pass.
 // pre_vol of the cells the faces need, then the face fluxes, then the
-// update, all through shared memory.  TY = 8.
-// fields: 0 density1, 1 energy1, 2 vol_flux_x, 3 vol_flux_y
+// update, all through shared memory; each stage spreads its items evenly
+// over the block's 256 threads.
 template <typename T>
 __device__ __forceinline__ T cell_limiter_value(T sigma, T sigma3, T sigma4, T diffuw, T diffdw) {
   const T one_by_six = T(1.0 / 6.0);
@@ -382,104 +382,118 @@ struct CellOut {
   void *density1, *energy1, *mass_flux;
 };
 
-// Shared layout of the cell sweep beyond the staged boxes.
-template <int DIR> struct CellShared {
-  static constexpr int TY = 8;
-  // pre_vol: DIR 1: rows TY x cells [x0-2, x0+66); DIR 2: rows [y0-2, y0+TY+2) x 64 columns
-  static constexpr int PV_W = DIR == 1 ? TILE_X + 4 : TILE_X, PV_H = DIR == 1 ? TY : TY + 4;
-  // fluxes: DIR 1: TY rows x 65 faces; DIR 2: TY+1 face rows x 64 columns
-  static constexpr int F_W = DIR == 1 ? TILE_X + 1 : TILE_X, F_H = DIR == 1 ? TY : TY + 1;
+// Tile of the cell sweep: LA cells along the sweep x LL lines across.
+// Staged boxes (BOX_X x BH, tensor rows from y0 - YH): density1, energy1,
+// vol_flux_x, vol_flux_y.  pre_vol covers cells -1 .. LA along the sweep
+// (the donors of the tile's faces), fluxes faces 0 .. LA.
+template <typename T, int DIR, int TY> struct CellLayout {
+  static constexpr int LA = DIR == 1 ? TILE_X : TY;
+  static constexpr int LL = DIR == 1 ? TY : TILE_X;
+  static constexpr int YH = DIR == 1 ? 1 : 2;
+  static constexpr int BH = DIR == 1 ? TY + 2 : TY + 4;
+  static constexpr int BOX = BOX_X * BH;
+  static constexpr int BOXS = (BOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+  static constexpr int NPV = LA + 2, NF = LA + 1;
+  static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + (size_t)2 * NF * LL * sizeof(double) + (size_t)NPV * LL * sizeof(T);
+  __device__ static constexpr int pv(int p, int l) { return DIR == 1 ? l * NPV + p : p * LL + l; } // p = cell + 1
+  __device__ static constexpr int fx(int p, int l) { return DIR == 1 ? l * NF + p : p * LL + l; }  // p = face
+  __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
+    if (DIR == 1) {
+      p = k % np, l = k / np;
+    } else {
+      l = k % nl, p = k / nl;
+    }
+  }
 };
 
-template <typename T, int DIR>
+template <typename T, int DIR, int TY>
 __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
                                                      int fold, int *err) {
-  using L = CellShared<DIR>;
-  constexpr int TY = L::TY;
-  using C = Tile<TY>;
+  using L = CellLayout<T, DIR, TY>;
+  constexpr int LA = L::LA, LL = L::LL, YH = L::YH;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   T *sm = reinterpret_cast<T *>(smraw);
-  double *s_mf = reinterpret_cast<double *>(smraw + 4 * C::BOX * sizeof(T));
-  double *s_ef = s_mf + L::F_W * L::F_H;
-  T *s_pv = reinterpret_cast<T *>(s_ef + L::F_W * L::F_H);
+  double *s_mf = reinterpret_cast<double *>(sm + 4 * L::BOXS);
+  double *s_ef = s_mf + L::NF * LL;
+  T *s_pv = reinterpret_cast<T *>(s_ef + L::NF * LL);
   const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
   const int nf = (sweep == 1) ? 4 : (DIR == 1 ? 3 : 4); // sweep 2 of x needs no y fluxes
-  if (!stage_tiles(sm, maps, nf, C::BOX, off, x0, y0, &bar, err)) return;
-  const T *D1 = sm, *E1 = sm + C::BOX, *VFX = sm + 2 * C::BOX, *VFY = sm + 3 * C::BOX;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int na = DIR == 1 ? m.nx : m.ny;
+  if (!stage_boxes(sm, maps, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH, &bar, err)) return;
+  const T *D1 = sm, *E1 = sm + L::BOXS, *VFX = sm + 2 * L::BOXS, *VFY = sm + 3 * L::BOXS;
+  const int tid = threadIdx.y * 64 + threadIdx.x;
+  const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
+  const int a0 = DIR == 1 ? x0 : y0, l0 = DIR == 1 ? y0 : x0;
   const int pitch = (int)m.pitch;
-  // (1) pre_vol (advec_cell.cpp:42-61 / :134-153) of the cells the sweep touches
-  for (int py = ty; py < L::PV_H; py += 4)
-    for (int px = tx; px < L::PV_W; px += 64) {
-      const int i = DIR == 1 ? x0 - 2 + px : x0 + px;
-      const int j = DIR == 1 ? y0 + py : y0 - 2 + py;
-      if (i > m.nx + 3 || j > m.ny + 3) continue;
-      const int b = (j - y0 + HALO) * BOX_X + (i - x0 + HALO);
-      const T vol = m.celldx_t[i] * m.celldy_t[j];
-      T pv;
-      if (DIR == 1) {
-        pv = sweep == 1 ? vol + (VFX[b + 1] - VFX[b] + VFY[b + BOX_X] - VFY[b]) : vol + VFX[b + 1] - VFX[b];
-      } else {
-        pv = sweep == 1 ? vol + (VFY[b + BOX_X] - VFY[b] + VFX[b + 1] - VFX[b]) : vol + VFY[b + BOX_X] - VFY[b];
-      }
-      s_pv[py * L::PV_W + px] = pv;
+  constexpr int ST = DIR == 1 ? 1 : BOX_X; // box stride along the sweep
+  auto bidx = [&](int i, int j) { return (j - y0 + YH) * BOX_X + (i - x0 + HALO); };
+  // (1) pre_vol (advec_cell.cpp:42-61 / :134-153) of cells a0-1 .. a0+LA
+  for (int t = tid; t < L::NPV * LL; t += 256) {
+    int p, l;
+    L::item(t, L::NPV, LL, p, l);
+    const int a = a0 - 1 + p, line = l0 + l;
+    const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+    if (i > m.nx + 3 || j > m.ny + 3) continue;
+    const int b = bidx(i, j);
+    const T vol = m.celldx_t[i] * m.celldy_t[j];
+    T pv;
+    if (DIR == 1) {
+      pv = sweep == 1 ? vol + (VFX[b + 1] - VFX[b] + VFY[b + BOX_X] - VFY[b]) : vol + VFX[b + 1] - VFX[b];
+    } else {
+      pv = sweep == 1 ? vol + (VFY[b + BOX_X] - VFY[b] + VFX[b + 1] - VFX[b]) : vol + VFY[b + BOX_X] - VFY[b];
     }
+    s_pv[L::pv(p, l)] = pv;
+  }
   __syncthreads();
-  // (2) face fluxes (:63-113 / :155-205), faces [x0, x0+64] or [y0, y0+TY]
+  // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
   const double *vdx = DIR == 1 ? m.vertexdx : m.vertexdy;
-  for (int fy = ty; fy < L::F_H; fy += 4)
-    for (int fx = tx; fx < L::F_W; fx += 64) {
-      const int i = x0 + fx, j = y0 + fy;         // face (i, j)
-      const int f = DIR == 1 ? i : j;             // position along the sweep
-      if (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3)) continue;
-      const int b = (j - y0 + HALO) * BOX_X + (i - x0 + HALO);
-      const int step = DIR == 1 ? 1 : BOX_X;      // box stride along the sweep
-      const T flux = DIR == 1 ? VFX[b] : VFY[b];
-      int upwind, donor, downwind, dif;
-      if (flux > T(0.0)) {
-        upwind = f - 2; donor = f - 1; downwind = f; dif = donor;
-      } else {
-        upwind = (f + 1 < na + 2) ? f + 1 : na + 2;
-        donor = f; downwind = f - 1; dif = upwind;
-      }
-      const int bd = b + (donor - f) * step, bu = b + (upwind - f) * step, bw = b + (downwind - f) * step;
-      const T pre_vol_d = DIR == 1 ? s_pv[fy * L::PV_W + (donor - (x0 - 2))] : s_pv[(donor - (y0 - 2)) * L::PV_W + fx];
-      T sigmat = (fabs(flux)) / (pre_vol_d);
-      T sigma3 = (T(1.0) + sigmat) * (T)((vdx[f]) / (vdx[dif]));
-      T sigma4 = T(2.0) - sigmat;
-      T sigmav = sigmat;
-      const T dd = D1[bd], du = D1[bu], dw = D1[bw];
-      T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
-      T mass_flux = flux * (dd + limiter);
-      T sigmam = (fabs(mass_flux)) / ((dd * pre_vol_d));
-      const T ed = E1[bd], eu = E1[bu], ew = E1[bw];
-      limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
-      s_mf[fy * L::F_W + fx] = (double)mass_flux;
-      s_ef[fy * L::F_W + fx] = (double)mass_flux * (double)(ed + limiter);
-      T *mf = (T *)out.mass_flux;
-      const bool halo_face = fold && f == na + 3; // with a fold, face na+3 takes its halo value
-      if (!halo_face) mf[gidx(pitch, i, j)] = mass_flux;
-      if (fold && f < na + 3 && edge_tile(m.nx, m.ny, x0, y0, TY))
-        fold_halo(mf, m, halo_rule(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y), fold, i, j, mass_flux);
+  const bool edge = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+  for (int t = tid; t < L::NF * LL; t += 256) {
+    int p, l;
+    L::item(t, L::NF, LL, p, l);
+    const int f = a0 + p, line = l0 + l; // position of the face along the sweep
+    const int i = DIR == 1 ? f : line, j = DIR == 1 ? line : f;
+    if (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3)) continue;
+    const int b = bidx(i, j);
+    const T flux = DIR == 1 ? VFX[b] : VFY[b];
+    int upwind, donor, downwind, dif;
+    if (flux > T(0.0)) {
+      upwind = f - 2; donor = f - 1; downwind = f; dif = donor;
+    } else {
+      upwind = (f + 1 < na + 2) ? f + 1 : na + 2;
+      donor = f; downwind = f - 1; dif = upwind;
     }
+    const int bd = b + (donor - f) * ST, bu = b + (upwind - f) * ST, bw = b + (downwind - f) * ST;
+    const T pre_vol_d = s_pv[L::pv(donor - a0 + 1, l)];
+    T sigmat = (fabs(flux)) / (pre_vol_d);
+    T sigma3 = (T(1.0) + sigmat) * (T)((vdx[f]) / (vdx[dif]));
+    T sigma4 = T(2.0) - sigmat;
+    T sigmav = sigmat;
+    const T dd = D1[bd], du = D1[bu], dw = D1[bw];
+    T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
+    T mass_flux = flux * (dd + limiter);
+    T sigmam = (fabs(mass_flux)) / ((dd * pre_vol_d));
+    const T ed = E1[bd], eu = E1[bu], ew = E1[bw];
+    limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
+    s_mf[L::fx(p, l)] = (double)mass_flux;
+    s_ef[L::fx(p, l)] = (double)mass_flux * (double)(ed + limiter);
+    T *mf = (T *)out.mass_flux;
+    const bool halo_face = fold && f == na + 3; // with a fold, face na+3 takes its halo value
+    if (!halo_face) mf[gidx(pitch, i, j)] = mass_flux;
+    if (edge && f < na + 3) fold_halo(mf, m, halo_rule(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y), fold, i, j, mass_flux);
+  }
   __syncthreads();
   // (3) the update (:117-129 / :209-221), mass/energy accumulation in FP64
-  const int i = x0 + tx;
-  if (i >= m.nx + 2) return;
-  const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
-#pragma unroll
-  for (int r = 0; r < C::RPT; ++r) {
-    const int j = y0 + ty + 4 * r, ly = HALO + ty + 4 * r;
-    if (j >= m.ny + 2) break;
-    const int b = ly * BOX_X + HALO + tx;
-    const int fy = ty + 4 * r;
-    const T pre_vol = DIR == 1 ? s_pv[fy * L::PV_W + tx + 2] : s_pv[(fy + 2) * L::PV_W + tx];
-    const double mf_lo = DIR == 1 ? s_mf[fy * L::F_W + tx] : s_mf[fy * L::F_W + tx];
-    const double mf_hi = DIR == 1 ? s_mf[fy * L::F_W + tx + 1] : s_mf[(fy + 1) * L::F_W + tx];
-    const double ef_lo = DIR == 1 ? s_ef[fy * L::F_W + tx] : s_ef[fy * L::F_W + tx];
-    const double ef_hi = DIR == 1 ? s_ef[fy * L::F_W + tx + 1] : s_ef[(fy + 1) * L::F_W + tx];
+  for (int t = tid; t < LA * LL; t += 256) {
+    int p, l;
+    L::item(t, LA, LL, p, l);
+    const int a = a0 + p, line = l0 + l;
+    const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+    if (i >= m.nx + 2 || j >= m.ny + 2) continue;
+    const int b = bidx(i, j);
+    const T pre_vol = s_pv[L::pv(p + 1, l)];
+    const double mf_lo = s_mf[L::fx(p, l)], mf_hi = s_mf[L::fx(p + 1, l)];
+    const double ef_lo = s_ef[L::fx(p, l)], ef_hi = s_ef[L::fx(p + 1, l)];
     const T vf_lo = DIR == 1 ? VFX[b] : VFY[b];
     const T vf_hi = DIR == 1 ? VFX[b + 1] : VFY[b + BOX_X];
     double pre_mass_s = (double)D1[b] * (double)pre_vol;
@@ -491,24 +505,32 @@ __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Map
     const int g = gidx(pitch, i, j);
     ((T *)out.density1)[g] = dnew;
     ((T *)out.energy1)[g] = enew;
-    if (do_fold) {
+    if (edge) {
       fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, dnew);
       fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, enew);
     }
   }
 }
 
-template <typename T, int DIR> constexpr size_t cell_smem_bytes() {
-  using L = CellShared<DIR>;
-  return 4 * Tile<L::TY>::BOX * sizeof(T) + 2 * L::F_W * L::F_H * sizeof(double) + L::PV_W * L::PV_H * sizeof(T);
-}
-
 // ---------------------------------------------------------------------------
 // advec_mom: src/serial/advec_mom.cpp:30-225, both velocities in one pass.
-// Positions p along the sweep map to nodes a = a0 - 2 + p (two extra nodes
-// on each side feed the fluxes of the updated ones).  TY = 8.
-// fields: 0 density1, 1 mass flux of the sweep, 2 xvel1, 3 yvel1, [4 the
-// other-direction volume flux, for post_vol of sweep 1]
+//
+// A block updates the nodes of a tile: LA nodes along the sweep (a) times LL
+// lines across it.  Positions p = 0 .. LA+2 along the sweep map to nodes
+// a = a0 - 2 + p; the stages cover only the positions the tile's outputs
+// need (node flux and cell mass p = 0..LA+2, node masses 1..LA+2, momentum
+// fluxes 1..LA+1, updates 2..LA+1), and every stage spreads its
+// (position, line) items evenly over the block's 256 threads.
+//
+// Cell masses density1 * post_vol are formed once per cell (the reference
+// forms each four times inside node_mass_post, :93-102 / :165-174, with the
+// same products and the same order of the sum, so the bits agree);
+// node_mass_post is re-formed from them where the update needs it.
+//
+// Staged boxes (BOX_X x BH, tensor rows from y0 - YH): xvel1, yvel1, then
+// density1, the sweep's mass flux and (sweep 1) the other direction's volume
+// flux.  The work arrays reuse the space of the last three once the first
+// stage has read them.
 template <typename T>
 __device__ __forceinline__ T mom_limiter_value(T vdiffuw, T vdiffdw, T sigma, T width, T dx_dif) {
   T limiter = T(0.0);
@@ -526,142 +548,190 @@ struct MomOut {
   void *xvel1, *yvel1;
 };
 
-template <int DIR> struct MomShared {
-  static constexpr int TY = 8;
-  // positions along the sweep x lines across
-  static constexpr int NP = DIR == 1 ? TILE_X + 4 : TY + 4; // node positions along the sweep
-  static constexpr int NL = DIR == 1 ? TY : TILE_X;         // lines
-  static constexpr int N = NP * NL;
+template <typename T, int DIR, int TY> struct MomLayout {
+  static constexpr int LA = DIR == 1 ? TILE_X : TY; // nodes along the sweep
+  static constexpr int LL = DIR == 1 ? TY : TILE_X; // lines across
+  static constexpr int YH = DIR == 1 ? 1 : 2;       // staged rows above the tile
+  static constexpr int BH = DIR == 1 ? TY + 2 : TY + 4;
+  static constexpr int BOX = BOX_X * BH;
+  static constexpr int BOXS = (BOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T); // 128-byte aligned stride
+  static constexpr int NP = LA + 3;                  // positions 0 .. LA+2
+  static constexpr int N_CM = NP * (LL + 1);         // cell masses: lines -1 .. LL-1
+  static constexpr int N_W = NP * LL;                // node arrays
+  static constexpr int SCRATCH = N_CM + 4 * N_W;    // cell masses, node flux, node_mass_pre, two momentum fluxes
+  static constexpr int REGION = SCRATCH > 3 * BOXS ? SCRATCH : 3 * BOXS;
+  static constexpr size_t SMEM = (size_t)(2 * BOXS + REGION) * sizeof(T);
+  // work-array indices: the thread-fastest coordinate is the contiguous one
+  __device__ static constexpr int cm(int p, int lc) { return DIR == 1 ? lc * NP + p : p * (LL + 1) + lc; }
+  __device__ static constexpr int w(int p, int l) { return DIR == 1 ? l * NP + p : p * LL + l; }
+  // the k-th item of an np x nl stage: (p, l) with the contiguous coordinate fastest
+  __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
+    if (DIR == 1) {
+      p = k % np, l = k / np;
+    } else {
+      l = k % nl, p = k / nl;
+    }
+  }
 };
 
-template <typename T, int DIR>
+template <typename T, int DIR, int TY>
 __global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps maps, MomOut out, Mesh<T> m, int off, int vel_mask,
                                                     int sweep, int fold, int *err) {
-  using L = MomShared<DIR>;
-  constexpr int TY = L::TY, NP = L::NP, NL = L::NL;
-  using C = Tile<TY>;
+  using L = MomLayout<T, DIR, TY>;
+  constexpr int LA = L::LA, LL = L::LL, NP = L::NP, YH = L::YH;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   T *sm = reinterpret_cast<T *>(smraw);
-  T *s_nf = sm + 5 * C::BOX, *s_nmpre = s_nf + L::N, *s_nmpost = s_nmpre + L::N, *s_mfu = s_nmpost + L::N, *s_mfv = s_mfu + L::N;
-  // shared index of (position p, line l): the fastest thread index walks the contiguous dimension
-  auto sidx = [](int p, int l) { return DIR == 1 ? l * NP + p : p * NL + l; };
   const int mom_sweep = DIR + 2 * (sweep - 1);
   const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
   const int nf = mom_sweep <= 2 ? 5 : 4;
-  if (!stage_tiles(sm, maps, nf, C::BOX, off, x0, y0, &bar, err)) return;
-  const T *D1 = sm, *MF = sm + C::BOX, *U1 = sm + 2 * C::BOX, *V1 = sm + 3 * C::BOX, *VFO = sm + 4 * C::BOX;
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  if (!stage_boxes(sm, maps, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH, &bar, err)) return;
+  const T *U1 = sm, *V1 = sm + L::BOXS, *D1 = sm + 2 * L::BOXS, *MF = sm + 3 * L::BOXS, *VFO = sm + 4 * L::BOXS;
+  T *region = sm + 2 * L::BOXS;
+  T *s_cm = region, *s_nf = s_cm + L::N_CM, *s_nmpre = s_nf + L::N_W, *s_mfu = s_nmpre + L::N_W, *s_mfv = s_mfu + L::N_W;
+  const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
-  const int a0 = DIR == 1 ? x0 : y0;
+  const int a0 = DIR == 1 ? x0 : y0, l0 = DIR == 1 ? y0 : x0;
   const int pitch = (int)m.pitch;
-  const int ST = DIR == 1 ? 1 : BOX_X; // box stride along the sweep
-  const int SL = DIR == 1 ? BOX_X : 1; // box stride across
-  // the thread's (position, line) walk: DIR 1 -> p along x (tx), l = rows (ty); DIR 2 -> p along y (ty), l = columns (tx)
-  const int p_start = DIR == 1 ? tx : ty, p_step = DIR == 1 ? 64 : 4;
-  const int l_start = DIR == 1 ? ty : tx, l_step = DIR == 1 ? 4 : 64;
-  auto box_of = [&](int a, int line) { // box index of node (a along the sweep, line across)
-    return DIR == 1 ? (line - y0 + HALO) * BOX_X + (a - x0 + HALO) : (a - y0 + HALO) * BOX_X + (line - x0 + HALO);
-  };
-  // post_vol of cell c = box index b (:42-77): mom_sweep 1 vol + vfy diff, 2 vol + vfx diff, 3/4 vol
-  auto post_vol = [&](int b, int ci, int cj) -> T {
-    const T vol = m.celldx_t[ci] * m.celldy_t[cj];
-    if (mom_sweep == 1) return vol + VFO[b + BOX_X] - VFO[b];
-    if (mom_sweep == 2) return vol + VFO[b + 1] - VFO[b];
-    return vol;
-  };
-  // (1) node_flux over nodes [0, na+3] (:84-88 / :156-160)
-  for (int l = l_start; l < NL; l += l_step) {
-    const int line = (DIR == 1 ? y0 : x0) + l;
-    for (int p = p_start; p < NP; p += p_step) {
-      const int a = a0 - 2 + p;
-      T nf = T(0.0);
-      if (line < nlmax + 3 && a >= 0 && a <= na + 3) {
-        const int b = box_of(a, line);
-        // dir 1: mf(a, j-1) + mf(a, j) + mf(a+1, j-1) + mf(a+1, j); dir 2: mf(i-1, a) + mf(i, a) + mf(i-1, a+1) + mf(i, a+1)
-        nf = T(0.25) * (MF[b - SL] + MF[b] + MF[b + ST - SL] + MF[b + ST]);
-      }
-      s_nf[sidx(p, l)] = nf;
-    }
-  }
-  __syncthreads();
-  // (2) node_mass_post / node_mass_pre over nodes [1, na+3] (:93-102 / :165-174)
-  for (int l = l_start; l < NL; l += l_step) {
-    const int line = (DIR == 1 ? y0 : x0) + l;
-    for (int p = p_start; p < NP; p += p_step) {
-      const int a = a0 - 2 + p;
-      T nmpost = T(1.0), nmpre = T(1.0);
-      if (line < nlmax + 3 && p >= 1 && a >= 1 && a <= na + 3) {
-        const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-        const int b = box_of(a, line); // node (i, j) = cell (i, j) in the box
-        nmpost = T(0.25) * (D1[b - BOX_X] * post_vol(b - BOX_X, i, j - 1) + D1[b] * post_vol(b, i, j) +
-                            D1[b - BOX_X - 1] * post_vol(b - BOX_X - 1, i - 1, j - 1) + D1[b - 1] * post_vol(b - 1, i - 1, j));
-        nmpre = nmpost - s_nf[sidx(p - 1, l)] + s_nf[sidx(p, l)];
-      }
-      s_nmpost[sidx(p, l)] = nmpost;
-      s_nmpre[sidx(p, l)] = nmpre;
-    }
-  }
-  __syncthreads();
-  // (3) mom_flux over nodes [1, na+2] (:108-133 / :180-205): positions [1, NP-2]
-  const T *celld = DIR == 1 ? m.celldx_t : m.celldy_t;
-  for (int l = l_start; l < NL; l += l_step) {
-    const int line = (DIR == 1 ? y0 : x0) + l;
-    for (int p = p_start; p < NP; p += p_step) {
-      const int a = a0 - 2 + p;
-      if (p < 1 || p > NP - 2 || line >= nlmax + 3 || a < 1 || a > na + 2) continue;
-      const T nf = s_nf[sidx(p, l)];
-      int upwind, donor, downwind, dif;
-      if (nf < T(0.0)) {
-        upwind = a + 2; donor = a + 1; downwind = a; dif = donor;
-      } else {
-        upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
-      }
-      const T sigma = (fabs(nf)) / (s_nmpre[sidx(p + (donor - a), l)]);
-      const T width = celld[a];
-      const int b = box_of(a, line);
-      const int bd = b + (donor - a) * ST, bu = b + (upwind - a) * ST, bw = b + (downwind - a) * ST;
-      if (vel_mask & 1) {
-        const T vd = U1[bd];
-        T lim = mom_limiter_value(vd - U1[bu], U1[bw] - vd, sigma, width, celld[dif]);
-        s_mfu[sidx(p, l)] = (vd + (T(1.0) - sigma) * lim) * nf;
-      }
-      if (vel_mask & 2) {
-        const T vd = V1[bd];
-        T lim = mom_limiter_value(vd - V1[bu], V1[bw] - vd, sigma, width, celld[dif]);
-        s_mfv[sidx(p, l)] = (vd + (T(1.0) - sigma) * lim) * nf;
-      }
-    }
-  }
-  __syncthreads();
-  // (4) velocity update over nodes [2, na+2] (:139-144 / :211-216): positions [2, NP-2)
-  const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
-  for (int l = l_start; l < NL; l += l_step) {
-    const int line = (DIR == 1 ? y0 : x0) + l;
-    for (int p = p_start; p < NP; p += p_step) {
-      const int a = a0 - 2 + p;
-      if (p < 2 || p >= NP - 2 || line >= nlmax + 3 || a > na + 2) continue;
-      const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-      const int b = box_of(a, line);
-      const T nmpre = s_nmpre[sidx(p, l)], nmpost = s_nmpost[sidx(p, l)];
-      const int g = gidx(pitch, i, j);
-      if (vel_mask & 1) {
-        T v = (U1[b] * nmpre + s_mfu[sidx(p - 1, l)] - s_mfu[sidx(p, l)]) / (nmpost);
-        ((T *)out.xvel1)[g] = v;
-        if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
-      }
-      if (vel_mask & 2) {
-        T v = (V1[b] * nmpre + s_mfv[sidx(p - 1, l)] - s_mfv[sidx(p, l)]) / (nmpost);
-        ((T *)out.yvel1)[g] = v;
-        if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
-      }
-    }
-  }
-}
+  constexpr int ST = DIR == 1 ? 1 : BOX_X; // box stride along the sweep
+  constexpr int SL = DIR == 1 ? BOX_X : 1; // box stride across
+  // box index of element (i, j)
+  auto bidx = [&](int i, int j) { return (j - y0 + YH) * BOX_X + (i - x0 + HALO); };
 
-template <typename T, int DIR> constexpr size_t mom_smem_bytes() {
-  using L = MomShared<DIR>;
-  return (5 * Tile<L::TY>::BOX + 5 * L::N) * sizeof(T);
+  // (1) cell masses and node fluxes into registers, then into the region
+  constexpr int K_CM = (L::N_CM + 255) / 256, K_NF = (L::N_W + 255) / 256;
+  T r_cm[K_CM], r_nf[K_NF];
+#pragma unroll
+  for (int k = 0; k < K_CM; ++k) {
+    const int t = tid + 256 * k;
+    T v = T(0.0);
+    if (t < L::N_CM) {
+      int p, lc;
+      L::item(t, NP, LL + 1, p, lc);
+      const int a = a0 - 2 + p, line = l0 - 1 + lc;
+      if (a >= 0 && a <= na + 3 && line >= 0 && line <= nlmax + 3) {
+        const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+        const int b = bidx(i, j);
+        const T vol = m.celldx_t[i] * m.celldy_t[j];
+        // post_vol (:42-77): mom_sweep 1 vol + vfy difference, 2 vol + vfx difference, 3/4 vol
+        const T pv = mom_sweep == 1 ? vol + VFO[b + BOX_X] - VFO[b] : mom_sweep == 2 ? vol + VFO[b + 1] - VFO[b] : vol;
+        v = D1[b] * pv;
+      }
+    }
+    r_cm[k] = v;
+  }
+#pragma unroll
+  for (int k = 0; k < K_NF; ++k) {
+    const int t = tid + 256 * k;
+    T v = T(0.0);
+    if (t < L::N_W) {
+      int p, l;
+      L::item(t, NP, LL, p, l);
+      const int a = a0 - 2 + p, line = l0 + l;
+      if (line < nlmax + 3 && a >= 0 && a <= na + 3) {
+        const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
+        // (:84-88 / :156-160) dir 1: mf(a, j-1) + mf(a, j) + mf(a+1, j-1) + mf(a+1, j); dir 2: mf(i-1, a) + mf(i, a) + mf(i-1, a+1) + mf(i, a+1)
+        v = T(0.25) * (MF[b - SL] + MF[b] + MF[b + ST - SL] + MF[b + ST]);
+      }
+    }
+    r_nf[k] = v;
+  }
+  __syncthreads(); // density1, mass flux and volume flux boxes are dead from here on
+#pragma unroll
+  for (int k = 0; k < K_CM; ++k) {
+    const int t = tid + 256 * k;
+    if (t < L::N_CM) {
+      int p, lc;
+      L::item(t, NP, LL + 1, p, lc);
+      s_cm[L::cm(p, lc)] = r_cm[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K_NF; ++k) {
+    const int t = tid + 256 * k;
+    if (t < L::N_W) {
+      int p, l;
+      L::item(t, NP, LL, p, l);
+      s_nf[L::w(p, l)] = r_nf[k];
+    }
+  }
+  __syncthreads();
+
+  // node_mass_post (:93-96 / :165-168) of node (p, l): cells (i, j-1), (i, j), (i-1, j-1), (i-1, j)
+  auto node_mass_post = [&](int p, int l) -> T {
+    if (DIR == 1)
+      return T(0.25) * (s_cm[L::cm(p, l)] + s_cm[L::cm(p, l + 1)] + s_cm[L::cm(p - 1, l)] + s_cm[L::cm(p - 1, l + 1)]);
+    return T(0.25) * (s_cm[L::cm(p - 1, l + 1)] + s_cm[L::cm(p, l + 1)] + s_cm[L::cm(p - 1, l)] + s_cm[L::cm(p, l)]);
+  };
+
+  // (2) node_mass_pre (:97-102 / :169-174) over positions 1 .. LA+2
+  for (int t = tid; t < (NP - 1) * LL; t += 256) {
+    int p, l;
+    L::item(t, NP - 1, LL, p, l);
+    p += 1;
+    const int a = a0 - 2 + p, line = l0 + l;
+    T nmpre = T(1.0);
+    if (line < nlmax + 3 && a >= 1 && a <= na + 3) nmpre = node_mass_post(p, l) - s_nf[L::w(p - 1, l)] + s_nf[L::w(p, l)];
+    s_nmpre[L::w(p, l)] = nmpre;
+  }
+  __syncthreads();
+
+  // (3) mom_flux (:108-133 / :180-205) over positions 1 .. LA+1
+  const T *celld = DIR == 1 ? m.celldx_t : m.celldy_t;
+  for (int t = tid; t < (LA + 1) * LL; t += 256) {
+    int p, l;
+    L::item(t, LA + 1, LL, p, l);
+    p += 1;
+    const int a = a0 - 2 + p, line = l0 + l;
+    if (line >= nlmax + 3 || a < 1 || a > na + 2) continue;
+    const T nfv = s_nf[L::w(p, l)];
+    int upwind, donor, downwind, dif;
+    if (nfv < T(0.0)) {
+      upwind = a + 2; donor = a + 1; downwind = a; dif = donor;
+    } else {
+      upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
+    }
+    const T sigma = (fabs(nfv)) / (s_nmpre[L::w(p + (donor - a), l)]);
+    const T width = celld[a];
+    const T dxd = celld[dif];
+    const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
+    const int bd = b + (donor - a) * ST, bu = b + (upwind - a) * ST, bw = b + (downwind - a) * ST;
+    if (vel_mask & 1) {
+      const T vd = U1[bd];
+      T lim = mom_limiter_value(vd - U1[bu], U1[bw] - vd, sigma, width, dxd);
+      s_mfu[L::w(p, l)] = (vd + (T(1.0) - sigma) * lim) * nfv;
+    }
+    if (vel_mask & 2) {
+      const T vd = V1[bd];
+      T lim = mom_limiter_value(vd - V1[bu], V1[bw] - vd, sigma, width, dxd);
+      s_mfv[L::w(p, l)] = (vd + (T(1.0) - sigma) * lim) * nfv;
+    }
+  }
+  __syncthreads();
+
+  // (4) velocity update (:139-144 / :211-216) over positions 2 .. LA+1
+  const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+  for (int t = tid; t < LA * LL; t += 256) {
+    int p, l;
+    L::item(t, LA, LL, p, l);
+    p += 2;
+    const int a = a0 - 2 + p, line = l0 + l;
+    if (line > nlmax + 2 || a > na + 2) continue;
+    const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+    const int b = bidx(i, j);
+    const T nmpre = s_nmpre[L::w(p, l)], nmpost = node_mass_post(p, l);
+    const int g = gidx(pitch, i, j);
+    if (vel_mask & 1) {
+      T v = (U1[b] * nmpre + s_mfu[L::w(p - 1, l)] - s_mfu[L::w(p, l)]) / (nmpost);
+      ((T *)out.xvel1)[g] = v;
+      if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
+    }
+    if (vel_mask & 2) {
+      T v = (V1[b] * nmpre + s_mfv[L::w(p - 1, l)] - s_mfv[L::w(p, l)]) / (nmpost);
+      ((T *)out.yvel1)[g] = v;
+      if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
+    }
+  }
 }
 
 } // namespace cb

@@ -85,4 +85,22 @@ __device__ __forceinline__ bool stage_tiles(T *sm, const Maps &maps, int nf, int
   return __syncthreads_and(ok) != 0;
 }
 
+// Like stage_tiles, for boxes of BOX_X x bh elements whose first element is
+// tensor coordinate (xs, ys), placed `stride` elements apart in shared
+// memory (stride * sizeof(T) a multiple of 128 bytes).
+template <typename T>
+__device__ __forceinline__ bool stage_boxes(T *sm, const Maps &maps, int nf, int stride, int bh, int xs, int ys, uint64_t *bar,
+                                            int *err) {
+  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+  if (leader) mbar_init(bar, 1);
+  __syncthreads();
+  if (leader) {
+    mbar_expect_tx(bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
+    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, &maps.m[f], xs, ys, bar);
+  }
+  bool ok = mbar_wait(bar, 0, err);
+  if (!ok) mbar_wait(bar, 0, nullptr);
+  return __syncthreads_and(ok) != 0;
+}
+
 } // namespace cb
