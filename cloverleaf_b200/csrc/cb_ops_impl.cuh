@@ -90,36 +90,43 @@ template <typename T> cudaError_t Ops<T>::ideal_gas(Chunk &c, int predict, int f
 
 template <typename T> cudaError_t Ops<T>::viscosity(Chunk &c, int fold) {
   constexpr int TY = 16;
-  const size_t smem = 4 * Tile<TY>::BOX * sizeof(T);
+  using B = Box1<T, TY>;
+  const size_t smem = 3 * B::BOXS * sizeof(T);
   cudaError_t e = allow_smem(kt_viscosity<T>, smem);
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
-  kt_viscosity<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {PRESSURE, DENSITY0, XVEL0, YVEL0}),
+  kt_viscosity<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {PRESSURE, XVEL0, YVEL0}), (const T *)c.base(DENSITY0),
                                                       (T *)c.base(VISCOSITY), mesh<T>(c), (int)c.off, fold, c.d_err);
   return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::calc_dt(Chunk &c, const DtConsts &k) {
   constexpr int TY = 16;
-  const size_t smem = 5 * Tile<TY>::BOX * sizeof(T);
+  using B = Box1<T, TY>;
+  const size_t smem = 2 * B::BOXS * sizeof(T);
   cudaError_t e = allow_smem(kt_calc_dt<T>, smem);
   if (e != cudaSuccess) return e;
   const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
-  const int grid = std::min(nt, c.sms * 3);
-  kt_calc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {SOUNDSPEED, VISCOSITY, DENSITY0, XVEL0, YVEL0}),
-                                                       mesh<T>(c), (int)c.off, k, tx, nt, c.d_dt_bits, c.d_err);
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt_calc_dt<T>, 256, smem)) != cudaSuccess) return e;
+  const int grid = std::min(nt, c.sms * std::max(per_sm, 1));
+  DtIn in{c.base(SOUNDSPEED), c.base(VISCOSITY), c.base(DENSITY0)};
+  kt_calc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {XVEL0, YVEL0}), in, mesh<T>(c), (int)c.off, k, tx, nt,
+                                                       c.d_dt_bits, c.d_err);
   return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::pdv(Chunk &c, int predict, double dt, int mode, int fold) {
   constexpr int TY = 8;
-  const size_t smem = 8 * Tile<TY>::BOX * sizeof(T);
-  cudaError_t e = allow_smem(kt_pdv<T>, smem);
+  using B = Box1<T, TY>;
+  const size_t smem = (predict ? 2 : 4) * B::BOXS * sizeof(T);
+  cudaError_t e = allow_smem(kt_pdv<T>, 4 * B::BOXS * sizeof(T));
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
+  PdvIn in{c.base(DENSITY0), c.base(ENERGY0), c.base(PRESSURE), c.base(VISCOSITY)};
   PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
-  Maps mp = maps_of<Tile<TY>::BH>(c, {DENSITY0, ENERGY0, PRESSURE, VISCOSITY, XVEL0, YVEL0, XVEL1, YVEL1});
-  kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, predict, (T)dt, mode, gm1<T>(c), fold, c.d_err);
+  Maps mp = maps_of<B::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1});
+  kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, mesh<T>(c), (int)c.off, predict, (T)dt, mode, gm1<T>(c), fold, c.d_err);
   return launched(c);
 }
 

@@ -37,17 +37,26 @@ __device__ __forceinline__ bool edge_tile(int nx, int ny, int x0, int y0, int ty
   return x0 < 12 || x0 + TILE_X > nx - 8 || y0 < 12 || y0 + ty > ny - 8;
 }
 
+// Staged boxes whose first row is y0 - 1: BH = rows + 2 (a one-row halo
+// above and below the tile), stride rounded to 128 bytes.
+template <typename T, int TY> struct Box1 {
+  static constexpr int BH = TY + 2;
+  static constexpr int BOXS = (BOX_X * BH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+  // box index of element (i, j) of the tile at (x0, y0)
+  __device__ static constexpr int at(int i, int j, int x0, int y0) { return (j - y0 + 1) * BOX_X + (i - x0 + HALO); }
+};
+
 // Re-armable staging for blocks that loop over several tiles: the barrier
 // is initialised once (init) and completes one phase per tile.
 template <typename T>
-__device__ __forceinline__ bool stage_loop(T *sm, const Maps &maps, int nf, int box_elems, int off, int x0, int y0, uint64_t *bar,
-                                           unsigned phase, bool init, int *err) {
+__device__ __forceinline__ bool stage_boxes_loop(T *sm, const Maps &maps, int nf, int stride, int bh, int xs, int ys, uint64_t *bar,
+                                                 unsigned phase, bool init, int *err) {
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
   if (init && leader) mbar_init(bar, 1);
   __syncthreads(); // the previous tile's readers are done with the boxes
   if (leader) {
-    mbar_expect_tx(bar, (unsigned)(nf * box_elems * sizeof(T)));
-    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * box_elems, &maps.m[f], off + x0 - HALO, y0 - HALO, bar);
+    mbar_expect_tx(bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
+    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, &maps.m[f], xs, ys, bar);
   }
   bool ok = mbar_wait(bar, phase, err);
   if (!ok) mbar_wait(bar, phase, nullptr);
@@ -55,20 +64,23 @@ __device__ __forceinline__ bool stage_loop(T *sm, const Maps &maps, int nf, int 
 }
 
 // ---------------------------------------------------------------------------
-// viscosity: src/serial/viscosity.cpp:30-68 (diry quirk at :57 kept).
+// viscosity: src/serial/viscosity.cpp:30-68 (diry quirk at :57 kept).  The
+// result is 0 whenever div >= 0 (:50), so the divisions are only evaluated
+// where the cell is compressed; the value is the same either way.
 template <typename T>
 __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, T v10, T v01, T v11, T p_l, T p_r, T p_b, T p_t,
                                              T density0, T cdx, T cdx1, T cdy, T cdy2) {
   T ugrad = (u10 + u11) - (u00 + u01);
   T vgrad = (v01 + v11) - (v00 + v10);
   T div = (cdx * (ugrad) + cdy * (vgrad));
+  if (div >= T(0.0)) return T(0.0);
   T strain2 = (T(0.5) * (u01 + u11 - u00 - u10)) / (cdy) + (T(0.5) * (v10 + v11 - v00 - v01)) / (cdx);
   T pgradx = (p_r - p_l) / (cdx + cdx1);
   T pgrady = (p_t - p_b) / (cdy + cdy2);
   T pgradx2 = pgradx * pgradx;
   T pgrady2 = pgrady * pgrady;
   T limiter = (((T(0.5) * (ugrad)) / (cdx)) * pgradx2 + ((T(0.5) * (vgrad)) / (cdy)) * pgrady2 + strain2 * pgradx * pgrady) / (fmax(pgradx2 + pgrady2, T(g_small)));
-  if ((limiter > T(0.0)) || (div >= T(0.0))) return T(0.0);
+  if (limiter > T(0.0)) return T(0.0);
   T dirx = T(1.0);
   if (pgradx < T(0.0)) dirx = T(-1.0);
   pgradx = dirx * fmax(T(g_small), fabs(pgradx));
@@ -83,30 +95,38 @@ __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, 
   return T(2.0) * density0 * grad2 * limiter * limiter;
 }
 
-// fields: 0 pressure, 1 density0, 2 xvel0, 3 yvel0
+// Staged: 0 pressure, 1 xvel0, 2 yvel0; density0 is read directly.
 template <typename T>
-__global__ void __launch_bounds__(256) kt_viscosity(const __grid_constant__ Maps maps, T *q_out, Mesh<T> m, int off, int fold, int *err) {
+__global__ void __launch_bounds__(256, 4) kt_viscosity(const __grid_constant__ Maps maps, const T *__restrict__ d0, T *q_out, Mesh<T> m, int off,
+                                                    int fold, int *err) {
   constexpr int TY = 16;
-  using C = Tile<TY>;
+  using B = Box1<T, TY>;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   T *sm = reinterpret_cast<T *>(smraw);
   const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  if (!stage_tiles(sm, maps, 4, C::BOX, off, x0, y0, &bar, err)) return;
-  const T *P = sm, *R = sm + C::BOX, *U = sm + 2 * C::BOX, *V = sm + 3 * C::BOX;
-  const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
+  if (!stage_boxes(sm, maps, 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1, &bar, err)) return;
+  const T *P = sm, *U = sm + B::BOXS, *V = sm + 2 * B::BOXS;
+  const int i = x0 + threadIdx.x;
   if (i >= m.nx + 2) return;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const HaloRule rule = halo_rule(VISCOSITY);
   const T cdx = m.celldx_t[i], cdx1 = m.celldx_t[i + 1];
   const int pitch = (int)m.pitch;
+  constexpr int RPT = TY / 4;
+  T rho[RPT];
 #pragma unroll
-  for (int r = 0; r < C::RPT; ++r) {
-    const int j = y0 + threadIdx.y + 4 * r, ly = HALO + threadIdx.y + 4 * r;
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
+    rho[r] = j < m.ny + 2 ? d0[gidx(pitch, i, j)] : T(0);
+  }
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
     if (j >= m.ny + 2) break;
-    const int b = ly * BOX_X + lx;
+    const int b = B::at(i, j, x0, y0);
     T q = viscosity_value(U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1], P[b - 1],
-                          P[b + 1], P[b - BOX_X], P[b + BOX_X], R[b], cdx, cdx1, m.celldy_t[j], m.celldy_t[j + 2]);
+                          P[b + 1], P[b - BOX_X], P[b + BOX_X], rho[r], cdx, cdx1, m.celldy_t[j], m.celldy_t[j + 2]);
     q_out[gidx(pitch, i, j)] = q;
     if (do_fold) fold_halo(q_out, m, rule, fold, i, j, q);
   }
@@ -115,7 +135,6 @@ __global__ void __launch_bounds__(256) kt_viscosity(const __grid_constant__ Maps
 // ---------------------------------------------------------------------------
 // calc_dt: src/serial/calc_dt.cpp:30-79.  Blocks loop over tiles; each
 // keeps the minimum of its cells and folds it into the result once.
-// fields: 0 soundspeed, 1 viscosity, 2 density0, 3 xvel0, 4 yvel0
 template <typename T>
 __device__ __forceinline__ T dt_value(T ss, T q, T d0, T u00, T u10, T u01, T u11, T v00, T v10, T v01, T v11, T dsx, T dsy,
                                       const DtConsts &k) {
@@ -145,29 +164,48 @@ __device__ __forceinline__ T dt_value(T ss, T q, T d0, T u00, T u10, T u01, T u1
   return fmin(dtct, fmin(dtut, fmin(dtvt, fmin(dtdivt, T(g_big)))));
 }
 
+struct DtIn {
+  const void *soundspeed, *viscosity, *density0;
+};
+
+// Staged: 0 xvel0, 1 yvel0; soundspeed, viscosity, density0 are read directly.
 template <typename T>
-__global__ void __launch_bounds__(256) kt_calc_dt(const __grid_constant__ Maps maps, Mesh<T> m, int off, DtConsts k, int tiles_x,
+__global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Maps maps, DtIn in, Mesh<T> m, int off, DtConsts k, int tiles_x,
                                                   int ntiles, unsigned long long *dt_bits, int *err) {
   constexpr int TY = 16;
-  using C = Tile<TY>;
+  using B = Box1<T, TY>;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   T *sm = reinterpret_cast<T *>(smraw);
-  const T *S = sm, *Q = sm + C::BOX, *R = sm + 2 * C::BOX, *U = sm + 3 * C::BOX, *V = sm + 4 * C::BOX;
+  const T *U = sm, *V = sm + B::BOXS;
+  const T *S = (const T *)in.soundspeed, *Q = (const T *)in.viscosity, *R = (const T *)in.density0;
+  const int pitch = (int)m.pitch;
+  constexpr int RPT = TY / 4;
   double vmin = g_big;
   unsigned phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
     const int x0 = 2 + (t % tiles_x) * TILE_X, y0 = 2 + (t / tiles_x) * TY;
-    if (!stage_loop(sm, maps, 5, C::BOX, off, x0, y0, &bar, phase, t == (int)blockIdx.x, err)) return;
-    const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
+    const int i = x0 + threadIdx.x;
+    // the directly read fields are loaded before the staging wait
+    T ss[RPT], qq[RPT], dd[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int j = y0 + threadIdx.y + 4 * r;
+      const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
+      const int g = gidx(pitch, i, j);
+      ss[r] = in_mesh ? S[g] : T(0);
+      qq[r] = in_mesh ? Q[g] : T(0);
+      dd[r] = in_mesh ? R[g] : T(1);
+    }
+    if (!stage_boxes_loop(sm, maps, 2, B::BOXS, B::BH, off + x0 - HALO, y0 - 1, &bar, phase, t == (int)blockIdx.x, err)) return;
     if (i < m.nx + 2) {
       const T dsx = m.celldx_t[i];
 #pragma unroll
-      for (int r = 0; r < C::RPT; ++r) {
-        const int j = y0 + threadIdx.y + 4 * r, ly = HALO + threadIdx.y + 4 * r;
+      for (int r = 0; r < RPT; ++r) {
+        const int j = y0 + threadIdx.y + 4 * r;
         if (j >= m.ny + 2) break;
-        const int b = ly * BOX_X + lx;
-        const double c = (double)dt_value(S[b], Q[b], R[b], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1],
+        const int b = B::at(i, j, x0, y0);
+        const double c = (double)dt_value(ss[r], qq[r], dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1],
                                           V[b + BOX_X], V[b + BOX_X + 1], dsx, m.celldy_t[j], k);
         vmin = fmin(c, vmin); // fmin drops a NaN candidate, as the reference's fmin does
       }
@@ -179,7 +217,6 @@ __global__ void __launch_bounds__(256) kt_calc_dt(const __grid_constant__ Maps m
 // ---------------------------------------------------------------------------
 // PdV: src/serial/PdV.cpp:36-87; mode 1 also does the predictor's
 // ideal_gas, pressure halo and revert (:92-133) in the same pass.
-// fields: 0 density0, 1 energy0, 2 pressure, 3 viscosity, 4 xvel0, 5 yvel0, [6 xvel1, 7 yvel1]
 template <typename T>
 __device__ __forceinline__ void pdv_value(bool predict, T dt, T xa, T ya, T vol, T u00, T u01, T u10, T u11, T v00, T v10, T v01, T v11,
                                           T w00, T w01, T w10, T w11, T z00, T z10, T z01, T z11, T d0, T e0, T p, T q, T &density1,
@@ -215,33 +252,49 @@ __device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressur
   soundspeed = sqrt(sound_speed_squared);
 }
 
+struct PdvIn {
+  const void *density0, *energy0, *pressure, *viscosity;
+};
 struct PdvOut {
   void *density1, *energy1, *pressure, *soundspeed;
 };
 
+// Staged: 0 xvel0, 1 yvel0, [2 xvel1, 3 yvel1]; the cell fields are read directly.
 template <typename T>
-__global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvOut out, Mesh<T> m, int off, int predict, T dt,
+__global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict, T dt,
                                               int mode, T gm1, int fold, int *err) {
   constexpr int TY = 8;
-  using C = Tile<TY>;
+  using B = Box1<T, TY>;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   T *sm = reinterpret_cast<T *>(smraw);
   const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  const int nf = predict ? 6 : 8;
-  if (!stage_tiles(sm, maps, nf, C::BOX, off, x0, y0, &bar, err)) return;
-  const T *D0 = sm, *E0 = sm + C::BOX, *P = sm + 2 * C::BOX, *Q = sm + 3 * C::BOX, *U0 = sm + 4 * C::BOX, *V0 = sm + 5 * C::BOX;
-  const T *U1 = sm + 6 * C::BOX, *V1 = sm + 7 * C::BOX;
-  const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
+  const int i = x0 + threadIdx.x;
+  const int pitch = (int)m.pitch;
+  constexpr int RPT = TY / 4;
+  // the cell fields are loaded before the staging wait
+  T rd[RPT], re[RPT], rp[RPT], rq[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
+    const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
+    const int g = gidx(pitch, i, j);
+    rd[r] = in_mesh ? ((const T *)in.density0)[g] : T(1);
+    re[r] = in_mesh ? ((const T *)in.energy0)[g] : T(0);
+    rp[r] = in_mesh ? ((const T *)in.pressure)[g] : T(0);
+    rq[r] = in_mesh ? ((const T *)in.viscosity)[g] : T(0);
+  }
+  const int nf = predict ? 2 : 4;
+  if (!stage_boxes(sm, maps, nf, B::BOXS, B::BH, off + x0 - HALO, y0 - 1, &bar, err)) return;
+  const T *U0 = sm, *V0 = sm + B::BOXS, *U1 = sm + 2 * B::BOXS, *V1 = sm + 3 * B::BOXS;
   if (i >= m.nx + 2) return;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
-  const int pitch = (int)m.pitch;
   const T cdx = m.celldx_t[i];
 #pragma unroll
-  for (int r = 0; r < C::RPT; ++r) {
-    const int j = y0 + threadIdx.y + 4 * r, ly = HALO + threadIdx.y + 4 * r;
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
     if (j >= m.ny + 2) break;
-    const int b = ly * BOX_X + lx;
+    const int b = B::at(i, j, x0, y0);
     const T cdy = m.celldy_t[j];
     const T vol = cdx * cdy;
     T w00 = T(0), w01 = T(0), w10 = T(0), w11 = T(0), z00 = T(0), z10 = T(0), z01 = T(0), z11 = T(0);
@@ -251,7 +304,7 @@ __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps,
     }
     T d1, e1;
     pdv_value(predict != 0, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
-              V0[b + BOX_X + 1], w00, w01, w10, w11, z00, z10, z01, z11, D0[b], E0[b], P[b], Q[b], d1, e1);
+              V0[b + BOX_X + 1], w00, w01, w10, w11, z00, z10, z01, z11, rd[r], re[r], rp[r], rq[r], d1, e1);
     const int g = gidx(pitch, i, j);
     if (mode == 0) {
       ((T *)out.density1)[g] = d1;
@@ -266,8 +319,8 @@ __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps,
       ((T *)out.pressure)[g] = p;
       ((T *)out.soundspeed)[g] = c;
       if (do_fold) fold_halo((T *)out.pressure, m, halo_rule(PRESSURE), fold, i, j, p);
-      ((T *)out.density1)[g] = D0[b];
-      ((T *)out.energy1)[g] = E0[b];
+      ((T *)out.density1)[g] = rd[r];
+      ((T *)out.energy1)[g] = re[r];
     }
   }
 }
