@@ -350,7 +350,7 @@ def main():
 
     # FP32 form, replaying the FP64 run's dt sequence, errors against FP64 at the same time
     dts = list(run64.dt_trace)
-    ms32, run32, c32, _, _ = run_form(FP32, S, args.warmup, args.steps, forced_dt=dts, world=world)
+    ms32, run32, c32, ph32, _ = run_form(FP32, S, args.warmup, args.steps, forced_dt=dts, with_phases=True, world=world)
     if world > 1:
         t = torch.tensor([ms32], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -370,7 +370,8 @@ def main():
 
     fp32 = {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
             "errors_vs_fp64": errs, "drift_fp64": drift(run64), "drift_fp32": drift(run32),
-            "dt_sequence": "the FP64 run's, replayed"}
+            "dt_sequence": "the FP64 run's, replayed",
+            "phase_ms_per_step": {k: ph32[0][k] / args.steps for k in sorted(ph32[0])}}
     c64.close()
     c32.close()
 

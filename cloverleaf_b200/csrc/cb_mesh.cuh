@@ -69,6 +69,15 @@ __host__ __device__ inline HaloRule halo_rule(int f) {
   return r;
 }
 
+// Quotient for terms that every step recomputes from the state (flux
+// limiters, the artificial viscosity, CFL bounds, the sound speed): the
+// exact IEEE quotient in FP64; in the FP32 form the approximate hardware
+// quotient (within 2 ulp), whose error does not build up from step to step.
+// The conservative updates (PdV, accelerate, the advection updates) always
+// use the exact operator.
+template <typename T> __device__ __forceinline__ T lim_div(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float lim_div<float>(float a, float b) { return __fdividef(a, b); }
+
 template <typename T> struct Mesh {
   int nx, ny;
   long long pitch;           // elements per row

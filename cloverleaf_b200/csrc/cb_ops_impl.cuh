@@ -16,7 +16,7 @@ namespace detail {
 
 template <typename T> Fields<T> fields(const Chunk &c) {
   Fields<T> F;
-  for (int f = 0; f < NUM_FIELDS; ++f) F.f[f] = (T *)c.base(f);
+  for (int f = 0; f < NUM_FIELDS; ++f) F.f[f] = f < 15 ? (T *)c.base(f) : nullptr; // work arrays and geometry are not stored
   return F;
 }
 
@@ -84,7 +84,7 @@ template <typename T> cudaError_t Ops<T>::generate_chunk(Chunk &c, const DevStat
 
 template <typename T> cudaError_t Ops<T>::ideal_gas(Chunk &c, int predict, int fold) {
   dim3 b(32, 8);
-  k_ideal_gas<T><<<grid2(c.nx, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), predict, gm1<T>(c), fold);
+  k_ideal_gas<T><<<grid2((c.nx + Vec16<T>::N - 1) / Vec16<T>::N, c.ny, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), predict, gm1<T>(c), fold);
   return launched(c);
 }
 
@@ -229,7 +229,7 @@ template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int 
 
 template <typename T> cudaError_t Ops<T>::reset_field(Chunk &c, int fold) {
   dim3 b(32, 8);
-  k_reset_field<T><<<grid2(c.nx + 1, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), fold);
+  k_reset_field<T><<<grid2((c.nx + 1 + Vec16<T>::N - 1) / Vec16<T>::N, c.ny + 1, b), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), fold);
   return launched(c);
 }
 

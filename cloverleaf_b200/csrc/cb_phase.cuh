@@ -14,6 +14,8 @@
 // `double` explicitly.
 #pragma once
 
+#include <cstring>
+
 #include "cb_mesh.cuh"
 #include "cb_ops.h"
 
@@ -92,7 +94,7 @@ __global__ void k_generate_chunk(Fields<T> F, Mesh<T> m, const DevState *st, int
 // reference's hard-coded gamma = 1.4).
 template <typename T>
 __device__ __forceinline__ void eos(T density, T energy, T gm1, T &pressure, T &soundspeed) {
-  T v = (T(1.0)) / (density);
+  T v = lim_div(T(1.0), density); // feeds the sound speed only
   pressure = gm1 * density * energy;
   T pressurebyenergy = gm1 * density;
   T pressurebyvolume = -density * pressure;
@@ -100,17 +102,71 @@ __device__ __forceinline__ void eos(T density, T energy, T gm1, T &pressure, T &
   soundspeed = sqrt(sound_speed_squared);
 }
 
+// 16-byte vectors of the storage type for the pointwise kernels.  The
+// first interior column (i = 2) of every field sits on a 256-byte
+// boundary, so elements i = 2 + N k start aligned vectors.
+template <typename T> struct Vec16;
+template <> struct Vec16<double> {
+  using type = double2;
+  static constexpr int N = 2;
+};
+template <> struct Vec16<float> {
+  using type = float4;
+  static constexpr int N = 4;
+};
+
+// True when the block of a pointwise kernel (columns [ilo, ihi], rows
+// [jlo, jhi]) lies within 8 elements of a mesh edge, where folds happen.
+__device__ __forceinline__ bool near_edge(int nx, int ny, int ilo, int ihi, int jlo, int jhi) {
+  return ilo < 10 || ihi > nx - 8 || jlo < 10 || jhi > ny - 8;
+}
+
+// Each thread handles N consecutive cells of one row (block 32 x 8).
 template <typename T>
 __global__ void k_ideal_gas(Fields<T> F, Mesh<T> m, int predict, T gm1, int fold) {
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int N = Vec16<T>::N;
+  using V = typename Vec16<T>::type;
+  const int i0 = 2 + (blockIdx.x * blockDim.x + threadIdx.x) * N;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= m.nx + 2 || j >= m.ny + 2) return;
-  const long long id = m.at(i, j);
-  T p, c;
-  eos(F.f[predict ? DENSITY1 : DENSITY0][id], F.f[predict ? ENERGY1 : ENERGY0][id], gm1, p, c);
-  F.f[PRESSURE][id] = p;
-  F.f[SOUNDSPEED][id] = c;
-  if (fold) fold_halo(F.f[PRESSURE], m, halo_rule(PRESSURE), fold, i, j, p);
+  const bool edge = fold && near_edge(m.nx, m.ny, 2 + blockIdx.x * blockDim.x * N, 2 + (blockIdx.x + 1) * blockDim.x * N,
+                                      2 + blockIdx.y * blockDim.y, 2 + (blockIdx.y + 1) * blockDim.y);
+  if (i0 >= m.nx + 2 || j >= m.ny + 2) return;
+  const long long id = m.at(i0, j);
+  const T *den = F.f[predict ? DENSITY1 : DENSITY0], *ene = F.f[predict ? ENERGY1 : ENERGY0];
+  T d[N], e[N], p[N], c[N];
+  const bool whole = i0 + N - 1 <= m.nx + 1;
+  if (whole) {
+    const V dv = *reinterpret_cast<const V *>(den + id), ev = *reinterpret_cast<const V *>(ene + id);
+    memcpy(d, &dv, sizeof(V));
+    memcpy(e, &ev, sizeof(V));
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      d[k] = i0 + k <= m.nx + 1 ? den[id + k] : T(1);
+      e[k] = i0 + k <= m.nx + 1 ? ene[id + k] : T(0);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k) eos(d[k], e[k], gm1, p[k], c[k]);
+  if (whole) {
+    V pv, cv;
+    memcpy(&pv, p, sizeof(V));
+    memcpy(&cv, c, sizeof(V));
+    *reinterpret_cast<V *>(F.f[PRESSURE] + id) = pv;
+    *reinterpret_cast<V *>(F.f[SOUNDSPEED] + id) = cv;
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      if (i0 + k <= m.nx + 1) {
+        F.f[PRESSURE][id + k] = p[k];
+        F.f[SOUNDSPEED][id + k] = c[k];
+      }
+  }
+  if (edge) {
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      if (i0 + k <= m.nx + 1) fold_halo(F.f[PRESSURE], m, halo_rule(PRESSURE), fold, i0 + k, j, p[k]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -152,27 +208,48 @@ __global__ void k_revert(Fields<T> F, Mesh<T> m) {
 // ---------------------------------------------------------------------------
 // reset_field: src/serial/reset_field.cpp:28-51.
 // With a fold, level 0 also gets the halo update_halo(depth) would give it.
+// Each thread copies N consecutive elements of one row (block 32 x 8):
+// cells [2, nx+1] x [2, ny+1] for density/energy, nodes [2, nx+2] x
+// [2, ny+2] for the velocities.
 template <typename T>
 __global__ void k_reset_field(Fields<T> F, Mesh<T> m, int fold) {
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int N = Vec16<T>::N;
+  using V = typename Vec16<T>::type;
+  const int i0 = 2 + (blockIdx.x * blockDim.x + threadIdx.x) * N;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= m.nx + 3 || j >= m.ny + 3) return;
-  const long long id = m.at(i, j);
-  if (i < m.nx + 2 && j < m.ny + 2) {
-    const T d = F.f[DENSITY1][id], e = F.f[ENERGY1][id];
-    F.f[DENSITY0][id] = d;
-    F.f[ENERGY0][id] = e;
-    if (fold) {
-      fold_halo(F.f[DENSITY0], m, halo_rule(DENSITY0), fold, i, j, d);
-      fold_halo(F.f[ENERGY0], m, halo_rule(ENERGY0), fold, i, j, e);
+  const bool edge = fold && near_edge(m.nx, m.ny, 2 + blockIdx.x * blockDim.x * N, 2 + (blockIdx.x + 1) * blockDim.x * N,
+                                      2 + blockIdx.y * blockDim.y, 2 + (blockIdx.y + 1) * blockDim.y);
+  if (i0 > m.nx + 2 || j > m.ny + 2) return;
+  const long long id = m.at(i0, j);
+  const bool cell_row = j <= m.ny + 1;
+  auto copy = [&](int src, int dst, int imax) {
+    if (i0 + N - 1 <= imax) {
+      *reinterpret_cast<V *>(F.f[dst] + id) = *reinterpret_cast<const V *>(F.f[src] + id);
+    } else {
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+        if (i0 + k <= imax) F.f[dst][id + k] = F.f[src][id + k];
     }
+  };
+  if (cell_row) {
+    copy(DENSITY1, DENSITY0, m.nx + 1);
+    copy(ENERGY1, ENERGY0, m.nx + 1);
   }
-  const T u = F.f[XVEL1][id], v = F.f[YVEL1][id];
-  F.f[XVEL0][id] = u;
-  F.f[YVEL0][id] = v;
-  if (fold) {
-    fold_halo(F.f[XVEL0], m, halo_rule(XVEL0), fold, i, j, u);
-    fold_halo(F.f[YVEL0], m, halo_rule(YVEL0), fold, i, j, v);
+  copy(XVEL1, XVEL0, m.nx + 2);
+  copy(YVEL1, YVEL0, m.nx + 2);
+  if (edge) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const int i = i0 + k;
+      if (cell_row && i <= m.nx + 1) {
+        fold_halo(F.f[DENSITY0], m, halo_rule(DENSITY0), fold, i, j, F.f[DENSITY0][id + k]);
+        fold_halo(F.f[ENERGY0], m, halo_rule(ENERGY0), fold, i, j, F.f[ENERGY0][id + k]);
+      }
+      if (i <= m.nx + 2) {
+        fold_halo(F.f[XVEL0], m, halo_rule(XVEL0), fold, i, j, F.f[XVEL0][id + k]);
+        fold_halo(F.f[YVEL0], m, halo_rule(YVEL0), fold, i, j, F.f[YVEL0][id + k]);
+      }
+    }
   }
 }
 

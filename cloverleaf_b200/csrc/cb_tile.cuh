@@ -74,12 +74,13 @@ __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, 
   T vgrad = (v01 + v11) - (v00 + v10);
   T div = (cdx * (ugrad) + cdy * (vgrad));
   if (div >= T(0.0)) return T(0.0);
-  T strain2 = (T(0.5) * (u01 + u11 - u00 - u10)) / (cdy) + (T(0.5) * (v10 + v11 - v00 - v01)) / (cdx);
-  T pgradx = (p_r - p_l) / (cdx + cdx1);
-  T pgrady = (p_t - p_b) / (cdy + cdy2);
+  T strain2 = lim_div(T(0.5) * (u01 + u11 - u00 - u10), cdy) + lim_div(T(0.5) * (v10 + v11 - v00 - v01), cdx);
+  T pgradx = lim_div(p_r - p_l, cdx + cdx1);
+  T pgrady = lim_div(p_t - p_b, cdy + cdy2);
   T pgradx2 = pgradx * pgradx;
   T pgrady2 = pgrady * pgrady;
-  T limiter = (((T(0.5) * (ugrad)) / (cdx)) * pgradx2 + ((T(0.5) * (vgrad)) / (cdy)) * pgrady2 + strain2 * pgradx * pgrady) / (fmax(pgradx2 + pgrady2, T(g_small)));
+  T limiter = lim_div(lim_div(T(0.5) * (ugrad), cdx) * pgradx2 + lim_div(T(0.5) * (vgrad), cdy) * pgrady2 + strain2 * pgradx * pgrady,
+                      fmax(pgradx2 + pgrady2, T(g_small)));
   if (limiter > T(0.0)) return T(0.0);
   T dirx = T(1.0);
   if (pgradx < T(0.0)) dirx = T(-1.0);
@@ -88,8 +89,8 @@ __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, 
   if (pgradx < T(0.0)) diry = T(-1.0);
   pgrady = diry * fmax(T(g_small), fabs(pgrady));
   T pgrad = sqrt(pgradx * pgradx + pgrady * pgrady);
-  T xgrad = fabs((cdx * pgrad) / (pgradx));
-  T ygrad = fabs((cdy * pgrad) / (pgrady));
+  T xgrad = fabs(lim_div(cdx * pgrad, pgradx));
+  T ygrad = fabs(lim_div(cdy * pgrad, pgrady));
   T grad = fmin(xgrad, ygrad);
   T grad2 = grad * grad;
   return T(2.0) * density0 * grad2 * limiter * limiter;
@@ -142,22 +143,22 @@ __device__ __forceinline__ T dt_value(T ss, T q, T d0, T u00, T u10, T u01, T u1
   const T xa0 = dsy, xa1 = dsy;   // xarea(i, j), xarea(i+1, j) = celldy[j]
   const T ya0 = dsx, ya1 = dsx;   // yarea(i, j), yarea(i, j+1) = celldx[i]
   T cc = ss * ss;
-  cc = cc + (T(2.0) * q) / (d0);
+  cc = cc + lim_div(T(2.0) * q, d0);
   cc = fmax(sqrt(cc), T(g_small));
-  T dtct = (T(k.dtc_safe) * fmin(dsx, dsy)) / (cc);
+  T dtct = lim_div(T(k.dtc_safe) * fmin(dsx, dsy), cc);
   T div = T(0.0);
   T dv1 = (u00 + u01) * xa0;
   T dv2 = (u10 + u11) * xa1;
   div = div + dv2 - dv1;
-  T dtut = (T(k.dtu_safe) * T(2.0) * vol) / (fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol));
+  T dtut = lim_div(T(k.dtu_safe) * T(2.0) * vol, fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol));
   dv1 = (v00 + v10) * ya0;
   dv2 = (v01 + v11) * ya1;
   div = div + dv2 - dv1;
-  T dtvt = (T(k.dtv_safe) * T(2.0) * vol) / (fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol));
-  div = (div) / (T(2.0) * vol);
+  T dtvt = lim_div(T(k.dtv_safe) * T(2.0) * vol, fmax(fmax(fabs(dv1), fabs(dv2)), T(g_small) * vol));
+  div = lim_div(div, T(2.0) * vol);
   T dtdivt;
   if (div < T(-g_small)) {
-    dtdivt = T(k.dtdiv_safe) * ((T(-1.0)) / (div));
+    dtdivt = T(k.dtdiv_safe) * lim_div(T(-1.0), div);
   } else {
     dtdivt = T(g_big);
   }
@@ -244,7 +245,7 @@ __device__ __forceinline__ void pdv_value(bool predict, T dt, T xa, T ya, T vol,
 
 template <typename T>
 __device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressure, T &soundspeed) {
-  T v = (T(1.0)) / (density);
+  T v = lim_div(T(1.0), density); // feeds the sound speed only
   pressure = gm1 * density * energy;
   T pressurebyenergy = gm1 * density;
   T pressurebyvolume = -density * pressure;
@@ -518,14 +519,14 @@ __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Map
     }
     const int bd = b + (donor - f) * ST, bu = b + (upwind - f) * ST, bw = b + (downwind - f) * ST;
     const T pre_vol_d = s_pv[L::pv(donor - a0 + 1, l)];
-    T sigmat = (fabs(flux)) / (pre_vol_d);
-    T sigma3 = (T(1.0) + sigmat) * (T)((vdx[f]) / (vdx[dif]));
+    T sigmat = lim_div(fabs(flux), pre_vol_d);
+    T sigma3 = (T(1.0) + sigmat) * lim_div((T)vdx[f], (T)vdx[dif]);
     T sigma4 = T(2.0) - sigmat;
     T sigmav = sigmat;
     const T dd = D1[bd], du = D1[bu], dw = D1[bw];
     T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
     T mass_flux = flux * (dd + limiter);
-    T sigmam = (fabs(mass_flux)) / ((dd * pre_vol_d));
+    T sigmam = lim_div(fabs(mass_flux), dd * pre_vol_d);
     const T ed = E1[bd], eu = E1[bu], ew = E1[bw];
     limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
     s_mf[L::fx(p, l)] = (double)mass_flux;
@@ -551,10 +552,19 @@ __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Map
     const T vf_hi = DIR == 1 ? VFX[b + 1] : VFY[b + BOX_X];
     double pre_mass_s = (double)D1[b] * (double)pre_vol;
     double post_mass_s = pre_mass_s + mf_lo - mf_hi;
-    double post_ener_s = ((double)E1[b] * pre_mass_s + ef_lo - ef_hi) / (post_mass_s);
+    double ener_s = (double)E1[b] * pre_mass_s + ef_lo - ef_hi;
     double advec_vol_s = (double)pre_vol + (double)vf_lo - (double)vf_hi;
-    const T dnew = (T)((post_mass_s) / (advec_vol_s));
-    const T enew = (T)post_ener_s;
+    T dnew, enew;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      const double post_ener_s = (ener_s) / (post_mass_s);
+      dnew = (T)((post_mass_s) / (advec_vol_s));
+      enew = (T)post_ener_s;
+    } else {
+      // FP32 form: the sums above stay FP64; the quotients are stored in
+      // FP32, so they are formed in FP32 from the rounded sums
+      dnew = (T)post_mass_s / (T)advec_vol_s;
+      enew = (T)ener_s / (T)post_mass_s;
+    }
     const int g = gidx(pitch, i, j);
     ((T *)out.density1)[g] = dnew;
     ((T *)out.energy1)[g] = enew;
@@ -592,7 +602,7 @@ __device__ __forceinline__ T mom_limiter_value(T vdiffuw, T vdiffdw, T sigma, T 
     T adw = fabs(vdiffdw);
     T wind = T(1.0);
     if (vdiffdw <= T(0.0)) wind = T(-1.0);
-    limiter = wind * fmin(fmin((width * (((T(2.0) - sigma) * adw) / (width) + ((T(1.0) + sigma) * auw) / (dx_dif))) / (T(6.0)), auw), adw);
+    limiter = wind * fmin(fmin(lim_div(width * (lim_div((T(2.0) - sigma) * adw, width) + lim_div((T(1.0) + sigma) * auw, dx_dif)), T(6.0)), auw), adw);
   }
   return limiter;
 }
@@ -744,7 +754,7 @@ __global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps
     } else {
       upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
     }
-    const T sigma = (fabs(nfv)) / (s_nmpre[L::w(p + (donor - a), l)]);
+    const T sigma = lim_div(fabs(nfv), s_nmpre[L::w(p + (donor - a), l)]);
     const T width = celld[a];
     const T dxd = celld[dif];
     const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
