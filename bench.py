@@ -233,6 +233,58 @@ def traffic_per_launch(kernel, cells):
         return None
 
 
+def batch_leg(n_decks, seq_sample):
+    """The batched ensemble: n_decks seeded decks of uneven size, each with its
+    own gamma and dt, run to t = 0.5 by one persistent launch (FP64 and FP32),
+    after the autotuner has picked the schedule; against the same decks run
+    one after the other through the C ABI (HydroRun per deck: the driver's
+    call sequence, dt read back every step) on a seeded sample."""
+    import numpy as np
+    from cloverleaf_b200 import FP32, FP64, Batch, Chunk, HydroRun, ensemble_decks
+    from cloverleaf_b200 import batch as B
+    decks = ensemble_decks(n_decks)
+    out = {"decks": n_decks, "seed": "0xC10E, numpy PCG64", "sides": list(B.ENSEMBLE_SIDES), "end_time": 0.5,
+           "cells": int(sum(d.x_cells * d.y_cells for d in decks))}
+    finals = {}
+    for prec, name in ((FP64, "fp64"), (FP32, "fp32")):
+        b = Batch(decks, prec)
+        best, trials = b.autotune(repeats=1)
+        ms = []
+        for _ in range(3):
+            b.run()
+            ms.append(b.synchronize())
+        res = [b.result(k) for k in range(n_decks)]
+        cs = sum(d.x_cells * d.y_cells * r.steps for d, r in zip(decks, res))
+        t = statistics.median(ms)
+        sched, lanes, ctas = b.schedule()
+        out[name] = {"value": cs / (t / 1e3), "unit": UNIT, "ms": t, "cell_steps": cs,
+                     "done": sum(r.status == B.DECK_DONE for r in res), "steps_min": min(r.steps for r in res),
+                     "steps_max": max(r.steps for r in res), "schedule": best, "lanes": lanes, "ctas": ctas,
+                     "launches_per_run": 1, "trials": trials}
+        finals[name] = [b.read(k, "density0")[2:-2, 2:-2] for k in range(0, n_decks, max(1, n_decks // 64))]
+        b.close()
+    l1 = [float(np.abs(a - c).sum() / np.abs(a).sum()) for a, c in zip(finals["fp64"], finals["fp32"])]
+    out["fp32"]["density_l1_rel_vs_fp64"] = {"max": max(l1), "mean": statistics.mean(l1), "decks_checked": len(l1)}
+    sample = decks[::max(1, n_decks // seq_sample)][:seq_sample]
+    for prec, name in ((FP64, "sequential_fp64"), (FP32, "sequential_fp32")):
+        cs, tsum = 0, 0.0
+        for dk in sample:
+            c = Chunk(dk.x_cells, dk.y_cells, precision=prec, gamma=dk.gamma)
+            r = HydroRun(c, dk)
+            c.synchronize()
+            t0 = time.perf_counter()
+            r.run()
+            c.synchronize()
+            tsum += time.perf_counter() - t0
+            cs += dk.x_cells * dk.y_cells * r.step
+            c.close()
+        out[name] = {"value": cs / tsum, "unit": UNIT, "sample": f"{len(sample)} of the {n_decks} decks (every "
+                     f"{max(1, n_decks // seq_sample)}th), one after the other, wall clock incl. the per-step dt read-back"}
+    out["speedup_fp64_vs_sequential"] = out["fp64"]["value"] / out["sequential_fp64"]["value"]
+    out["speedup_fp32_vs_sequential"] = out["fp32"]["value"] / out["sequential_fp32"]["value"]
+    return out
+
+
 def reference_exe():
     return os.path.join(ROOT, "oracle", "_ref", "omp")
 
@@ -318,6 +370,7 @@ def main():
     ap.add_argument("--size", type=int, default=7680)
     ap.add_argument("--large", type=int, default=15360, help="second FP64 size timed (0 to skip)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch", type=int, default=512, help="decks of the batched-ensemble leg (0 to skip)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -403,6 +456,13 @@ def main():
             "step_frac": value / world * STEP_ARRAYS * 8 / 1e9 / peak,
             "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)}}
 
+    batch = None
+    if args.batch:
+        try:
+            batch = batch_leg(args.batch, 32)
+        except Exception as e:
+            batch = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -418,7 +478,7 @@ def main():
                            "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "halo": "folded into producers"},
-                "roofline": roof, "fp32": fp32, "large": large, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:

@@ -31,7 +31,10 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk",
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
-           "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_field_summary_noalloc"]
+           "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_field_summary_noalloc",
+           "cb_batch_create", "cb_batch_destroy", "cb_batch_set_schedule", "cb_batch_get_schedule", "cb_batch_autotune",
+           "cb_batch_run", "cb_batch_synchronize", "cb_batch_deck_result", "cb_batch_read_summaries", "cb_batch_read_dt",
+           "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count"]
 
 
 class CloverError(RuntimeError):

@@ -137,33 +137,77 @@ using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
                                  const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+} // namespace
+
+namespace cb {
+
 // One 2-D tensor map per buffer and staged box height: the whole allocation
 // as a (pitch x ny+6) array, boxes of BOX_X x h elements (cb_tma.cuh).
-bool encode_maps(cb_chunk *c) {
+bool encode_buffer_maps(void *const *bufs, int nbuf, long long pitch, int ny, int precision, CUtensorMap (*maps)[NUM_BOX_H],
+                        std::string *err) {
   static EncodeTiled encode = nullptr;
   if (!encode) {
     void *fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn) {
-      g_err = "cuTensorMapEncodeTiled is not available from the driver";
+      *err = "cuTensorMapEncodeTiled is not available from the driver";
       return false;
     }
     encode = (EncodeTiled)fn;
   }
-  const cuuint64_t dims[2] = {(cuuint64_t)c->pitch, (cuuint64_t)(c->ny + 6)};
-  const cuuint64_t strides[1] = {(cuuint64_t)(c->pitch * c->esize)};
+  const size_t esize = precision == CB_FP64 ? 8 : 4;
+  const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)(ny + 6)};
+  const cuuint64_t strides[1] = {(cuuint64_t)(pitch * esize)};
   const cuuint32_t estr[2] = {1, 1};
-  for (int b = 0; b < NUM_BUF; ++b)
+  for (int b = 0; b < nbuf; ++b)
     for (int h = 0; h < NUM_BOX_H; ++h) {
       const cuuint32_t box[2] = {(cuuint32_t)BOX_X, (cuuint32_t)BOX_HEIGHTS[h]};
-      CUresult r = encode(&c->tmap[b][h], c->precision == CB_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                          c->buf[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CUresult r = encode(&maps[b][h], precision == CB_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, bufs[b],
+                          dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) {
-        g_err = "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r);
+        *err = "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r);
         return false;
       }
     }
+  return true;
+}
+
+// The 1-D geometry of src/serial/initialise_chunk.cpp:30-85 for a single
+// tile (t_left = t_bottom = 1), into g[NUM_GEOM] arrays of at least
+// max(nx, ny) + 5 entries.
+void chunk_geometry(int nx, int ny, double gxmin, double gymin, double gxmax, double gymax, double *const *g) {
+  const int x_min = 1, y_min = 1, x_max = nx, y_max = ny;
+  double dx = (gxmax - gxmin) / (double)(nx);
+  double dy = (gymax - gymin) / (double)(ny);
+  double xmin = gxmin + dx * (double)(1 - 1);
+  double ymin = gymin + dy * (double)(1 - 1);
+  const int xrange = (x_max + 3) - (x_min - 2) + 1, yrange = (y_max + 3) - (y_min - 2) + 1;
+  for (int j = 0; j < xrange; j++) {
+    g[VERTEXX][j] = xmin + dx * (j - 1 - x_min);
+    g[VERTEXDX][j] = dx;
+  }
+  for (int k = 0; k < yrange; k++) {
+    g[VERTEXY][k] = ymin + dy * (k - 1 - y_min);
+    g[VERTEXDY][k] = dy;
+  }
+  const int xrange1 = (x_max + 2) - (x_min - 2) + 1, yrange1 = (y_max + 2) - (y_min - 2) + 1;
+  for (int j = 0; j < xrange1; j++) {
+    g[CELLX][j] = 0.5 * (g[VERTEXX][j] + g[VERTEXX][j + 1]);
+    g[CELLDX][j] = dx;
+  }
+  for (int k = 0; k < yrange1; k++) {
+    g[CELLY][k] = 0.5 * (g[VERTEXY][k] + g[VERTEXY][k + 1]);
+    g[CELLDY][k] = dy;
+  }
+}
+
+} // namespace cb
+
+namespace {
+
+bool encode_maps(cb_chunk *c) {
+  if (!encode_buffer_maps(c->buf, NUM_BUF, c->pitch, c->ny, c->precision, c->tmap, &g_err)) return false;
   c->tmap_ok = true;
   return true;
 }
@@ -449,30 +493,7 @@ int cb_build_field(cb_chunk *c) {
 int cb_initialise_chunk(cb_chunk *c, double gxmin, double gymin, double gxmax, double gymax) {
   CB_CHECK_CHUNK(c);
   if (!(gxmax > gxmin) || !(gymax > gymin)) return fail(CB_EINVAL, "cb_initialise_chunk: empty domain");
-  const int x_min = 1, y_min = 1, x_max = c->nx, y_max = c->ny;
-  double dx = (gxmax - gxmin) / (double)(c->nx);
-  double dy = (gymax - gymin) / (double)(c->ny);
-  double xmin = gxmin + dx * (double)(1 - 1);
-  double ymin = gymin + dy * (double)(1 - 1);
-  double **g = c->geom_h;
-  const int xrange = (x_max + 3) - (x_min - 2) + 1, yrange = (y_max + 3) - (y_min - 2) + 1;
-  for (int j = 0; j < xrange; j++) {
-    g[VERTEXX][j] = xmin + dx * (j - 1 - x_min);
-    g[VERTEXDX][j] = dx;
-  }
-  for (int k = 0; k < yrange; k++) {
-    g[VERTEXY][k] = ymin + dy * (k - 1 - y_min);
-    g[VERTEXDY][k] = dy;
-  }
-  const int xrange1 = (x_max + 2) - (x_min - 2) + 1, yrange1 = (y_max + 2) - (y_min - 2) + 1;
-  for (int j = 0; j < xrange1; j++) {
-    g[CELLX][j] = 0.5 * (g[VERTEXX][j] + g[VERTEXX][j + 1]);
-    g[CELLDX][j] = dx;
-  }
-  for (int k = 0; k < yrange1; k++) {
-    g[CELLY][k] = 0.5 * (g[VERTEXY][k] + g[VERTEXY][k + 1]);
-    g[CELLDY][k] = dy;
-  }
+  chunk_geometry(c->nx, c->ny, gxmin, gymin, gxmax, gymax, c->geom_h);
   CB_CUDA(upload_geom(c));
   return CB_OK;
 }

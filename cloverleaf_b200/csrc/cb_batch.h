@@ -1,0 +1,88 @@
+// cb_batch.h -- device-side description of a batched ensemble of independent
+// decks and the declarations of the persistent ensemble kernel's launchers.
+//
+// A batch holds many meshes, each laid out exactly as a cb_chunk lays out
+// one (cb_chunk.h: same pitch, offset, 19 buffers and tensor maps), each
+// with its own gamma, states, dt controls and end time.  One launch of the
+// persistent kernel advances every deck from its initial state to its end:
+// the grid is split into lanes of CTAs, a lane runs its decks one after the
+// other, and the CTAs of a lane share each deck's tiles and meet at a lane
+// barrier between the phases.  Every CTA of a lane steps through the same
+// control flow (dt, time, step, summaries) with identical values, so no
+// control state has to be exchanged besides the dt minimum.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "cb_chunk.h"
+#include "cb_ops.h"
+
+namespace cb {
+
+constexpr int BATCH_MAX_STATES = 8;
+constexpr int BATCH_RECORD = 7;       // summary record: step, time, vol, mass, ie, ke, press
+constexpr int BATCH_MAX_LANE = 64;    // CTAs per lane at most
+constexpr int BATCH_VARIANTS = 2;     // tile-shape variants of the kernel (BatchTune)
+
+// Deck status after a run.
+enum : int {
+  DECK_PENDING = 0,     // not reached (the lane stopped earlier)
+  DECK_DONE = 1,        // reached end_time or end_step
+  DECK_SMALL_DT = 2,    // dt fell below dtmin (driver/timestep.cpp:96, :104-106)
+  DECK_STAGE_FAIL = 3,  // a tile's bulk copy did not arrive within the wait limit
+  DECK_SYNC_FAIL = 4,   // a lane barrier gave up (or another lane's did)
+};
+
+struct BatchDeck {
+  // layout (as cb_create lays out one chunk)
+  int nx, ny, off, pitch;
+  size_t buf_bytes;           // bytes of each buffer (a multiple of 256)
+  void *buf[NUM_BUF];         // the 15 state fields in field order, then the 4 spares
+  const CUtensorMap *maps;    // [NUM_BUF][NUM_BOX_H], in global memory
+  const double *geom_d[NUM_GEOM];
+  const void *geom_t[NUM_GEOM];
+  // the deck (driver/definitions.h:227-256 globals that the step reads)
+  double gm1;                 // gamma - 1
+  int nstates;
+  DevState states[BATCH_MAX_STATES];
+  double dtinit, dtmin, dtmax, dtrise, end_time;
+  int end_step, summary_frequency;
+  DtConsts k;
+  // records
+  double *summaries;          // BATCH_RECORD doubles per record
+  int max_summaries;
+  double *dt_trace;           // dt of each step
+  int max_steps;
+  unsigned long long *dt_slots; // 3 reduction slots, rotated by step
+  double *partials;           // 5 per CTA of the lane
+  // results, written by the lane's first CTA when the deck ends
+  int steps, nsummaries, status;
+  double time;
+};
+
+struct BatchLaunch {
+  BatchDeck *decks;
+  const int *cta_lane;   // lane of each CTA
+  const int *lane_cta0;  // first CTA of each lane
+  const int *lane_width; // CTAs of each lane
+  const int *lane_deck0; // decks of lane l: lane_decks[lane_deck0[l] .. lane_deck0[l + 1])
+  const int *lane_decks;
+  unsigned *lane_sync;   // one barrier counter per lane (zero at launch)
+  int *abort;            // set when a barrier wait gives up; ends every lane
+  int *err;              // set when a staging wait gives up
+};
+
+template <typename T> struct BatchOps {
+  // dynamic shared memory of the kernel variant
+  static size_t smem_bytes(int variant);
+  // resident CTAs per SM of the variant
+  static cudaError_t occupancy(int variant, int *per_sm);
+  // one launch of the whole ensemble (cooperative: every CTA co-resident)
+  static cudaError_t launch(int variant, const BatchLaunch &a, int grid, cudaStream_t s);
+};
+
+extern template struct BatchOps<double>;
+extern template struct BatchOps<float>;
+
+} // namespace cb

@@ -3,3 +3,6 @@
 #include "cb_ops_impl.cuh"
 
 template struct cb::Ops<float>;
+
+#include "cb_batch_impl.cuh"
+template struct cb::BatchOps<float>;

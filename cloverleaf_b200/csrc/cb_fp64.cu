@@ -4,3 +4,6 @@
 #include "cb_ops_impl.cuh"
 
 template struct cb::Ops<double>;
+
+#include "cb_batch_impl.cuh"
+template struct cb::BatchOps<double>;

@@ -45,11 +45,11 @@ __device__ __forceinline__ bool state_hits(const DevState &s, const Mesh<T> &m, 
   return false;
 }
 
+// Element (i, j) of the full extents (cells [0, nx+4) x [0, ny+4), nodes up
+// to nx+4 / ny+4).
 template <typename T>
-__global__ void k_generate_chunk(Fields<T> F, Mesh<T> m, const DevState *st, int nstates, const double *cellx,
-                                 const double *celly, const double *vertexx, const double *vertexy) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void generate_element(const Fields<T> &F, const Mesh<T> &m, const DevState *st, int nstates, const double *cellx,
+                                                 const double *celly, const double *vertexx, const double *vertexy, int i, int j) {
   const int xr = m.nx + 4, yr = m.ny + 4;
   if (i > xr || j > yr) return;
   // cell part (cells cover [0, xr) x [0, yr))
@@ -89,6 +89,13 @@ __global__ void k_generate_chunk(Fields<T> F, Mesh<T> m, const DevState *st, int
   }
 }
 
+template <typename T>
+__global__ void k_generate_chunk(Fields<T> F, Mesh<T> m, const DevState *st, int nstates, const double *cellx,
+                                 const double *celly, const double *vertexx, const double *vertexy) {
+  generate_element(F, m, st, nstates, cellx, celly, vertexx, vertexy, blockIdx.x * blockDim.x + threadIdx.x,
+                   blockIdx.y * blockDim.y + threadIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // ideal_gas: src/serial/ideal_gas.cpp:28-48.  gm1 = gamma - 1 (0.4 at the
 // reference's hard-coded gamma = 1.4).
@@ -121,15 +128,19 @@ __device__ __forceinline__ bool near_edge(int nx, int ny, int ilo, int ihi, int 
   return ilo < 10 || ihi > nx - 8 || jlo < 10 || jhi > ny - 8;
 }
 
-// Each thread handles N consecutive cells of one row (block 32 x 8).
+// Blocks of the pointwise phases are 32 x 8 threads.
+constexpr int PW_X = 32, PW_Y = 8;
+
+// One 32 x 8 block (block coordinates (bx, by), thread (tx, ty)); each
+// thread handles N consecutive cells of one row.
 template <typename T>
-__global__ void k_ideal_gas(Fields<T> F, Mesh<T> m, int predict, T gm1, int fold) {
+__device__ __forceinline__ void ideal_gas_block(const Fields<T> &F, const Mesh<T> &m, int predict, T gm1, int fold, int bx, int by, int tx,
+                                                int ty) {
   constexpr int N = Vec16<T>::N;
   using V = typename Vec16<T>::type;
-  const int i0 = 2 + (blockIdx.x * blockDim.x + threadIdx.x) * N;
-  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  const bool edge = fold && near_edge(m.nx, m.ny, 2 + blockIdx.x * blockDim.x * N, 2 + (blockIdx.x + 1) * blockDim.x * N,
-                                      2 + blockIdx.y * blockDim.y, 2 + (blockIdx.y + 1) * blockDim.y);
+  const int i0 = 2 + (bx * PW_X + tx) * N;
+  const int j = 2 + by * PW_Y + ty;
+  const bool edge = fold && near_edge(m.nx, m.ny, 2 + bx * PW_X * N, 2 + (bx + 1) * PW_X * N, 2 + by * PW_Y, 2 + (by + 1) * PW_Y);
   if (i0 >= m.nx + 2 || j >= m.ny + 2) return;
   const long long id = m.at(i0, j);
   const T *den = F.f[predict ? DENSITY1 : DENSITY0], *ene = F.f[predict ? ENERGY1 : ENERGY0];
@@ -167,6 +178,11 @@ __global__ void k_ideal_gas(Fields<T> F, Mesh<T> m, int predict, T gm1, int fold
     for (int k = 0; k < N; ++k)
       if (i0 + k <= m.nx + 1) fold_halo(F.f[PRESSURE], m, halo_rule(PRESSURE), fold, i0 + k, j, p[k]);
   }
+}
+
+template <typename T>
+__global__ void k_ideal_gas(Fields<T> F, Mesh<T> m, int predict, T gm1, int fold) {
+  ideal_gas_block(F, m, predict, gm1, fold, blockIdx.x, blockIdx.y, threadIdx.x, threadIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -212,13 +228,12 @@ __global__ void k_revert(Fields<T> F, Mesh<T> m) {
 // cells [2, nx+1] x [2, ny+1] for density/energy, nodes [2, nx+2] x
 // [2, ny+2] for the velocities.
 template <typename T>
-__global__ void k_reset_field(Fields<T> F, Mesh<T> m, int fold) {
+__device__ __forceinline__ void reset_field_block(const Fields<T> &F, const Mesh<T> &m, int fold, int bx, int by, int tx, int ty) {
   constexpr int N = Vec16<T>::N;
   using V = typename Vec16<T>::type;
-  const int i0 = 2 + (blockIdx.x * blockDim.x + threadIdx.x) * N;
-  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-  const bool edge = fold && near_edge(m.nx, m.ny, 2 + blockIdx.x * blockDim.x * N, 2 + (blockIdx.x + 1) * blockDim.x * N,
-                                      2 + blockIdx.y * blockDim.y, 2 + (blockIdx.y + 1) * blockDim.y);
+  const int i0 = 2 + (bx * PW_X + tx) * N;
+  const int j = 2 + by * PW_Y + ty;
+  const bool edge = fold && near_edge(m.nx, m.ny, 2 + bx * PW_X * N, 2 + (bx + 1) * PW_X * N, 2 + by * PW_Y, 2 + (by + 1) * PW_Y);
   if (i0 > m.nx + 2 || j > m.ny + 2) return;
   const long long id = m.at(i0, j);
   const bool cell_row = j <= m.ny + 1;
@@ -290,16 +305,18 @@ __global__ void k_copy_ring(RingPair rp, Mesh<T> m, int ilo, int ihi, int jlo, i
   dst[m.at(i, j)] = src[m.at(i, j)];
 }
 
+template <typename T>
+__global__ void k_reset_field(Fields<T> F, Mesh<T> m, int fold) {
+  reset_field_block(F, m, fold, blockIdx.x, blockIdx.y, threadIdx.x, threadIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // update_halo: src/serial/update_halo.cpp:33-684 in two launches: pass 0 does
 // bottom then top for every column, pass 1 left then right for every row, so
 // corner and tiny-mesh semantics are the reference's exactly.
+// Column (pass 0) or row (pass 1) t of field f's halo fill.
 template <typename T>
-__global__ void k_update_halo(Fields<T> F, Mesh<T> m, HaloJob job, int depth, int pass) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int fi = blockIdx.y;
-  if (fi >= job.nfields) return;
-  const int f = job.field[fi];
+__device__ __forceinline__ void halo_fill(const Fields<T> &F, const Mesh<T> &m, int f, int depth, int pass, int t) {
   const HaloRule r = halo_rule(f);
   T *a = F.f[f];
   const int d = depth;
@@ -319,12 +336,44 @@ __global__ void k_update_halo(Fields<T> F, Mesh<T> m, HaloJob job, int depth, in
   }
 }
 
+template <typename T>
+__global__ void k_update_halo(Fields<T> F, Mesh<T> m, HaloJob job, int depth, int pass) {
+  if ((int)blockIdx.y >= job.nfields) return;
+  halo_fill(F, m, job.field[blockIdx.y], depth, pass, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // field_summary: src/serial/field_summary.cpp:44-104 -- ideal_gas on level 0
 // (writing pressure and soundspeed as the reference does), then the five
 // sums.  Per-cell terms are formed exactly as the reference forms them; the
 // sums are FP64 block partials, reduced by the last block in block order, so
 // the result does not depend on scheduling.
+// The cell's ideal_gas (pressure and soundspeed written) and its terms of
+// the five sums, added to s.
+template <typename T>
+__device__ __forceinline__ void summary_cell(const Fields<T> &F, const Mesh<T> &m, T gm1, int i, int j, double s[5]) {
+  const long long id = m.at(i, j);
+  const T d0 = F.f[DENSITY0][id], e0 = F.f[ENERGY0][id];
+  T p, c;
+  eos(d0, e0, gm1, p, c);
+  F.f[PRESSURE][id] = p;
+  F.f[SOUNDSPEED][id] = c;
+  const T *u = F.f[XVEL0], *v = F.f[YVEL0];
+  double vsqrd = 0.0;
+  for (int kv = j; kv <= j + 1; ++kv)
+    for (int jv = i; jv <= i + 1; ++jv) {
+      const double uu = u[m.at(jv, kv)], vv = v[m.at(jv, kv)];
+      vsqrd += 0.25 * (uu * uu + vv * vv);
+    }
+  const double cell_vol = m.celldx[i] * m.celldy[j];
+  const double cell_mass = cell_vol * (double)d0;
+  s[0] += cell_vol;
+  s[1] += cell_mass;
+  s[2] += cell_mass * (double)e0;
+  s[3] += cell_mass * 0.5 * vsqrd;
+  s[4] += cell_vol * (double)p;
+}
+
 template <typename T>
 __global__ void k_field_summary(Fields<T> F, Mesh<T> m, T gm1, double *partials, unsigned int *counter, double *out,
                                 int tiles_x, int ntiles) {
@@ -333,26 +382,7 @@ __global__ void k_field_summary(Fields<T> F, Mesh<T> m, T gm1, double *partials,
     const int i = 2 + (t % tiles_x) * blockDim.x + threadIdx.x;
     const int j = 2 + (t / tiles_x) * blockDim.y + threadIdx.y;
     if (i >= m.nx + 2 || j >= m.ny + 2) continue;
-    const long long id = m.at(i, j);
-    const T d0 = F.f[DENSITY0][id], e0 = F.f[ENERGY0][id];
-    T p, c;
-    eos(d0, e0, gm1, p, c);
-    F.f[PRESSURE][id] = p;
-    F.f[SOUNDSPEED][id] = c;
-    const T *u = F.f[XVEL0], *v = F.f[YVEL0];
-    double vsqrd = 0.0;
-    for (int kv = j; kv <= j + 1; ++kv)
-      for (int jv = i; jv <= i + 1; ++jv) {
-        const double uu = u[m.at(jv, kv)], vv = v[m.at(jv, kv)];
-        vsqrd += 0.25 * (uu * uu + vv * vv);
-      }
-    const double cell_vol = m.celldx[i] * m.celldy[j];
-    const double cell_mass = cell_vol * (double)d0;
-    s[0] += cell_vol;
-    s[1] += cell_mass;
-    s[2] += cell_mass * (double)e0;
-    s[3] += cell_mass * 0.5 * vsqrd;
-    s[4] += cell_vol * (double)p;
+    summary_cell(F, m, gm1, i, j, s);
   }
   // block reduction (fixed tree order)
   __shared__ double red[5][256];

@@ -46,20 +46,51 @@ template <typename T, int TY> struct Box1 {
   __device__ static constexpr int at(int i, int j, int x0, int y0) { return (j - y0 + 1) * BOX_X + (i - x0 + HALO); }
 };
 
-// Re-armable staging for blocks that loop over several tiles: the barrier
-// is initialised once (init) and completes one phase per tile.
+// Map pointers of the fields a tile stages: the tensor maps live in kernel
+// parameter space (one-launch kernels) or in global memory (the batch
+// kernel); either address is valid for a bulk tensor copy.
+struct MapSet {
+  const CUtensorMap *m[8];
+};
+
+__device__ __forceinline__ MapSet map_set(const Maps &maps, int nf) {
+  MapSet s;
+#pragma unroll
+  for (int f = 0; f < 8; ++f) s.m[f] = f < nf ? &maps.m[f] : nullptr;
+  return s;
+}
+
+// Staging state of a block: its shared-memory mbarrier, the parity of the
+// next completion, and whether the barrier still needs its init.  A
+// one-launch kernel stages once; the batch kernel re-arms the same barrier
+// for every tile it processes.
+struct TileCtx {
+  uint64_t *bar;
+  unsigned phase;
+  bool fresh;
+  int *err;
+};
+
+__device__ __forceinline__ TileCtx tile_ctx(uint64_t *bar, int *err) { return TileCtx{bar, 0u, true, err}; }
+
+// Stages fields ms.m[0..nf) as boxes of BOX_X x bh elements whose first
+// element is tensor coordinate (xs, ys), `stride` elements apart in shared
+// memory (stride * sizeof(T) a multiple of 128 bytes).  Called by every
+// thread of the block; returns false in every thread if the copies did not
+// arrive within the wait limit.
 template <typename T>
-__device__ __forceinline__ bool stage_boxes_loop(T *sm, const Maps &maps, int nf, int stride, int bh, int xs, int ys, uint64_t *bar,
-                                                 unsigned phase, bool init, int *err) {
+__device__ __forceinline__ bool stage(TileCtx &cx, T *sm, const MapSet &ms, int nf, int stride, int bh, int xs, int ys) {
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
-  if (init && leader) mbar_init(bar, 1);
-  __syncthreads(); // the previous tile's readers are done with the boxes
+  if (cx.fresh && leader) mbar_init(cx.bar, 1);
+  __syncthreads(); // barrier initialised; the previous tile's readers are done with the boxes
   if (leader) {
-    mbar_expect_tx(bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
-    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, &maps.m[f], xs, ys, bar);
+    mbar_expect_tx(cx.bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
+    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, ms.m[f], xs, ys, cx.bar);
   }
-  bool ok = mbar_wait(bar, phase, err);
-  if (!ok) mbar_wait(bar, phase, nullptr);
+  bool ok = mbar_wait(cx.bar, cx.phase, cx.err);
+  if (!ok) mbar_wait(cx.bar, cx.phase, nullptr); // a second bounded wait for copies still in flight
+  cx.phase ^= 1u;
+  cx.fresh = false;
   return __syncthreads_and(ok) != 0;
 }
 
@@ -96,20 +127,21 @@ __device__ __forceinline__ T viscosity_value(T u00, T u10, T u01, T u11, T v00, 
   return T(2.0) * density0 * grad2 * limiter * limiter;
 }
 
-// Staged: 0 pressure, 1 xvel0, 2 yvel0; density0 is read directly.
+// One viscosity tile (64 x 16 cells at tile coordinates (bx, by)).
+// Staged: ms 0 pressure, 1 xvel0, 2 yvel0; density0 is read directly.
+constexpr int VISC_TY = 16;
+template <typename T> constexpr size_t visc_smem() { return 3 * Box1<T, VISC_TY>::BOXS * sizeof(T); }
+
 template <typename T>
-__global__ void __launch_bounds__(256, 4) kt_viscosity(const __grid_constant__ Maps maps, const T *__restrict__ d0, T *q_out, Mesh<T> m, int off,
-                                                    int fold, int *err) {
-  constexpr int TY = 16;
+__device__ __forceinline__ bool viscosity_tile(TileCtx &cx, T *sm, const MapSet &ms, const T *d0, T *q_out, const Mesh<T> &m, int off,
+                                               int bx, int by, int fold) {
+  constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  if (!stage_boxes(sm, maps, 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1, &bar, err)) return;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  if (!stage(cx, sm, ms, 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
   const T *P = sm, *U = sm + B::BOXS, *V = sm + 2 * B::BOXS;
   const int i = x0 + threadIdx.x;
-  if (i >= m.nx + 2) return;
+  if (i >= m.nx + 2) return true;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const HaloRule rule = halo_rule(VISCOSITY);
   const T cdx = m.celldx_t[i], cdx1 = m.celldx_t[i + 1];
@@ -131,6 +163,16 @@ __global__ void __launch_bounds__(256, 4) kt_viscosity(const __grid_constant__ M
     q_out[gidx(pitch, i, j)] = q;
     if (do_fold) fold_halo(q_out, m, rule, fold, i, j, q);
   }
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 4) kt_viscosity(const __grid_constant__ Maps maps, const T *__restrict__ d0, T *q_out, Mesh<T> m, int off,
+                                                    int fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  viscosity_tile(cx, reinterpret_cast<T *>(smraw), map_set(maps, 3), d0, q_out, m, off, blockIdx.x, blockIdx.y, fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -169,49 +211,62 @@ struct DtIn {
   const void *soundspeed, *viscosity, *density0;
 };
 
-// Staged: 0 xvel0, 1 yvel0; soundspeed, viscosity, density0 are read directly.
+// One calc_dt tile (64 x 16 cells); folds the tile's candidates into vmin.
+// Staged: ms 0 xvel0, 1 yvel0; soundspeed, viscosity, density0 are read directly.
+constexpr int DT_TY = 16;
+template <typename T> constexpr size_t dt_smem() { return 2 * Box1<T, DT_TY>::BOXS * sizeof(T); }
+
 template <typename T>
-__global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Maps maps, DtIn in, Mesh<T> m, int off, DtConsts k, int tiles_x,
-                                                  int ntiles, unsigned long long *dt_bits, int *err) {
-  constexpr int TY = 16;
+__device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, const Mesh<T> &m, int off,
+                                             const DtConsts &k, int bx, int by, double &vmin) {
+  constexpr int TY = DT_TY;
   using B = Box1<T, TY>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
   const T *U = sm, *V = sm + B::BOXS;
   const T *S = (const T *)in.soundspeed, *Q = (const T *)in.viscosity, *R = (const T *)in.density0;
   const int pitch = (int)m.pitch;
   constexpr int RPT = TY / 4;
-  double vmin = g_big;
-  unsigned phase = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
-    const int x0 = 2 + (t % tiles_x) * TILE_X, y0 = 2 + (t / tiles_x) * TY;
-    const int i = x0 + threadIdx.x;
-    // the directly read fields are loaded before the staging wait
-    T ss[RPT], qq[RPT], dd[RPT];
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  const int i = x0 + threadIdx.x;
+  // the directly read fields are loaded before the staging wait
+  T ss[RPT], qq[RPT], dd[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
+    const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
+    const int g = gidx(pitch, i, j);
+    ss[r] = in_mesh ? S[g] : T(0);
+    qq[r] = in_mesh ? Q[g] : T(0);
+    dd[r] = in_mesh ? R[g] : T(1);
+  }
+  if (!stage(cx, sm, ms, 2, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  if (i < m.nx + 2) {
+    const T dsx = m.celldx_t[i];
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
       const int j = y0 + threadIdx.y + 4 * r;
-      const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
-      const int g = gidx(pitch, i, j);
-      ss[r] = in_mesh ? S[g] : T(0);
-      qq[r] = in_mesh ? Q[g] : T(0);
-      dd[r] = in_mesh ? R[g] : T(1);
-    }
-    if (!stage_boxes_loop(sm, maps, 2, B::BOXS, B::BH, off + x0 - HALO, y0 - 1, &bar, phase, t == (int)blockIdx.x, err)) return;
-    if (i < m.nx + 2) {
-      const T dsx = m.celldx_t[i];
-#pragma unroll
-      for (int r = 0; r < RPT; ++r) {
-        const int j = y0 + threadIdx.y + 4 * r;
-        if (j >= m.ny + 2) break;
-        const int b = B::at(i, j, x0, y0);
-        const double c = (double)dt_value(ss[r], qq[r], dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1],
-                                          V[b + BOX_X], V[b + BOX_X + 1], dsx, m.celldy_t[j], k);
-        vmin = fmin(c, vmin); // fmin drops a NaN candidate, as the reference's fmin does
-      }
+      if (j >= m.ny + 2) break;
+      const int b = B::at(i, j, x0, y0);
+      const double c = (double)dt_value(ss[r], qq[r], dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1],
+                                        V[b + BOX_X], V[b + BOX_X + 1], dsx, m.celldy_t[j], k);
+      vmin = fmin(c, vmin); // fmin drops a NaN candidate, as the reference's fmin does
     }
   }
+  return true;
+}
+
+// Blocks loop over tiles; each keeps the minimum of its cells and folds it
+// into the result once.
+template <typename T>
+__global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Maps maps, DtIn in, Mesh<T> m, int off, DtConsts k, int tiles_x,
+                                                  int ntiles, unsigned long long *dt_bits, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  T *sm = reinterpret_cast<T *>(smraw);
+  TileCtx cx = tile_ctx(&bar, err);
+  const MapSet ms = map_set(maps, 2);
+  double vmin = g_big;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    if (!calc_dt_tile(cx, sm, ms, in, m, off, k, t % tiles_x, t / tiles_x, vmin)) return;
   block_min_to(vmin, dt_bits);
 }
 
@@ -260,16 +315,17 @@ struct PdvOut {
   void *density1, *energy1, *pressure, *soundspeed;
 };
 
-// Staged: 0 xvel0, 1 yvel0, [2 xvel1, 3 yvel1]; the cell fields are read directly.
+// One PdV tile (64 x 8 cells).
+// Staged: ms 0 xvel0, 1 yvel0, [2 xvel1, 3 yvel1]; the cell fields are read directly.
+constexpr int PDV_TY = 8;
+template <typename T> constexpr size_t pdv_smem() { return 4 * Box1<T, PDV_TY>::BOXS * sizeof(T); }
+
 template <typename T>
-__global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict, T dt,
-                                              int mode, T gm1, int fold, int *err) {
-  constexpr int TY = 8;
+__device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, const PdvIn &in, const PdvOut &out, const Mesh<T> &m, int off,
+                                         int predict, T dt, int mode, T gm1, int fold, int bx, int by) {
+  constexpr int TY = PDV_TY;
   using B = Box1<T, TY>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const int i = x0 + threadIdx.x;
   const int pitch = (int)m.pitch;
   constexpr int RPT = TY / 4;
@@ -286,9 +342,9 @@ __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps,
     rq[r] = in_mesh ? ((const T *)in.viscosity)[g] : T(0);
   }
   const int nf = predict ? 2 : 4;
-  if (!stage_boxes(sm, maps, nf, B::BOXS, B::BH, off + x0 - HALO, y0 - 1, &bar, err)) return;
+  if (!stage(cx, sm, ms, nf, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
   const T *U0 = sm, *V0 = sm + B::BOXS, *U1 = sm + 2 * B::BOXS, *V1 = sm + 3 * B::BOXS;
-  if (i >= m.nx + 2) return;
+  if (i >= m.nx + 2) return true;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const T cdx = m.celldx_t[i];
 #pragma unroll
@@ -324,24 +380,35 @@ __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps,
       ((T *)out.energy1)[g] = re[r];
     }
   }
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict, T dt,
+                                              int mode, T gm1, int fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  pdv_tile(cx, reinterpret_cast<T *>(smraw), map_set(maps, predict ? 2 : 4), in, out, m, off, predict, dt, mode, gm1, fold, blockIdx.x,
+           blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
 // accelerate: src/serial/accelerate.cpp:28-56, nodes [2, nx+2] x [2, ny+2].
 // fields: 0 density0, 1 pressure, 2 viscosity, 3 xvel0, 4 yvel0
-template <typename T>
-__global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Maps maps, T *u_out, T *v_out, Mesh<T> m, int off, T dt,
-                                                     int fold, int *err) {
-  constexpr int TY = 16;
+// One tile of TY node rows; the one-launch kernel uses TY = ACC_TY.
+constexpr int ACC_TY = 16;
+template <typename T, int TY> constexpr size_t acc_smem() { return 5 * Tile<TY>::BOX * sizeof(T); }
+
+template <typename T, int TY>
+__device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet &ms, T *u_out, T *v_out, const Mesh<T> &m, int off, T dt,
+                                                int fold, int bx, int by) {
   using C = Tile<TY>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  if (!stage_tiles(sm, maps, 5, C::BOX, off, x0, y0, &bar, err)) return;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  if (!stage(cx, sm, ms, 5, C::BOX, C::BH, off + x0 - HALO, y0 - HALO)) return false;
   const T *D0 = sm, *P = sm + C::BOX, *Q = sm + 2 * C::BOX, *U0 = sm + 3 * C::BOX, *V0 = sm + 4 * C::BOX;
   const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
-  if (i >= m.nx + 3) return;
+  if (i >= m.nx + 3) return true;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const int pitch = (int)m.pitch;
   const T halfdt = T(0.5) * dt;
@@ -369,6 +436,16 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
       fold_halo(v_out, m, halo_rule(YVEL1), fold, i, j, v);
     }
   }
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Maps maps, T *u_out, T *v_out, Mesh<T> m, int off, T dt,
+                                                     int fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  accelerate_tile<T, ACC_TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 5), u_out, v_out, m, off, dt, fold, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -376,19 +453,18 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 // With a fold, the extra row of x faces and column of y faces (overwritten
 // by update_halo) take their halo values.
 // fields: 0 xvel0, 1 yvel0, 2 xvel1, 3 yvel1
-template <typename T>
-__global__ void __launch_bounds__(256) kt_flux_calc(const __grid_constant__ Maps maps, T *fx_out, T *fy_out, Mesh<T> m, int off, T dt,
-                                                    int fold, int *err) {
-  constexpr int TY = 16;
+constexpr int FLUX_TY = 16;
+template <typename T, int TY> constexpr size_t flux_smem() { return 4 * Tile<TY>::BOX * sizeof(T); }
+
+template <typename T, int TY>
+__device__ __forceinline__ bool flux_calc_tile(TileCtx &cx, T *sm, const MapSet &ms, T *fx_out, T *fy_out, const Mesh<T> &m, int off, T dt,
+                                               int fold, int bx, int by) {
   using C = Tile<TY>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  if (!stage_tiles(sm, maps, 4, C::BOX, off, x0, y0, &bar, err)) return;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  if (!stage(cx, sm, ms, 4, C::BOX, C::BH, off + x0 - HALO, y0 - HALO)) return false;
   const T *U0 = sm, *V0 = sm + C::BOX, *U1 = sm + 2 * C::BOX, *V1 = sm + 3 * C::BOX;
   const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
-  if (i >= m.nx + 3) return;
+  if (i >= m.nx + 3) return true;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const int pitch = (int)m.pitch;
   const T cdx = m.celldx_t[i];
@@ -414,6 +490,16 @@ __global__ void __launch_bounds__(256) kt_flux_calc(const __grid_constant__ Maps
       if (do_fold) fold_halo(fy_out, m, halo_rule(VOL_FLUX_Y), fold, i, j, fy);
     }
   }
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kt_flux_calc(const __grid_constant__ Maps maps, T *fx_out, T *fy_out, Mesh<T> m, int off, T dt,
+                                                    int fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  flux_calc_tile<T, FLUX_TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 4), fx_out, fy_out, m, off, dt, fold, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -461,19 +547,16 @@ template <typename T, int DIR, int TY> struct CellLayout {
 };
 
 template <typename T, int DIR, int TY>
-__global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
-                                                     int fold, int *err) {
+__device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
+                                                int sweep, int fold, int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, YH = L::YH;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
   double *s_mf = reinterpret_cast<double *>(sm + 4 * L::BOXS);
   double *s_ef = s_mf + L::NF * LL;
   T *s_pv = reinterpret_cast<T *>(s_ef + L::NF * LL);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const int nf = (sweep == 1) ? 4 : (DIR == 1 ? 3 : 4); // sweep 2 of x needs no y fluxes
-  if (!stage_boxes(sm, maps, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH, &bar, err)) return;
+  if (!stage(cx, sm, ms, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH)) return false;
   const T *D1 = sm, *E1 = sm + L::BOXS, *VFX = sm + 2 * L::BOXS, *VFY = sm + 3 * L::BOXS;
   const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
@@ -573,6 +656,16 @@ __global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Map
       fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, enew);
     }
   }
+  return true;
+}
+
+template <typename T, int DIR, int TY>
+__global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
+                                                     int fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  advec_cell_tile<T, DIR, TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 4), out, m, off, sweep, fold, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -638,17 +731,14 @@ template <typename T, int DIR, int TY> struct MomLayout {
 };
 
 template <typename T, int DIR, int TY>
-__global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps maps, MomOut out, Mesh<T> m, int off, int vel_mask,
-                                                    int sweep, int fold, int *err) {
+__device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
+                                               int vel_mask, int sweep, int fold, int bx, int by) {
   using L = MomLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, NP = L::NP, YH = L::YH;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
   const int mom_sweep = DIR + 2 * (sweep - 1);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const int nf = mom_sweep <= 2 ? 5 : 4;
-  if (!stage_boxes(sm, maps, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH, &bar, err)) return;
+  if (!stage(cx, sm, ms, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH)) return false;
   const T *U1 = sm, *V1 = sm + L::BOXS, *D1 = sm + 2 * L::BOXS, *MF = sm + 3 * L::BOXS, *VFO = sm + 4 * L::BOXS;
   T *region = sm + 2 * L::BOXS;
   T *s_cm = region, *s_nf = s_cm + L::N_CM, *s_nmpre = s_nf + L::N_W, *s_mfu = s_nmpre + L::N_W, *s_mfv = s_mfu + L::N_W;
@@ -795,6 +885,16 @@ __global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps
       if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
     }
   }
+  return true;
+}
+
+template <typename T, int DIR, int TY>
+__global__ void __launch_bounds__(256) kt_advec_mom(const __grid_constant__ Maps maps, MomOut out, Mesh<T> m, int off, int vel_mask,
+                                                    int sweep, int fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  advec_mom_tile<T, DIR, TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 5), out, m, off, vel_mask, sweep, fold, blockIdx.x, blockIdx.y);
 }
 
 } // namespace cb

@@ -66,41 +66,4 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase, int *er
   return false;
 }
 
-// Stages the boxes of fields maps.m[0..nf) for the tile at (x0, y0) into
-// consecutive boxes of `box_elems` elements starting at `sm`.  Called by
-// every thread of the block; returns false in every thread if the copies
-// did not arrive within the wait limit.
-template <typename T>
-__device__ __forceinline__ bool stage_tiles(T *sm, const Maps &maps, int nf, int box_elems, int off, int x0, int y0,
-                                            uint64_t *bar, int *err) {
-  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
-  if (leader) mbar_init(bar, 1);
-  __syncthreads();
-  if (leader) {
-    mbar_expect_tx(bar, (unsigned)(nf * box_elems * sizeof(T)));
-    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * box_elems, &maps.m[f], off + x0 - HALO, y0 - HALO, bar);
-  }
-  bool ok = mbar_wait(bar, 0, err);
-  if (!ok) mbar_wait(bar, 0, nullptr); // give copies still in flight a second bounded wait before leaving
-  return __syncthreads_and(ok) != 0;
-}
-
-// Like stage_tiles, for boxes of BOX_X x bh elements whose first element is
-// tensor coordinate (xs, ys), placed `stride` elements apart in shared
-// memory (stride * sizeof(T) a multiple of 128 bytes).
-template <typename T>
-__device__ __forceinline__ bool stage_boxes(T *sm, const Maps &maps, int nf, int stride, int bh, int xs, int ys, uint64_t *bar,
-                                            int *err) {
-  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
-  if (leader) mbar_init(bar, 1);
-  __syncthreads();
-  if (leader) {
-    mbar_expect_tx(bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
-    for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, &maps.m[f], xs, ys, bar);
-  }
-  bool ok = mbar_wait(bar, 0, err);
-  if (!ok) mbar_wait(bar, 0, nullptr);
-  return __syncthreads_and(ok) != 0;
-}
-
 } // namespace cb

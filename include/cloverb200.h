@@ -143,6 +143,87 @@ int cb_get_stream(cb_chunk *c, void **stream);
 /* Number of kernels the library has launched for this chunk so far. */
 int cb_launch_count(const cb_chunk *c, long long *count);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble: many independent decks advanced by one persistent
+ * kernel launch.  No counterpart in the reference, whose driver runs one
+ * deck per process; each deck here follows exactly the per-chunk sequence
+ * of the calls above (the reference driver's, driver/start.cpp:43-138 and
+ * driver/hydro.cpp:46-223) with its own gamma, states, dt controls and end
+ * time, and its fields end bit-identical to that sequence's.
+ * ------------------------------------------------------------------------ */
+typedef struct cb_batch cb_batch;
+
+#define CB_DECK_MAX_STATES 8
+
+/* One deck: mesh, domain, gamma, states (index 0 the background; extents
+ * already nudged as driver/read_input.cpp:268-276 does) and the controls of
+ * driver/definitions.h:227-256.  nx and ny must be at least 8. */
+typedef struct {
+  int nx, ny;
+  double xmin, ymin, xmax, ymax;
+  double gamma;
+  int nstates;
+  cb_state states[CB_DECK_MAX_STATES];
+  double dtinit, dtmin, dtmax, dtrise;
+  double dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;
+  double end_time;
+  int end_step;
+  int summary_frequency;
+} cb_deck;
+
+/* Deck status after a run. */
+enum { CB_DECK_PENDING = 0, CB_DECK_DONE = 1, CB_DECK_SMALL_DT = 2, CB_DECK_STAGE_FAIL = 3, CB_DECK_SYNC_FAIL = 4 };
+
+/* How the persistent launch is laid out.  A deck of c cells runs on a lane of
+ * w CTAs, w the power of two >= c / cells_per_cta (at most max_lane_width
+ * and the deck's tile count); lanes of each width get a share of the grid in
+ * proportion to their decks' estimated work, and decks go to the lane with
+ * the least work so far, largest first.  ctas_per_sm (0 = as many as fit)
+ * sets the grid; variant picks the tile shapes (0: 64 x 16 tiles for
+ * accelerate and flux_calc, 1: 64 x 8 tiles and more CTAs per SM). */
+typedef struct {
+  int cells_per_cta;
+  int max_lane_width;
+  int ctas_per_sm;
+  int variant;
+} cb_batch_schedule;
+
+typedef struct {
+  cb_batch_schedule schedule;
+  int lanes, ctas;
+  float ms; /* mean time of one whole-ensemble run */
+} cb_batch_trial;
+
+/* Allocates every deck's fields (one pool on `device`), its geometry
+ * (src/serial/initialise_chunk.cpp:30-85) and tensor maps, and a default
+ * schedule. */
+int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device, cb_batch **out);
+int cb_batch_destroy(cb_batch *b);
+/* Lays the launch out (see cb_batch_schedule) and captures it in a CUDA graph. */
+int cb_batch_set_schedule(cb_batch *b, const cb_batch_schedule *s);
+int cb_batch_get_schedule(const cb_batch *b, cb_batch_schedule *s, int *lanes, int *ctas);
+/* Runs the ensemble once per candidate schedule (plus a warm-up) and keeps the
+ * fastest; trials[0..*ntrials) receives every candidate's timing. */
+int cb_batch_autotune(cb_batch *b, int repeats, cb_batch_trial *trials, int max_trials, int *ntrials, cb_batch_schedule *best);
+/* Enqueues one run of the whole ensemble from t = 0 (one graph launch: the
+ * descriptors are reset and the persistent kernel advances every deck to its
+ * end) and returns without waiting. */
+int cb_batch_run(cb_batch *b);
+/* Waits for the run and checks the launch; *ms receives its device time. */
+int cb_batch_synchronize(cb_batch *b, float *ms);
+/* Results of deck `deck` of the last run: status (CB_DECK_*), steps, time reached, summary records. */
+int cb_batch_deck_result(cb_batch *b, int deck, int *status, int *steps, double *time, int *nsummaries);
+/* Summary records (step, time, volume, mass, internal energy, kinetic energy,
+ * pressure*volume: 7 doubles each) of deck `deck`; *count = records written. */
+int cb_batch_read_summaries(cb_batch *b, int deck, double *out, int max_records, int *count);
+/* dt of every step of deck `deck`. */
+int cb_batch_read_dt(cb_batch *b, int deck, double *out, int max_steps, int *count);
+/* Final field of deck `deck`, as cb_read_field. */
+int cb_batch_read_field(cb_batch *b, int deck, int field, double *host, size_t n, int layout);
+int cb_batch_get_stream(cb_batch *b, void **stream);
+/* Kernels the batch has launched so far. */
+int cb_batch_launch_count(const cb_batch *b, long long *count);
+
 /* The field summary of cb_field_summary (ideal_gas, then the five sums) over
  * FP64 device arrays the caller owns, allocating no memory: for callers that
  * must not allocate device memory where they need the summary (their device
