@@ -11,3 +11,4 @@ from .chunk import (FIELD_ID, FIELD_NAMES, FP32, FP64, GEOM_ID, GEOM_NAMES, Chun
 from .deck import Deck, State, benchmark_deck, format_deck, nudged, parse_deck, read_deck  # noqa: F401
 from .hydro import HydroRun, Summary  # noqa: F401
 from .batch import Batch, ensemble_deck, ensemble_decks  # noqa: F401
+from .adjoint import Adjoint, kinetic_energy_function  # noqa: F401

@@ -34,7 +34,10 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_field_summary_noalloc",
            "cb_batch_create", "cb_batch_destroy", "cb_batch_set_schedule", "cb_batch_get_schedule", "cb_batch_autotune",
            "cb_batch_run", "cb_batch_synchronize", "cb_batch_deck_result", "cb_batch_read_summaries", "cb_batch_read_dt",
-           "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count"]
+           "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count",
+           "cb_adjoint_create", "cb_adjoint_destroy", "cb_adjoint_set_initial", "cb_adjoint_set_checkpoint_interval",
+           "cb_adjoint_forward", "cb_adjoint_dt", "cb_adjoint_gradient", "cb_adjoint_tangent", "cb_adjoint_read_tangent",
+           "cb_adjoint_read_field", "cb_adjoint_stats"]
 
 
 class CloverError(RuntimeError):

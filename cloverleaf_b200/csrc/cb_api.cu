@@ -19,8 +19,6 @@
 #include "cb_ops.h"
 #include "cb_tma.cuh"
 
-struct cb_chunk : cb::Chunk {};
-
 using namespace cb;
 
 namespace {

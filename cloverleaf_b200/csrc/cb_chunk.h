@@ -72,3 +72,6 @@ struct Chunk {
 };
 
 } // namespace cb
+
+// The C ABI's opaque handle (include/cloverb200.h) is the chunk itself.
+struct cb_chunk : cb::Chunk {};

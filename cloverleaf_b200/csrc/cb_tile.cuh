@@ -396,6 +396,20 @@ __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps,
 // ---------------------------------------------------------------------------
 // accelerate: src/serial/accelerate.cpp:28-56, nodes [2, nx+2] x [2, ny+2].
 // fields: 0 density0, 1 pressure, 2 viscosity, 3 xvel0, 4 yvel0
+// Velocity of node (i, j) (src/serial/accelerate.cpp:38-52): cells mm =
+// (i-1, j-1), m0 = (i-1, j), 00 = (i, j), 0m = (i, j-1); xa = xarea(i, j),
+// xa_m = xarea(i, j-1), ya = yarea(i, j), ya_m = yarea(i-1, j).
+template <typename T>
+__device__ __forceinline__ void accel_value(T halfdt, T vol_mm, T vol_m0, T vol_00, T vol_0m, T xa, T xa_m, T ya, T ya_m, T d_mm, T d_m0,
+                                            T d_00, T d_0m, T p_00, T p_m0, T p_0m, T p_mm, T q_00, T q_m0, T q_0m, T q_mm, T u0, T v0, T &u,
+                                            T &v) {
+  T stepbymass_s = (halfdt) / (((d_mm * vol_mm + d_m0 * vol_m0 + d_00 * vol_00 + d_0m * vol_0m) * T(0.25)));
+  u = u0 - stepbymass_s * (xa * (p_00 - p_m0) + xa_m * (p_0m - p_mm));
+  v = v0 - stepbymass_s * (ya * (p_00 - p_0m) + ya_m * (p_m0 - p_mm));
+  u = u - stepbymass_s * (xa * (q_00 - q_m0) + xa_m * (q_0m - q_mm));
+  v = v - stepbymass_s * (ya * (q_00 - q_0m) + ya_m * (q_m0 - q_mm));
+}
+
 // One tile of TY node rows; the one-launch kernel uses TY = ACC_TY.
 constexpr int ACC_TY = 16;
 template <typename T, int TY> constexpr size_t acc_smem() { return 5 * Tile<TY>::BOX * sizeof(T); }
@@ -421,13 +435,9 @@ __device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet
     const T cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
     const T vol_mm = cdxm * cdym, vol_m0 = cdxm * cdy, vol_00 = cdx * cdy, vol_0m = cdx * cdym;
     const int c00 = b, cm0 = b - 1, c0m = b - BOX_X, cmm = b - BOX_X - 1;
-    T stepbymass_s = (halfdt) / (((D0[cmm] * vol_mm + D0[cm0] * vol_m0 + D0[c00] * vol_00 + D0[c0m] * vol_0m) * T(0.25)));
-    const T xa = cdy, xa_m = cdym; // xarea(i, j), xarea(i, j-1)
-    const T ya = cdx, ya_m = cdxm; // yarea(i, j), yarea(i-1, j)
-    T u = U0[c00] - stepbymass_s * (xa * (P[c00] - P[cm0]) + xa_m * (P[c0m] - P[cmm]));
-    T v = V0[c00] - stepbymass_s * (ya * (P[c00] - P[c0m]) + ya_m * (P[cm0] - P[cmm]));
-    u = u - stepbymass_s * (xa * (Q[c00] - Q[cm0]) + xa_m * (Q[c0m] - Q[cmm]));
-    v = v - stepbymass_s * (ya * (Q[c00] - Q[c0m]) + ya_m * (Q[cm0] - Q[cmm]));
+    T u, v;
+    accel_value(halfdt, vol_mm, vol_m0, vol_00, vol_0m, cdy, cdym, cdx, cdxm, D0[cmm], D0[cm0], D0[c00], D0[c0m], P[c00], P[cm0], P[c0m],
+                P[cmm], Q[c00], Q[cm0], Q[c0m], Q[cmm], U0[c00], V0[c00], u, v);
     const int g = gidx(pitch, i, j);
     u_out[g] = u;
     v_out[g] = v;
@@ -453,6 +463,13 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 // With a fold, the extra row of x faces and column of y faces (overwritten
 // by update_halo) take their halo values.
 // fields: 0 xvel0, 1 yvel0, 2 xvel1, 3 yvel1
+// Volume flux through a face (src/serial/flux_calc.cpp:33-40): width is
+// xarea (celldy) for x faces, yarea (celldx) for y faces; a0, a1 the level-0
+// velocities of the face's two nodes, b0, b1 the level-1 ones.
+template <typename T> __device__ __forceinline__ T flux_value(T dt, T width, T a0, T a1, T b0, T b1) {
+  return T(0.25) * dt * width * (a0 + a1 + b0 + b1);
+}
+
 constexpr int FLUX_TY = 16;
 template <typename T, int TY> constexpr size_t flux_smem() { return 4 * Tile<TY>::BOX * sizeof(T); }
 
@@ -473,8 +490,8 @@ __device__ __forceinline__ bool flux_calc_tile(TileCtx &cx, T *sm, const MapSet 
     const int j = y0 + threadIdx.y + 4 * r, ly = HALO + threadIdx.y + 4 * r;
     if (j >= m.ny + 3) break;
     const int b = ly * BOX_X + lx;
-    T fx = T(0.25) * dt * m.celldy_t[j] * (U0[b] + U0[b + BOX_X] + U1[b] + U1[b + BOX_X]);
-    T fy = T(0.25) * dt * cdx * (V0[b] + V0[b + 1] + V1[b] + V1[b + 1]);
+    T fx = flux_value(dt, m.celldy_t[j], U0[b], U0[b + BOX_X], U1[b], U1[b + BOX_X]);
+    T fy = flux_value(dt, cdx, V0[b], V0[b + 1], V1[b], V1[b + 1]);
     const int g = gidx(pitch, i, j);
     if (!fold) {
       fx_out[g] = fx;
@@ -516,6 +533,48 @@ __device__ __forceinline__ T cell_limiter_value(T sigma, T sigma3, T sigma4, T d
     return (T(1.0) - sigma) * wind * fmin(fmin(fabs(diffuw), fabs(diffdw)), one_by_six * (sigma3 * fabs(diffuw) + sigma4 * fabs(diffdw)));
   }
   return T(0.0);
+}
+
+// pre_vol of a cell (src/serial/advec_cell.cpp:42-61 / :134-153): sweep 1
+// adds both directions' flux differences (the sweep's first), sweep 2 only
+// the sweep direction's.
+template <typename T> __device__ __forceinline__ T cell_pre_vol1(T vol, T a_lo, T a_hi, T b_lo, T b_hi) {
+  return vol + (a_hi - a_lo + b_hi - b_lo);
+}
+template <typename T> __device__ __forceinline__ T cell_pre_vol2(T vol, T a_lo, T a_hi) { return vol + a_hi - a_lo; }
+
+// Mass flux through a face and the energy the flux carries per unit mass
+// (:63-113 / :155-205): flux the face's volume flux, donor/upwind/downwind
+// the cells the flux's sign selects (d* densities, e* energies), pre_vol_d
+// the donor's pre_vol, vdx_f / vdx_dif the vertex widths at the face and at
+// the cell the limiter's ratio uses.  The energy flux is mass_flux * e_adv.
+template <typename T>
+__device__ __forceinline__ void cell_face_value(T flux, T pre_vol_d, T vdx_f, T vdx_dif, T dd, T du, T dw, T ed, T eu, T ew, T &mass_flux,
+                                                T &e_adv) {
+  T sigmat = lim_div(fabs(flux), pre_vol_d);
+  T sigma3 = (T(1.0) + sigmat) * lim_div(vdx_f, vdx_dif);
+  T sigma4 = T(2.0) - sigmat;
+  T sigmav = sigmat;
+  T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
+  mass_flux = flux * (dd + limiter);
+  T sigmam = lim_div(fabs(mass_flux), dd * pre_vol_d);
+  limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
+  e_adv = ed + limiter;
+}
+
+// The cell's update (:117-129 / :209-221) in the precision of its mass and
+// energy accumulation: mf/ef the mass and energy fluxes of its low and high
+// faces, vf the volume fluxes.
+template <typename S>
+__device__ __forceinline__ void cell_update_value(S d1, S e1, S pre_vol, S mf_lo, S mf_hi, S ef_lo, S ef_hi, S vf_lo, S vf_hi, S &dnew,
+                                                  S &enew) {
+  S pre_mass_s = d1 * pre_vol;
+  S post_mass_s = pre_mass_s + mf_lo - mf_hi;
+  S ener_s = e1 * pre_mass_s + ef_lo - ef_hi;
+  S advec_vol_s = pre_vol + vf_lo - vf_hi;
+  S post_ener_s = (ener_s) / (post_mass_s);
+  dnew = (post_mass_s) / (advec_vol_s);
+  enew = post_ener_s;
 }
 
 struct CellOut {
@@ -575,9 +634,9 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     const T vol = m.celldx_t[i] * m.celldy_t[j];
     T pv;
     if (DIR == 1) {
-      pv = sweep == 1 ? vol + (VFX[b + 1] - VFX[b] + VFY[b + BOX_X] - VFY[b]) : vol + VFX[b + 1] - VFX[b];
+      pv = sweep == 1 ? cell_pre_vol1(vol, VFX[b], VFX[b + 1], VFY[b], VFY[b + BOX_X]) : cell_pre_vol2(vol, VFX[b], VFX[b + 1]);
     } else {
-      pv = sweep == 1 ? vol + (VFY[b + BOX_X] - VFY[b] + VFX[b + 1] - VFX[b]) : vol + VFY[b + BOX_X] - VFY[b];
+      pv = sweep == 1 ? cell_pre_vol1(vol, VFY[b], VFY[b + BOX_X], VFX[b], VFX[b + 1]) : cell_pre_vol2(vol, VFY[b], VFY[b + BOX_X]);
     }
     s_pv[L::pv(p, l)] = pv;
   }
@@ -602,18 +661,10 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     }
     const int bd = b + (donor - f) * ST, bu = b + (upwind - f) * ST, bw = b + (downwind - f) * ST;
     const T pre_vol_d = s_pv[L::pv(donor - a0 + 1, l)];
-    T sigmat = lim_div(fabs(flux), pre_vol_d);
-    T sigma3 = (T(1.0) + sigmat) * lim_div((T)vdx[f], (T)vdx[dif]);
-    T sigma4 = T(2.0) - sigmat;
-    T sigmav = sigmat;
-    const T dd = D1[bd], du = D1[bu], dw = D1[bw];
-    T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
-    T mass_flux = flux * (dd + limiter);
-    T sigmam = lim_div(fabs(mass_flux), dd * pre_vol_d);
-    const T ed = E1[bd], eu = E1[bu], ew = E1[bw];
-    limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
+    T mass_flux, e_adv;
+    cell_face_value(flux, pre_vol_d, (T)vdx[f], (T)vdx[dif], D1[bd], D1[bu], D1[bw], E1[bd], E1[bu], E1[bw], mass_flux, e_adv);
     s_mf[L::fx(p, l)] = (double)mass_flux;
-    s_ef[L::fx(p, l)] = (double)mass_flux * (double)(ed + limiter);
+    s_ef[L::fx(p, l)] = (double)mass_flux * (double)(e_adv);
     T *mf = (T *)out.mass_flux;
     const bool halo_face = fold && f == na + 3; // with a fold, face na+3 takes its halo value
     if (!halo_face) mf[gidx(pitch, i, j)] = mass_flux;
@@ -633,16 +684,17 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     const double ef_lo = s_ef[L::fx(p, l)], ef_hi = s_ef[L::fx(p + 1, l)];
     const T vf_lo = DIR == 1 ? VFX[b] : VFY[b];
     const T vf_hi = DIR == 1 ? VFX[b + 1] : VFY[b + BOX_X];
-    double pre_mass_s = (double)D1[b] * (double)pre_vol;
-    double post_mass_s = pre_mass_s + mf_lo - mf_hi;
-    double ener_s = (double)E1[b] * pre_mass_s + ef_lo - ef_hi;
-    double advec_vol_s = (double)pre_vol + (double)vf_lo - (double)vf_hi;
     T dnew, enew;
     if constexpr (sizeof(T) == sizeof(double)) {
-      const double post_ener_s = (ener_s) / (post_mass_s);
-      dnew = (T)((post_mass_s) / (advec_vol_s));
-      enew = (T)post_ener_s;
+      double dn, en;
+      cell_update_value<double>(D1[b], E1[b], pre_vol, mf_lo, mf_hi, ef_lo, ef_hi, vf_lo, vf_hi, dn, en);
+      dnew = (T)dn;
+      enew = (T)en;
     } else {
+      double pre_mass_s = (double)D1[b] * (double)pre_vol;
+      double post_mass_s = pre_mass_s + mf_lo - mf_hi;
+      double ener_s = (double)E1[b] * pre_mass_s + ef_lo - ef_hi;
+      double advec_vol_s = (double)pre_vol + (double)vf_lo - (double)vf_hi;
       // FP32 form: the sums above stay FP64; the quotients are stored in
       // FP32, so they are formed in FP32 from the rounded sums
       dnew = (T)post_mass_s / (T)advec_vol_s;
@@ -698,6 +750,38 @@ __device__ __forceinline__ T mom_limiter_value(T vdiffuw, T vdiffdw, T sigma, T 
     limiter = wind * fmin(fmin(lim_div(width * (lim_div((T(2.0) - sigma) * adw, width) + lim_div((T(1.0) + sigma) * auw, dx_dif)), T(6.0)), auw), adw);
   }
   return limiter;
+}
+
+// The sum of four terms scaled by 0.25: node flux (four mass fluxes,
+// src/serial/advec_mom.cpp:84-88 / :156-160) and node_mass_post (four cell
+// masses density1 * post_vol, :93-96 / :165-168).
+template <typename T> __device__ __forceinline__ T quarter_sum(T a, T b, T c, T d) { return T(0.25) * (a + b + c + d); }
+
+// post_vol of a cell (:42-77): mom_sweep 1 vol + the y flux difference, 2
+// vol + the x flux difference, 3 and 4 vol.
+template <typename T> __device__ __forceinline__ T mom_post_vol(int mom_sweep, T vol, T lo, T hi) {
+  return mom_sweep <= 2 ? vol + hi - lo : vol;
+}
+
+// node_mass_pre (:97-102 / :169-174) from node_mass_post and the node fluxes
+// on the node's low and high side.
+template <typename T> __device__ __forceinline__ T mom_node_mass_pre(T post, T nf_lo, T nf_hi) { return post - nf_lo + nf_hi; }
+
+// sigma of a node's momentum flux (:120 / :192).
+template <typename T> __device__ __forceinline__ T mom_sigma(T node_flux, T node_mass_pre_donor) {
+  return lim_div(fabs(node_flux), node_mass_pre_donor);
+}
+
+// Momentum flux of one velocity component (:121-133 / :193-205): vd, vu, vw
+// the velocities at the donor, upwind and downwind nodes.
+template <typename T> __device__ __forceinline__ T mom_flux_value(T sigma, T node_flux, T width, T dx_dif, T vd, T vu, T vw) {
+  T lim = mom_limiter_value(vd - vu, vw - vd, sigma, width, dx_dif);
+  return (vd + (T(1.0) - sigma) * lim) * node_flux;
+}
+
+// Velocity update (:139-144 / :211-216).
+template <typename T> __device__ __forceinline__ T mom_update_value(T vel, T nm_pre, T nm_post, T mf_lo, T mf_hi) {
+  return (vel * nm_pre + mf_lo - mf_hi) / (nm_post);
 }
 
 struct MomOut {
@@ -767,7 +851,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
         const int b = bidx(i, j);
         const T vol = m.celldx_t[i] * m.celldy_t[j];
         // post_vol (:42-77): mom_sweep 1 vol + vfy difference, 2 vol + vfx difference, 3/4 vol
-        const T pv = mom_sweep == 1 ? vol + VFO[b + BOX_X] - VFO[b] : mom_sweep == 2 ? vol + VFO[b + 1] - VFO[b] : vol;
+        const T pv = mom_sweep == 1 ? mom_post_vol(1, vol, VFO[b], VFO[b + BOX_X]) : mom_sweep == 2 ? mom_post_vol(2, vol, VFO[b], VFO[b + 1]) : vol;
         v = D1[b] * pv;
       }
     }
@@ -784,7 +868,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
       if (line < nlmax + 3 && a >= 0 && a <= na + 3) {
         const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
         // (:84-88 / :156-160) dir 1: mf(a, j-1) + mf(a, j) + mf(a+1, j-1) + mf(a+1, j); dir 2: mf(i-1, a) + mf(i, a) + mf(i-1, a+1) + mf(i, a+1)
-        v = T(0.25) * (MF[b - SL] + MF[b] + MF[b + ST - SL] + MF[b + ST]);
+        v = quarter_sum(MF[b - SL], MF[b], MF[b + ST - SL], MF[b + ST]);
       }
     }
     r_nf[k] = v;
@@ -812,9 +896,8 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
 
   // node_mass_post (:93-96 / :165-168) of node (p, l): cells (i, j-1), (i, j), (i-1, j-1), (i-1, j)
   auto node_mass_post = [&](int p, int l) -> T {
-    if (DIR == 1)
-      return T(0.25) * (s_cm[L::cm(p, l)] + s_cm[L::cm(p, l + 1)] + s_cm[L::cm(p - 1, l)] + s_cm[L::cm(p - 1, l + 1)]);
-    return T(0.25) * (s_cm[L::cm(p - 1, l + 1)] + s_cm[L::cm(p, l + 1)] + s_cm[L::cm(p - 1, l)] + s_cm[L::cm(p, l)]);
+    if (DIR == 1) return quarter_sum(s_cm[L::cm(p, l)], s_cm[L::cm(p, l + 1)], s_cm[L::cm(p - 1, l)], s_cm[L::cm(p - 1, l + 1)]);
+    return quarter_sum(s_cm[L::cm(p - 1, l + 1)], s_cm[L::cm(p, l + 1)], s_cm[L::cm(p - 1, l)], s_cm[L::cm(p, l)]);
   };
 
   // (2) node_mass_pre (:97-102 / :169-174) over positions 1 .. LA+2
@@ -824,7 +907,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
     p += 1;
     const int a = a0 - 2 + p, line = l0 + l;
     T nmpre = T(1.0);
-    if (line < nlmax + 3 && a >= 1 && a <= na + 3) nmpre = node_mass_post(p, l) - s_nf[L::w(p - 1, l)] + s_nf[L::w(p, l)];
+    if (line < nlmax + 3 && a >= 1 && a <= na + 3) nmpre = mom_node_mass_pre(node_mass_post(p, l), s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]);
     s_nmpre[L::w(p, l)] = nmpre;
   }
   __syncthreads();
@@ -844,21 +927,13 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
     } else {
       upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
     }
-    const T sigma = lim_div(fabs(nfv), s_nmpre[L::w(p + (donor - a), l)]);
+    const T sigma = mom_sigma(nfv, s_nmpre[L::w(p + (donor - a), l)]);
     const T width = celld[a];
     const T dxd = celld[dif];
     const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
     const int bd = b + (donor - a) * ST, bu = b + (upwind - a) * ST, bw = b + (downwind - a) * ST;
-    if (vel_mask & 1) {
-      const T vd = U1[bd];
-      T lim = mom_limiter_value(vd - U1[bu], U1[bw] - vd, sigma, width, dxd);
-      s_mfu[L::w(p, l)] = (vd + (T(1.0) - sigma) * lim) * nfv;
-    }
-    if (vel_mask & 2) {
-      const T vd = V1[bd];
-      T lim = mom_limiter_value(vd - V1[bu], V1[bw] - vd, sigma, width, dxd);
-      s_mfv[L::w(p, l)] = (vd + (T(1.0) - sigma) * lim) * nfv;
-    }
+    if (vel_mask & 1) s_mfu[L::w(p, l)] = mom_flux_value(sigma, nfv, width, dxd, U1[bd], U1[bu], U1[bw]);
+    if (vel_mask & 2) s_mfv[L::w(p, l)] = mom_flux_value(sigma, nfv, width, dxd, V1[bd], V1[bu], V1[bw]);
   }
   __syncthreads();
 
@@ -875,12 +950,12 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
     const T nmpre = s_nmpre[L::w(p, l)], nmpost = node_mass_post(p, l);
     const int g = gidx(pitch, i, j);
     if (vel_mask & 1) {
-      T v = (U1[b] * nmpre + s_mfu[L::w(p - 1, l)] - s_mfu[L::w(p, l)]) / (nmpost);
+      T v = mom_update_value(U1[b], nmpre, nmpost, s_mfu[L::w(p - 1, l)], s_mfu[L::w(p, l)]);
       ((T *)out.xvel1)[g] = v;
       if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
     }
     if (vel_mask & 2) {
-      T v = (V1[b] * nmpre + s_mfv[L::w(p - 1, l)] - s_mfv[L::w(p, l)]) / (nmpost);
+      T v = mom_update_value(V1[b], nmpre, nmpost, s_mfv[L::w(p - 1, l)], s_mfv[L::w(p, l)]);
       ((T *)out.yvel1)[g] = v;
       if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
     }

@@ -224,6 +224,51 @@ int cb_batch_get_stream(cb_batch *b, void **stream);
 /* Kernels the batch has launched so far. */
 int cb_batch_launch_count(const cb_batch *b, long long *count);
 
+/* ------------------------------------------------------------------------
+ * Adjoint: the gradient of the final kinetic energy (field_summary's ke
+ * after the last step) with respect to the initial interior density0 and
+ * energy0 of every cell and to gamma, with the dt sequence of the forward
+ * run held fixed.  No counterpart in the reference.  FP64 only.  The
+ * forward run is the plain path above (the driver's call order); the
+ * reverse sweep runs hand-written adjoint kernels of every phase over
+ * checkpoints of the level-0 state every K steps (K = ceil(sqrt(steps))
+ * unless set), re-running each segment and each step forward as it goes.
+ * ------------------------------------------------------------------------ */
+typedef struct cb_adjoint cb_adjoint;
+
+/* A problem from a deck (mesh, domain, states, dt controls; nx, ny >= 8).
+ * The initial state is the deck's until cb_adjoint_set_initial replaces it. */
+int cb_adjoint_create(const cb_deck *deck, int device, cb_adjoint **out);
+int cb_adjoint_destroy(cb_adjoint *a);
+/* Initial interior density0 and energy0 (nx * ny values each, x fastest)
+ * and gamma; the halos follow from the interior as the driver's start
+ * (driver/start.cpp:103-118) makes them. */
+int cb_adjoint_set_initial(cb_adjoint *a, const double *density0, const double *energy0, double gamma);
+/* Steps between checkpoints (0: ceil(sqrt(steps))). */
+int cb_adjoint_set_checkpoint_interval(cb_adjoint *a, int k);
+/* Forward run of `steps` steps from the initial state.  dt NULL: each step's
+ * dt comes from calc_dt and the driver's clamp (driver/timestep.cpp:75-96)
+ * and is recorded; else the given sequence is used.  *ke receives the final
+ * kinetic energy. */
+int cb_adjoint_forward(cb_adjoint *a, int steps, const double *dt, double *ke);
+/* The last forward run's dt sequence. */
+int cb_adjoint_dt(const cb_adjoint *a, double *out, int max_steps, int *count);
+/* Reverse sweep of the last forward run: dKE/d density0, dKE/d energy0
+ * (nx * ny each, x fastest; either may be NULL) and dKE/d gamma. */
+int cb_adjoint_gradient(cb_adjoint *a, double *g_density0, double *g_energy0, double *g_gamma);
+/* Tangent-linear run of the last forward run's map in the direction
+ * (d_density0, d_energy0, d_gamma): *ke the final kinetic energy, *dke its
+ * directional derivative. */
+int cb_adjoint_tangent(cb_adjoint *a, const double *d_density0, const double *d_energy0, double d_gamma, double *ke, double *dke);
+/* Final field of the last tangent run: which 0 its values (the plain
+ * path's), 1 its tangents; n = the field's extent as cb_get_extent. */
+int cb_adjoint_read_tangent(cb_adjoint *a, int field, int which, double *host, size_t n);
+/* A field of the primal chunk as it stands (cb_read_field, x fastest). */
+int cb_adjoint_read_field(cb_adjoint *a, int field, double *host, size_t n);
+/* Checkpoint interval and count of the last forward run, steps re-run by
+ * the last reverse sweep, and the device memory the adjoint holds. */
+int cb_adjoint_stats(const cb_adjoint *a, int *checkpoint_interval, int *checkpoints, long long *recomputed_steps, size_t *device_bytes);
+
 /* The field summary of cb_field_summary (ideal_gas, then the five sums) over
  * FP64 device arrays the caller owns, allocating no memory: for callers that
  * must not allocate device memory where they need the summary (their device
