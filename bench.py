@@ -44,6 +44,13 @@ PHASE_ARRAYS = {"ideal_gas": 4, "viscosity": 5, "calc_dt": 8, "pdv_predict": 11 
 STEP_ARRAYS = 105  # the step's phases, ideal_gas .. reset_field
 
 
+def _plain(o):
+    """numpy scalars in the JSON line as plain numbers."""
+    if hasattr(o, "item"):
+        return o.item()
+    raise TypeError(f"not JSON serialisable: {type(o).__name__}")
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -285,6 +292,100 @@ def batch_leg(n_decks, seq_sample):
     return out
 
 
+def ke_exact(adj, dk):
+    """The final kinetic energy of an Adjoint's primal chunk as an exactly
+    rounded sum (math.fsum) of the per-cell terms of field_summary
+    (src/serial/field_summary.cpp:70-90), so that finite differences of it
+    carry no summation-order noise."""
+    import math
+    import numpy as np
+    nx, ny = dk.x_cells, dk.y_cells
+    d = adj.read_field("density0")[2:ny + 2, 2:nx + 2]
+    u = adj.read_field("xvel0")
+    v = adj.read_field("yvel0")
+    vsq = np.zeros((ny, nx))
+    for kv in (0, 1):
+        for jv in (0, 1):
+            uu, vv = u[2 + kv:ny + 2 + kv, 2 + jv:nx + 2 + jv], v[2 + kv:ny + 2 + kv, 2 + jv:nx + 2 + jv]
+            vsq = vsq + 0.25 * (uu * uu + vv * vv)
+    vol = ((dk.xmax - dk.xmin) / nx) * ((dk.ymax - dk.ymin) / ny)
+    return math.fsum(((vol * d) * 0.5 * vsq).ravel())
+
+
+def adjoint_leg(n=480, steps=200, fd_cells=64, hs=(1e-6, 1e-4)):
+    """The adjoint run: the benchmark layout at n x n with a seeded +-5%
+    uniform perturbation of every cell's initial density and energy, `steps`
+    steps; the gradient of the final kinetic energy by the reverse sweep,
+    checked against the tangent-linear run (dot-product test, two seeded
+    directions) and against central finite differences of the exactly summed
+    kinetic energy at `fd_cells` seeded cells (and gamma), with the forward
+    run's dt sequence held fixed, at step h = 1e-6 and, for comparison, 1e-4."""
+    import numpy as np
+    import torch
+    from cloverleaf_b200 import Adjoint, benchmark_deck, nudged
+    dk = nudged(benchmark_deck(n, end_step=steps))
+    adj = Adjoint(dk, device=torch.cuda.current_device())
+    rng = np.random.default_rng(0xAD7)
+    rho = adj.read_field("density0")[2:-2, 2:-2] * (1.0 + rng.uniform(-0.05, 0.05, (n, n)))
+    e = adj.read_field("energy0")[2:-2, 2:-2] * (1.0 + rng.uniform(-0.05, 0.05, (n, n)))
+    adj.set_initial(rho, e, 1.4)
+    t0 = time.perf_counter()
+    ke = adj.forward(steps)
+    t_fwd = time.perf_counter() - t0
+    dts = adj.dt()
+    t0 = time.perf_counter()
+    gr, ge, gg = adj.gradient()
+    t_rev = time.perf_counter() - t0
+    st = adj.stats()
+    dots = []
+    t_tan = 0.0
+    for k in range(2):
+        dr, de, dg = rng.standard_normal((n, n)), rng.standard_normal((n, n)), float(rng.standard_normal())
+        t0 = time.perf_counter()
+        _, dke = adj.tangent(dr, de, dg)
+        t_tan = time.perf_counter() - t0
+        lhs = float((gr * dr).sum() + (ge * de).sum() + gg * dg)
+        scale = float(np.abs(gr * dr).sum() + np.abs(ge * de).sum() + abs(gg * dg))
+        dots.append(abs(lhs - dke) / scale)
+    cells = [(int(rng.integers(n)), int(rng.integers(n))) for _ in range(fd_cells)]
+    gmax = max(float(np.abs(gr).max()), float(np.abs(ge).max()))
+    fd = {}
+    t0 = time.perf_counter()
+    for h in hs:
+        errs = []
+        for (j, i) in cells:
+            for which, g in (("rho", gr), ("e", ge)):
+                vals = []
+                for s in (1.0, -1.0):
+                    r2, e2 = rho.copy(), e.copy()
+                    (r2 if which == "rho" else e2)[j, i] += s * h
+                    adj.set_initial(r2, e2, 1.4)
+                    adj.forward(steps, dts)
+                    vals.append(ke_exact(adj, dk))
+                d = (vals[0] - vals[1]) / (2 * h)
+                errs.append(abs(d - g[j, i]) / max(abs(g[j, i]), 1e-6 * gmax))
+        vals = []
+        for s in (1.0, -1.0):
+            adj.set_initial(rho, e, 1.4 + s * h)
+            adj.forward(steps, dts)
+            vals.append(ke_exact(adj, dk))
+        dg_fd = (vals[0] - vals[1]) / (2 * h)
+        errs = sorted(errs)
+        fd[f"h={h:g}"] = {"rel_err_median": errs[len(errs) // 2], "rel_err_p90": errs[int(0.9 * len(errs))],
+                          "rel_err_max": errs[-1], "over_1e-3": int(sum(x > 1e-3 for x in errs)),
+                          "gamma_fd": dg_fd, "gamma_rel_err": abs(dg_fd - gg) / abs(gg)}
+    t_fd = time.perf_counter() - t0
+    adj.close()
+    return {"mesh": f"{n}x{n}", "steps": steps, "perturbation": "+-5% uniform per cell, seed 0xAD7", "ke": ke,
+            "forward_s": t_fwd, "gradient_s": t_rev, "tangent_s": t_tan, "fd_s": t_fd,
+            "cell_steps_per_s_forward": n * n * steps / t_fwd,
+            "checkpoint_interval": st["checkpoint_interval"], "checkpoints": st["checkpoints"],
+            "recomputed_steps": st["recomputed_steps"], "device_mb": st["device_bytes"] / 2 ** 20,
+            "dot_test_rel": max(dots), "gamma_adjoint": gg, "grad_max_abs": gmax,
+            "fd": {"cells": fd_cells, "objective": "final kinetic energy summed exactly (math.fsum of the per-cell terms)",
+                   "rel_err": "|fd - adjoint| / max(|adjoint|, 1e-6 max|grad|)", **fd}}
+
+
 def reference_exe():
     return os.path.join(ROOT, "oracle", "_ref", "omp")
 
@@ -371,6 +472,8 @@ def main():
     ap.add_argument("--large", type=int, default=15360, help="second FP64 size timed (0 to skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--batch", type=int, default=512, help="decks of the batched-ensemble leg (0 to skip)")
+    ap.add_argument("--adjoint", type=int, default=480, help="mesh side of the adjoint leg (0 to skip)")
+    ap.add_argument("--adjoint-steps", type=int, default=200)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -463,6 +566,13 @@ def main():
         except Exception as e:
             batch = {"error": str(e)}
 
+    adjoint = None
+    if args.adjoint:
+        try:
+            adjoint = adjoint_leg(args.adjoint, args.adjoint_steps)
+        except Exception as e:
+            adjoint = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -478,9 +588,9 @@ def main():
                            "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "halo": "folded into producers"},
-                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "cpu_baseline": cpu}
-        print(json.dumps(line))
+        print(json.dumps(line, default=_plain))
     if world > 1:
         torch.distributed.destroy_process_group()
 

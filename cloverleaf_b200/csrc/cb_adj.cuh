@@ -191,7 +191,7 @@ template <typename S> __global__ void k_tl_cell_face(Grid g, int dir, VD vf, VD 
   cell_stencil(flux > S(0.0), f, na, donor, upwind, downwind, dif);
   const double *vd = dir == 1 ? g.vdx : g.vdy;
   S mflux, eadv;
-  cell_face_value<S>(flux, A(pv, donor), S(vd[f]), S(vd[dif]), A(rho, donor), A(rho, upwind), A(rho, downwind), A(e, donor), A(e, upwind),
+  cell_face_value<S>(flux, A(pv, donor), S(vd[f] / vd[dif]), A(rho, donor), A(rho, upwind), A(rho, downwind), A(e, donor), A(e, upwind),
                      A(e, downwind), mflux, eadv);
   const int c = g.at(ci(dir, f, l), cj(dir, f, l));
   IO<S>::st(mf, c, mflux);
@@ -641,7 +641,7 @@ __global__ void k_adj_cell_face(Grid g, int dir, const double *vf, const double 
   const double *vd = dir == 1 ? g.vdx : g.vdy;
   const int cd = G(donor), cu = G(upwind), cw = G(downwind);
   X mflux, eadv;
-  cell_face_value<X>(flux, X::var(pv[cd], 1), X(vd[f]), X(vd[dif]), X::var(rho[cd], 2), X::var(rho[cu], 3), X::var(rho[cw], 4),
+  cell_face_value<X>(flux, X::var(pv[cd], 1), X(vd[f] / vd[dif]), X::var(rho[cd], 2), X::var(rho[cu], 3), X::var(rho[cw], 4),
                      X::var(e[cd], 5), X::var(e[cu], 6), X::var(e[cw], 7), mflux, eadv);
   const X eflux = mflux * eadv;
   double gr[8];

@@ -89,6 +89,19 @@ int check_depth(int d, bool allow0) {
 }
 
 cudaError_t upload_geom(cb_chunk *c) {
+  {
+    // reciprocals of the widths, rounded to nearest (the divisors of width_ratio)
+    std::vector<double> r(4 * (size_t)c->geom_len, 0.0);
+    const int src[4] = {CELLDX, CELLDY, VERTEXDX, VERTEXDY};
+    for (int q = 0; q < 4; ++q)
+      for (int k = 0; k < c->geom_len; ++k) {
+        const double w = c->geom_h[src[q]][k];
+        r[(size_t)q * c->geom_len + k] = w != 0.0 ? 1.0 / w : 0.0;
+      }
+    cudaError_t e = cudaMemcpyAsync(c->rgeom_d, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream); // r dies here
+    if (e != cudaSuccess) return e;
+  }
   for (int g = 0; g < NUM_GEOM; ++g) {
     cudaError_t e = cudaMemcpyAsync(c->geom_d[g], c->geom_h[g], sizeof(double) * c->geom_len, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return e;
@@ -115,6 +128,8 @@ void release(cb_chunk *c) {
     c->geom_t[g] = nullptr;
     c->geom_h[g] = nullptr;
   }
+  if (c->rgeom_d) cudaFree(c->rgeom_d);
+  c->rgeom_d = nullptr;
   if (c->d_dt_bits) cudaFree(c->d_dt_bits);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_counter) cudaFree(c->d_counter);
@@ -311,6 +326,7 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
       c->geom_t[g] = c->geom_d[g];
     }
   }
+  if ((e = cudaMalloc(&c->rgeom_d, sizeof(double) * 4 * c->geom_len)) != cudaSuccess) return bail(e, "geometry");
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   c->summary_grid = c->sms * 8;
   if ((e = cudaMalloc(&c->d_dt_bits, sizeof(unsigned long long))) != cudaSuccess) return bail(e, "scratch");

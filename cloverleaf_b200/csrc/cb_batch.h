@@ -42,6 +42,8 @@ struct BatchDeck {
   const CUtensorMap *maps;    // [NUM_BUF][NUM_BOX_H], in global memory
   const double *geom_d[NUM_GEOM];
   const void *geom_t[NUM_GEOM];
+  const double *rgeom;        // 1 / celldx, 1 / celldy, 1 / vertexdx, 1 / vertexdy
+  int geom_len;
   // the deck (driver/definitions.h:227-256 globals that the step reads)
   double gm1;                 // gamma - 1
   int nstates;

@@ -39,6 +39,7 @@ struct cb_batch {
   std::vector<double> work;         // estimated cells x steps of each deck
   void *pool = nullptr;             // fields of every deck
   double *geom = nullptr;           // FP64 geometry of every deck
+  double *rgeom = nullptr;          // reciprocal widths of every deck
   void *geom_t = nullptr;           // geometry in the storage type (FP32 form)
   CUtensorMap *maps = nullptr;      // [deck][NUM_BUF][NUM_BOX_H]
   double *records = nullptr;        // summaries, dt traces, partials
@@ -204,7 +205,7 @@ void release(cb_batch *b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
-  for (void *p : {(void *)b->pool, (void *)b->geom, b->geom_t, (void *)b->maps, (void *)b->records, (void *)b->slots, (void *)b->d_desc,
+  for (void *p : {(void *)b->pool, (void *)b->geom, (void *)b->rgeom, b->geom_t, (void *)b->maps, (void *)b->records, (void *)b->slots, (void *)b->d_desc,
                   (void *)b->d_plan, (void *)b->d_sync, (void *)b->d_flags})
     if (p) cudaFree(p);
   if (b->h_desc) cudaFreeHost(b->h_desc);
@@ -213,6 +214,7 @@ void release(cb_batch *b) {
   if (b->stream) cudaStreamDestroy(b->stream);
   b->pool = nullptr;
   b->geom = nullptr;
+  b->rgeom = nullptr;
   b->geom_t = nullptr;
   b->maps = nullptr;
   b->records = nullptr;
@@ -320,6 +322,7 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
   if ((e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) return bail(e, "events");
   if ((e = cudaMalloc(&b->pool, pool_bytes)) != cudaSuccess) return bail(e, "fields");
   if ((e = cudaMalloc(&b->geom, geom_elems * sizeof(double))) != cudaSuccess) return bail(e, "geometry");
+  if ((e = cudaMalloc(&b->rgeom, geom_elems / 2 * sizeof(double))) != cudaSuccess) return bail(e, "geometry");
   if (precision == CB_FP32 && (e = cudaMalloc(&b->geom_t, geom_elems * sizeof(float))) != cudaSuccess) return bail(e, "geometry");
   if ((e = cudaMalloc(&b->maps, sizeof(CUtensorMap) * NUM_BUF * NUM_BOX_H * ndecks)) != cudaSuccess) return bail(e, "tensor maps");
   if ((e = cudaMalloc(&b->records, sizeof(double) * rec_elems)) != cudaSuccess) return bail(e, "records");
@@ -327,7 +330,7 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
   if ((e = cudaMalloc(&b->d_desc, sizeof(BatchDeck) * ndecks)) != cudaSuccess) return bail(e, "descriptors");
   if ((e = cudaMallocHost(&b->h_desc, sizeof(BatchDeck) * ndecks)) != cudaSuccess) return bail(e, "descriptors");
   if ((e = cudaMalloc(&b->d_flags, sizeof(int) * 2)) != cudaSuccess) return bail(e, "scratch");
-  std::vector<double> gh(geom_elems, 0.0);
+  std::vector<double> gh(geom_elems, 0.0), rh(geom_elems / 2, 0.0);
   std::vector<CUtensorMap> maps((size_t)NUM_BUF * NUM_BOX_H * ndecks);
   for (int k = 0; k < ndecks; ++k) {
     const cb_deck &d = decks[k];
@@ -341,6 +344,13 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
       D.geom_t[q] = precision == CB_FP64 ? (const void *)D.geom_d[q] : (const void *)((float *)b->geom_t + geom_off[k] + (size_t)q * glen);
     }
     chunk_geometry(d.nx, d.ny, d.xmin, d.ymin, d.xmax, d.ymax, g);
+    // reciprocals of the widths, rounded to nearest (the divisors of width_ratio)
+    const int rsrc[4] = {CELLDX, CELLDY, VERTEXDX, VERTEXDY};
+    double *rk = rh.data() + geom_off[k] / 2;
+    for (int q = 0; q < 4; ++q)
+      for (int x = 0; x < glen; ++x) rk[(size_t)q * glen + x] = g[rsrc[q]][x] != 0.0 ? 1.0 / g[rsrc[q]][x] : 0.0;
+    D.rgeom = b->rgeom + geom_off[k] / 2;
+    D.geom_len = glen;
     std::string err;
     if (!encode_buffer_maps(D.buf, NUM_BUF, D.pitch, d.ny, precision,
                             reinterpret_cast<CUtensorMap(*)[NUM_BOX_H]>(&maps[(size_t)k * NUM_BUF * NUM_BOX_H]), &err)) {
@@ -369,6 +379,7 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
     D.dt_slots = b->slots + 4 * (size_t)k;
   }
   if ((e = cudaMemcpy(b->geom, gh.data(), sizeof(double) * geom_elems, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "geometry");
+  if ((e = cudaMemcpy(b->rgeom, rh.data(), sizeof(double) * rh.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "geometry");
   if (precision == CB_FP32) {
     std::vector<float> gf(gh.begin(), gh.end());
     if ((e = cudaMemcpy(b->geom_t, gf.data(), sizeof(float) * geom_elems, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "geometry");

@@ -230,6 +230,10 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
   d.m.vertexdy = D->geom_d[VERTEXDY];
   d.m.celldx_t = (const T *)D->geom_t[CELLDX];
   d.m.celldy_t = (const T *)D->geom_t[CELLDY];
+  d.m.rcelldx = D->rgeom;
+  d.m.rcelldy = D->rgeom + D->geom_len;
+  d.m.rvertexdx = D->rgeom + 2 * D->geom_len;
+  d.m.rvertexdy = D->rgeom + 3 * D->geom_len;
   const Mesh<T> &m = d.m;
   const int off = D->off;
   const T gm1 = (T)D->gm1;

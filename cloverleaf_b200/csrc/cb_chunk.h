@@ -47,6 +47,7 @@ struct Chunk {
   double *geom_d[NUM_GEOM] = {};
   void *geom_t[NUM_GEOM] = {};
   double *geom_h[NUM_GEOM] = {};
+  double *rgeom_d = nullptr; // 1 / celldx, 1 / celldy, 1 / vertexdx, 1 / vertexdy (4 x geom_len, FP64)
   int geom_len = 0;
 
   cudaStream_t stream = nullptr;

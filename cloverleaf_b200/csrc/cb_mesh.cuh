@@ -78,11 +78,28 @@ __host__ __device__ inline HaloRule halo_rule(int f) {
 template <typename T> __device__ __forceinline__ T lim_div(T a, T b) { return a / b; }
 template <> __device__ __forceinline__ float lim_div<float>(float a, float b) { return __fdividef(a, b); }
 
+// x / w for positive mesh widths x and w, given r = 1 / w rounded to nearest
+// (computed on the host), by correction steps q <- RN(q + (x - q w) r) with
+// the remainder formed exactly by a fused multiply-add.  q0 = RN(x r) lies
+// within 1.5 ulp of x / w; one step brings it within an ulp; then
+// Markstein's theorem (P. W. Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990:
+// with r within half an ulp of 1 / w and q within an ulp of x / w,
+// RN(q + (x - q w) r) = RN(x / w)) makes the second step the correctly
+// rounded quotient, the value of x / w.  Valid for normal operands whose
+// quotient and remainders stay normal, as ratios of mesh widths do.
+__device__ __forceinline__ double width_ratio(double x, double w, double r) {
+  double q = x * r;
+  q = fma(fma(-q, w, x), r, q);
+  return fma(fma(-q, w, x), r, q);
+}
+
 template <typename T> struct Mesh {
   int nx, ny;
   long long pitch;           // elements per row
   const double *celldx, *celldy, *vertexdx, *vertexdy; // 1-D geometry (FP64 always)
   const T *celldx_t, *celldy_t;                        // the same widths in the storage type
+  const double *rcelldx, *rcelldy, *rvertexdx, *rvertexdy; // their reciprocals, rounded to nearest
 
   __device__ __forceinline__ long long at(int i, int j) const { return (long long)j * pitch + i; }
 };

@@ -31,6 +31,10 @@ template <typename T> Mesh<T> mesh(const Chunk &c) {
   m.vertexdy = c.geom_d[VERTEXDY];
   m.celldx_t = (const T *)c.geom_t[CELLDX];
   m.celldy_t = (const T *)c.geom_t[CELLDY];
+  m.rcelldx = c.rgeom_d;
+  m.rcelldy = c.rgeom_d + c.geom_len;
+  m.rvertexdx = c.rgeom_d + 2 * c.geom_len;
+  m.rvertexdy = c.rgeom_d + 3 * c.geom_len;
   return m;
 }
 

@@ -207,6 +207,39 @@ __device__ __forceinline__ T dt_value(T ss, T q, T d0, T u00, T u10, T u01, T u1
   return fmin(dtct, fmin(dtut, fmin(dtvt, fmin(dtdivt, T(g_big)))));
 }
 
+// An estimate of dt_value<double> for the minimum search: the same
+// expressions with the quotients (__fdividef) and the square root taken in
+// single precision from the double operands.  Error bound, relative to the
+// exact value of each term: operands rounded to float 2^-24 each, the
+// quotients within 2 ulp (2^-22), the root correctly rounded; dtct carries
+// at most 6e-7, dtut and dtvt 4e-7, dtdivt 8e-7 (its branch is taken for
+// quotients within 1e-5 of the threshold, so the estimate of a term can only
+// fall below the exact one there), and min() keeps the largest of those.
+// Operand magnitudes stay inside float's range for every state the
+// reference admits (quotients below g_big = 1e21, denominators above
+// g_small * volume).
+__device__ __forceinline__ double dt_estimate(double ss, double q, double d0, double u00, double u10, double u01, double u11, double v00,
+                                              double v10, double v01, double v11, double dsx, double dsy, const DtConsts &k) {
+  const double vol = dsx * dsy;
+  const double cc = ss * ss + (double)__fdividef((float)(2.0 * q), (float)d0);
+  const float ccs = fmaxf(sqrtf((float)cc), (float)g_small);
+  const float dtct = __fdividef((float)(k.dtc_safe * fmin(dsx, dsy)), ccs);
+  double dv1 = (u00 + u01) * dsy, dv2 = (u10 + u11) * dsy;
+  double div = dv2 - dv1;
+  const float dtut = __fdividef((float)(k.dtu_safe * 2.0 * vol), (float)fmax(fmax(fabs(dv1), fabs(dv2)), g_small * vol));
+  dv1 = (v00 + v10) * dsx;
+  dv2 = (v01 + v11) * dsx;
+  div = div + dv2 - dv1;
+  const float dtvt = __fdividef((float)(k.dtv_safe * 2.0 * vol), (float)fmax(fmax(fabs(dv1), fabs(dv2)), g_small * vol));
+  const float divq = __fdividef((float)div, (float)(2.0 * vol));
+  const float dtdivt = divq < -(float)g_small * (1.0f - 1e-5f) ? (float)k.dtdiv_safe * __fdividef(-1.0f, divq) : (float)g_big;
+  return (double)fminf(dtct, fminf(dtut, fminf(dtvt, fminf(dtdivt, (float)g_big))));
+}
+
+// Cells whose estimate exceeds the minimum found so far by more than this
+// factor cannot hold the minimum (the estimate's error is below 1e-6).
+constexpr double DT_SKIP = 1.0 + 1e-4;
+
 struct DtIn {
   const void *soundspeed, *viscosity, *density0;
 };
@@ -239,6 +272,8 @@ __device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
     dd[r] = in_mesh ? R[g] : T(1);
   }
   if (!stage(cx, sm, ms, 2, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  // FP64: the exact value only where the estimate can beat the warp's minimum so far
+  const double thr = sizeof(T) == sizeof(double) ? warp_min(vmin) * DT_SKIP : 0.0;
   if (i < m.nx + 2) {
     const T dsx = m.celldx_t[i];
 #pragma unroll
@@ -246,6 +281,11 @@ __device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
       const int j = y0 + threadIdx.y + 4 * r;
       if (j >= m.ny + 2) break;
       const int b = B::at(i, j, x0, y0);
+      if constexpr (sizeof(T) == sizeof(double)) {
+        const double est = dt_estimate(ss[r], qq[r], dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
+                                       V[b + BOX_X + 1], dsx, m.celldy_t[j], k);
+        if (est > thr) continue; // NaN estimates fall through to the exact value
+      }
       const double c = (double)dt_value(ss[r], qq[r], dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1],
                                         V[b + BOX_X], V[b + BOX_X + 1], dsx, m.celldy_t[j], k);
       vmin = fmin(c, vmin); // fmin drops a NaN candidate, as the reference's fmin does
@@ -547,12 +587,12 @@ template <typename T> __device__ __forceinline__ T cell_pre_vol2(T vol, T a_lo, 
 // (:63-113 / :155-205): flux the face's volume flux, donor/upwind/downwind
 // the cells the flux's sign selects (d* densities, e* energies), pre_vol_d
 // the donor's pre_vol, vdx_f / vdx_dif the vertex widths at the face and at
-// the cell the limiter's ratio uses.  The energy flux is mass_flux * e_adv.
+// the cell the limiter's ratio uses; ratio = vdx_f / vdx_dif.  The energy
+// flux is mass_flux * e_adv.
 template <typename T>
-__device__ __forceinline__ void cell_face_value(T flux, T pre_vol_d, T vdx_f, T vdx_dif, T dd, T du, T dw, T ed, T eu, T ew, T &mass_flux,
-                                                T &e_adv) {
+__device__ __forceinline__ void cell_face_value(T flux, T pre_vol_d, T ratio, T dd, T du, T dw, T ed, T eu, T ew, T &mass_flux, T &e_adv) {
   T sigmat = lim_div(fabs(flux), pre_vol_d);
-  T sigma3 = (T(1.0) + sigmat) * lim_div(vdx_f, vdx_dif);
+  T sigma3 = (T(1.0) + sigmat) * ratio;
   T sigma4 = T(2.0) - sigmat;
   T sigmav = sigmat;
   T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
@@ -643,6 +683,7 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
   __syncthreads();
   // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
   const double *vdx = DIR == 1 ? m.vertexdx : m.vertexdy;
+  const double *rvdx = DIR == 1 ? m.rvertexdx : m.rvertexdy;
   const bool edge = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   for (int t = tid; t < L::NF * LL; t += 256) {
     int p, l;
@@ -662,7 +703,13 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     const int bd = b + (donor - f) * ST, bu = b + (upwind - f) * ST, bw = b + (downwind - f) * ST;
     const T pre_vol_d = s_pv[L::pv(donor - a0 + 1, l)];
     T mass_flux, e_adv;
-    cell_face_value(flux, pre_vol_d, (T)vdx[f], (T)vdx[dif], D1[bd], D1[bu], D1[bw], E1[bd], E1[bu], E1[bw], mass_flux, e_adv);
+    T ratio;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      ratio = width_ratio(vdx[f], vdx[dif], rvdx[dif]); // = vdx[f] / vdx[dif]
+    } else {
+      ratio = lim_div((T)vdx[f], (T)vdx[dif]);
+    }
+    cell_face_value(flux, pre_vol_d, ratio, D1[bd], D1[bu], D1[bw], E1[bd], E1[bu], E1[bw], mass_flux, e_adv);
     s_mf[L::fx(p, l)] = (double)mass_flux;
     s_ef[L::fx(p, l)] = (double)mass_flux * (double)(e_adv);
     T *mf = (T *)out.mass_flux;
@@ -711,8 +758,10 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
   return true;
 }
 
+// Five blocks per SM: the register budget that keeps the staged boxes of
+// five tiles resident.
 template <typename T, int DIR, int TY>
-__global__ void __launch_bounds__(256) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
+__global__ void __launch_bounds__(256, 5) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
                                                      int fold, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;

@@ -269,6 +269,12 @@ int cb_adjoint_read_field(cb_adjoint *a, int field, double *host, size_t n);
  * the last reverse sweep, and the device memory the adjoint holds. */
 int cb_adjoint_stats(const cb_adjoint *a, int *checkpoint_interval, int *checkpoints, long long *recomputed_steps, size_t *device_bytes);
 
+/* Self-test of the FP64 kernels' quotient of two mesh widths (formed with a
+ * precomputed reciprocal) against the device's division operator on
+ * `samples` pseudo-random pairs of positive operands; *mismatches counts the
+ * quotients that differ in any bit.  No counterpart in the reference. */
+int cb_selftest_width_ratio(long long samples, unsigned long long seed, long long *mismatches);
+
 /* The field summary of cb_field_summary (ideal_gas, then the five sums) over
  * FP64 device arrays the caller owns, allocating no memory: for callers that
  * must not allocate device memory where they need the summary (their device
