@@ -24,6 +24,10 @@ namespace cb {
 // Tile shapes of the batch kernel variants: the rows per tile of accelerate
 // and flux_calc (the phases with the largest staged boxes) set the shared
 // memory per CTA and with it the CTAs per SM.
+// Rows per advection tile in both precisions: the decks are small, and more,
+// smaller tiles spread a deck's phase more evenly over its lane.
+constexpr int BATCH_ADV_TY = 8;
+
 template <int V> struct BatchTune;
 template <> struct BatchTune<0> {
   static constexpr int ACC = 16, FLUX = 16, MINB = 3;
@@ -40,10 +44,10 @@ template <typename T, int V> constexpr size_t batch_smem() {
   s = mx(s, pdv_smem<T>());
   s = mx(s, acc_smem<T, BT::ACC>());
   s = mx(s, flux_smem<T, BT::FLUX>());
-  s = mx(s, CellLayout<T, 1, CB_CELL_TY_X>::SMEM);
-  s = mx(s, CellLayout<T, 2, CB_CELL_TY_Y>::SMEM);
-  s = mx(s, MomLayout<T, 1, CB_MOM_TY_X>::SMEM);
-  s = mx(s, MomLayout<T, 2, CB_MOM_TY_Y>::SMEM);
+  s = mx(s, CellLayout<T, 1, BATCH_ADV_TY>::SMEM);
+  s = mx(s, CellLayout<T, 2, BATCH_ADV_TY>::SMEM);
+  s = mx(s, MomLayout<T, 1, BATCH_ADV_TY>::SMEM);
+  s = mx(s, MomLayout<T, 2, BATCH_ADV_TY>::SMEM);
   s = mx(s, (size_t)5 * 256 * sizeof(double)); // the summary's block reduction
   return s;
 }
@@ -115,24 +119,25 @@ struct BufMap {
   }
 };
 
+// The deck a lane works on, kept in shared memory (one copy per CTA, written
+// by thread 0): the phases read it there instead of holding it in registers.
 template <typename T> struct DeckCtx {
   const BatchDeck *D;
   Mesh<T> m;
-  int rank, w, tid;
+  int rank, w;
   BufMap bm;
+  MapSet ms; // tensor maps of the current phase (read by the staging thread only)
+  Fields<T> F; // field pointers under the current buffer map (set_fields)
 
   __device__ T *base(int b) const { return (T *)D->buf[b] + D->off; }
   __device__ T *field(int f) const { return base(bm.of(f)); }
-  __device__ Fields<T> fields() const {
-    Fields<T> F;
+  __device__ void set_fields() {
     for (int f = 0; f < NUM_FIELDS; ++f) F.f[f] = f < 15 ? field(f) : nullptr;
-    return F;
   }
-  template <int H> __device__ MapSet maps(int n, const int *fl) const {
-    MapSet s;
+  // Sets ms to the maps of fields fl[0..n) (called by thread 0 before a phase's tiles).
+  template <int H> __device__ void set_maps(int n, const int *fl) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) s.m[k] = k < n ? &D->maps[bm.of(fl[k]) * NUM_BOX_H + box_slot<H>()] : nullptr;
-    return s;
+    for (int k = 0; k < 8; ++k) ms.m[k] = k < n ? &D->maps[bm.of(fl[k]) * NUM_BOX_H + box_slot<H>()] : nullptr;
   }
 };
 
@@ -145,10 +150,11 @@ template <typename T> struct DeckCtx {
 
 template <typename T, int DIR>
 __device__ __forceinline__ bool batch_advec_cell(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep) {
-  constexpr int TY = DIR == 1 ? CB_CELL_TY_X : CB_CELL_TY_Y;
+  constexpr int TY = BATCH_ADV_TY;
   using L = CellLayout<T, DIR, TY>;
   const int fl[4] = {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y};
-  const MapSet ms = d.template maps<L::BH>(4, fl);
+  if (threadIdx.x == 0 && threadIdx.y == 0) d.template set_maps<L::BH>(4, fl);
+  const MapSet &ms = d.ms;
   const CellOut out{d.base(d.bm.spare(0)), d.base(d.bm.spare(1)), d.field(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
   const int tx = (d.m.nx + TILE_X - 1) / TILE_X, nt = tx * ((d.m.ny + TY - 1) / TY);
   CB_LANE_TILES(d, nt, tx, (advec_cell_tile<T, DIR, TY>(cx, sm, ms, out, d.m, d.D->off, sweep, 2, bx, by)));
@@ -157,12 +163,13 @@ __device__ __forceinline__ bool batch_advec_cell(TileCtx &cx, T *sm, DeckCtx<T> 
 
 template <typename T, int DIR>
 __device__ __forceinline__ bool batch_advec_mom(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep, int fold) {
-  constexpr int TY = DIR == 1 ? CB_MOM_TY_X : CB_MOM_TY_Y;
+  constexpr int TY = BATCH_ADV_TY;
   using L = MomLayout<T, DIR, TY>;
   const int mom_sweep = DIR + 2 * (sweep - 1);
   const int mf = DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y;
   const int fl[5] = {XVEL1, YVEL1, DENSITY1, mf, mom_sweep == 1 ? VOL_FLUX_Y : VOL_FLUX_X};
-  const MapSet ms = d.template maps<L::BH>(mom_sweep <= 2 ? 5 : 4, fl);
+  if (threadIdx.x == 0 && threadIdx.y == 0) d.template set_maps<L::BH>(mom_sweep <= 2 ? 5 : 4, fl);
+  const MapSet &ms = d.ms;
   const MomOut out{d.base(d.bm.spare(2)), d.base(d.bm.spare(3))};
   const int tx = (d.m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((d.m.ny + 1 + TY - 1) / TY);
   CB_LANE_TILES(d, nt, tx, (advec_mom_tile<T, DIR, TY>(cx, sm, ms, out, d.m, d.D->off, 3, sweep, fold, bx, by)));
@@ -174,27 +181,28 @@ __device__ __forceinline__ bool batch_advec_mom(TileCtx &cx, T *sm, DeckCtx<T> &
 // lane's first CTA adds the partials in CTA order into the record.
 template <typename T>
 __device__ __forceinline__ bool batch_summary(T *sm, DeckCtx<T> &d, unsigned *ctr, int *abort, int step, double time, int &nsum) {
-  const Fields<T> F = d.fields();
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const Fields<T> &F = d.F;
   const T gm1 = (T)d.D->gm1;
   double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   const int tx = (d.m.nx + PW_X - 1) / PW_X, nt = tx * ((d.m.ny + PW_Y - 1) / PW_Y);
   for (int t = d.rank; t < nt; t += d.w) {
-    const int i = 2 + (t % tx) * PW_X + (d.tid & 31), j = 2 + (t / tx) * PW_Y + (d.tid >> 5);
+    const int i = 2 + (t % tx) * PW_X + (tid & 31), j = 2 + (t / tx) * PW_Y + (tid >> 5);
     if (i < d.m.nx + 2 && j < d.m.ny + 2) summary_cell(F, d.m, gm1, i, j, s);
   }
   double *red = reinterpret_cast<double *>(sm);
   __syncthreads(); // sm may still hold the previous phase's boxes
-  for (int q = 0; q < 5; ++q) red[q * 256 + d.tid] = s[q];
+  for (int q = 0; q < 5; ++q) red[q * 256 + tid] = s[q];
   __syncthreads();
   for (int h = 128; h > 0; h >>= 1) {
-    if (d.tid < h)
-      for (int q = 0; q < 5; ++q) red[q * 256 + d.tid] += red[q * 256 + d.tid + h];
+    if (tid < h)
+      for (int q = 0; q < 5; ++q) red[q * 256 + tid] += red[q * 256 + tid + h];
     __syncthreads();
   }
-  if (d.tid == 0)
+  if (tid == 0)
     for (int q = 0; q < 5; ++q) d.D->partials[d.rank * 5 + q] = red[q * 256];
   if (!lane_sync(ctr, d.w, abort)) return false;
-  if (d.rank == 0 && d.tid == 0) {
+  if (d.rank == 0 && tid == 0) {
     double tot[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (int r = 0; r < d.w; ++r)
       for (int q = 0; q < 5; ++q) tot[q] += ((volatile double *)d.D->partials)[r * 5 + q];
@@ -213,14 +221,17 @@ __device__ __forceinline__ bool batch_summary(T *sm, DeckCtx<T> &d, unsigned *ct
 // (the lane then stops); a deck that ends early for physical reasons (dt
 // below dtmin) returns true with its status set.
 template <typename T, int V>
-__device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, int rank, int w, unsigned *ctr, int *abort) {
+__device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, int rank, int w, unsigned *ctr, int *abort) {
   using BT = BatchTune<V>;
   constexpr int N = Vec16<T>::N;
-  DeckCtx<T> d;
+  __shared__ DeckCtx<T> d;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  __syncthreads(); // the previous deck's readers are done with d
+  if (tid == 0) {
   d.D = D;
   d.rank = rank;
   d.w = w;
-  d.tid = threadIdx.y * blockDim.x + threadIdx.x;
+  d.bm = BufMap{};
   d.m.nx = D->nx;
   d.m.ny = D->ny;
   d.m.pitch = D->pitch;
@@ -234,14 +245,17 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
   d.m.rcelldy = D->rgeom + D->geom_len;
   d.m.rvertexdx = D->rgeom + 2 * D->geom_len;
   d.m.rvertexdy = D->rgeom + 3 * D->geom_len;
+  d.set_fields();
+  }
+  __syncthreads();
   const Mesh<T> &m = d.m;
   const int off = D->off;
   const T gm1 = (T)D->gm1;
-  const int ptx = d.tid & 31, pty = d.tid >> 5; // thread of a 32 x 8 pointwise block
-  const int lt = rank * 256 + d.tid, lstride = w * 256;
+  const int ptx = tid & 31, pty = tid >> 5; // thread of a 32 x 8 pointwise block
+  const int lt = rank * 256 + tid, lstride = w * 256;
   int status = DECK_PENDING;
   auto finish = [&](int st, int steps, double time, int nsum) {
-    if (rank == 0 && d.tid == 0) {
+    if (rank == 0 && tid == 0) {
       D->status = st;
       D->steps = steps;
       D->time = time;
@@ -272,12 +286,12 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
       uint4 *p = (uint4 *)D->buf[b];
       for (size_t e = lt; e < nv; e += lstride) p[e] = make_uint4(0u, 0u, 0u, 0u);
     }
-    if (rank == 0 && d.tid < 3) D->dt_slots[d.tid] = (unsigned long long)__double_as_longlong(g_big);
+    if (rank == 0 && tid < 3) D->dt_slots[tid] = (unsigned long long)__double_as_longlong(g_big);
   }
   CB_SYNC();
   // generate_chunk over the full extents, then ideal_gas on level 0
   {
-    const Fields<T> F = d.fields();
+    const Fields<T> &F = d.F;
     const int ex = m.nx + 5, ey = m.ny + 5;
     for (int e = lt; e < ex * ey; e += lstride)
       generate_element(F, m, D->states, D->nstates, D->geom_d[CELLX], D->geom_d[CELLY], D->geom_d[VERTEXX], D->geom_d[VERTEXY], e % ex,
@@ -285,7 +299,7 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
   }
   CB_SYNC();
   {
-    const Fields<T> F = d.fields();
+    const Fields<T> &F = d.F;
     const int gx = ((m.nx + N - 1) / N + PW_X - 1) / PW_X, gy = (m.ny + PW_Y - 1) / PW_Y;
     for (int vb = rank; vb < gx * gy; vb += w) ideal_gas_block(F, m, 0, gm1, 0, vb % gx, vb / gx, ptx, pty);
   }
@@ -294,7 +308,7 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
   // bottom/top of every column, then left/right of every row
   {
     const int hf[10] = {DENSITY0, ENERGY0, PRESSURE, VISCOSITY, DENSITY1, ENERGY1, XVEL0, YVEL0, XVEL1, YVEL1};
-    const Fields<T> F = d.fields();
+    const Fields<T> &F = d.F;
     const int len = (m.nx > m.ny ? m.nx : m.ny) + 5 + 4;
     for (int pass = 0; pass < 2; ++pass) {
       for (int e = lt; e < 10 * len; e += lstride) halo_fill(F, m, hf[e / len], 2, pass, e % len);
@@ -312,14 +326,15 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     ++step;
     // timestep (driver/timestep.cpp:37-109)
     {
-      const Fields<T> F = d.fields();
+      const Fields<T> &F = d.F;
       const int gx = ((m.nx + N - 1) / N + PW_X - 1) / PW_X, gy = (m.ny + PW_Y - 1) / PW_Y;
       for (int vb = rank; vb < gx * gy; vb += w) ideal_gas_block(F, m, 0, gm1, 1, vb % gx, vb / gx, ptx, pty);
     }
     CB_SYNC();
     {
       const int fl[3] = {PRESSURE, XVEL0, YVEL0};
-      const MapSet ms = d.template maps<Box1<T, VISC_TY>::BH>(3, fl);
+      if (tid == 0) d.template set_maps<Box1<T, VISC_TY>::BH>(3, fl);
+      const MapSet &ms = d.ms;
       const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + VISC_TY - 1) / VISC_TY);
       for (int t = rank; t < nt; t += w)
         CB_PHASE(viscosity_tile(cx, sm, ms, d.field(DENSITY0), d.field(VISCOSITY), m, off, t % tx, t / tx, 1));
@@ -328,7 +343,8 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     unsigned long long *slot = D->dt_slots + step % 3;
     {
       const int fl[2] = {XVEL0, YVEL0};
-      const MapSet ms = d.template maps<Box1<T, DT_TY>::BH>(2, fl);
+      if (tid == 0) d.template set_maps<Box1<T, DT_TY>::BH>(2, fl);
+      const MapSet &ms = d.ms;
       const DtIn in{d.field(SOUNDSPEED), d.field(VISCOSITY), d.field(DENSITY0)};
       const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + DT_TY - 1) / DT_TY);
       double vmin = g_big;
@@ -337,13 +353,13 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     }
     CB_SYNC();
     const double dtlp = __longlong_as_double((long long)*(volatile unsigned long long *)slot);
-    if (rank == 0 && d.tid == 0) D->dt_slots[(step + 1) % 3] = (unsigned long long)__double_as_longlong(g_big);
+    if (rank == 0 && tid == 0) D->dt_slots[(step + 1) % 3] = (unsigned long long)__double_as_longlong(g_big);
     dt = g_big;
     if (dtlp <= dt) dt = dtlp;
     double mm = dtold * D->dtrise;
     mm = mm < dt ? mm : dt;
     dt = D->dtmax < mm ? D->dtmax : mm;
-    if (rank == 0 && d.tid == 0 && step - 1 < D->max_steps) D->dt_trace[step - 1] = dt;
+    if (rank == 0 && tid == 0 && step - 1 < D->max_steps) D->dt_trace[step - 1] = dt;
     if (dt < D->dtmin) {
       status = DECK_SMALL_DT;
       break;
@@ -352,7 +368,8 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     // PdV predictor with ideal_gas, the pressure halo and revert (src/serial/PdV.cpp:92-133)
     {
       const int fl[4] = {XVEL0, YVEL0, XVEL1, YVEL1};
-      const MapSet ms = d.template maps<Box1<T, PDV_TY>::BH>(2, fl);
+      if (tid == 0) d.template set_maps<Box1<T, PDV_TY>::BH>(2, fl);
+      const MapSet &ms = d.ms;
       const PdvIn in{d.field(DENSITY0), d.field(ENERGY0), d.field(PRESSURE), d.field(VISCOSITY)};
       const PdvOut out{d.field(DENSITY1), d.field(ENERGY1), d.field(PRESSURE), d.field(SOUNDSPEED)};
       const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + PDV_TY - 1) / PDV_TY);
@@ -361,7 +378,8 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     CB_SYNC();
     {
       const int fl[5] = {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0};
-      const MapSet ms = d.template maps<Tile<BT::ACC>::BH>(5, fl);
+      if (tid == 0) d.template set_maps<Tile<BT::ACC>::BH>(5, fl);
+      const MapSet &ms = d.ms;
       const int tx = (m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + 1 + BT::ACC - 1) / BT::ACC);
       for (int t = rank; t < nt; t += w)
         CB_PHASE((accelerate_tile<T, BT::ACC>(cx, sm, ms, d.field(XVEL1), d.field(YVEL1), m, off, (T)dt, 2, t % tx, t / tx)));
@@ -369,7 +387,8 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     CB_SYNC();
     {
       const int fl[4] = {XVEL0, YVEL0, XVEL1, YVEL1};
-      const MapSet ms = d.template maps<Box1<T, PDV_TY>::BH>(4, fl);
+      if (tid == 0) d.template set_maps<Box1<T, PDV_TY>::BH>(4, fl);
+      const MapSet &ms = d.ms;
       const PdvIn in{d.field(DENSITY0), d.field(ENERGY0), d.field(PRESSURE), d.field(VISCOSITY)};
       const PdvOut out{d.field(DENSITY1), d.field(ENERGY1), d.field(PRESSURE), d.field(SOUNDSPEED)};
       const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + PDV_TY - 1) / PDV_TY);
@@ -378,7 +397,8 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     CB_SYNC();
     {
       const int fl[4] = {XVEL0, YVEL0, XVEL1, YVEL1};
-      const MapSet ms = d.template maps<Tile<BT::FLUX>::BH>(4, fl);
+      if (tid == 0) d.template set_maps<Tile<BT::FLUX>::BH>(4, fl);
+      const MapSet &ms = d.ms;
       const int tx = (m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + 1 + BT::FLUX - 1) / BT::FLUX);
       for (int t = rank; t < nt; t += w)
         CB_PHASE((flux_calc_tile<T, BT::FLUX>(cx, sm, ms, d.field(VOL_FLUX_X), d.field(VOL_FLUX_Y), m, off, (T)dt, 2, t % tx, t / tx)));
@@ -386,20 +406,25 @@ __device__ __noinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D, in
     CB_SYNC();
     // advection (driver/advection.cpp:29-105): the two advec_mom calls of a sweep in one pass
     const int dir1 = advect_x ? 1 : 2, dir2 = advect_x ? 2 : 1;
+    // the buffer map changes after each lane barrier, by thread 0, before anyone reads it again
     CB_PHASE((dir1 == 1 ? batch_advec_cell<T, 1>(cx, sm, d, 1) : batch_advec_cell<T, 2>(cx, sm, d, 1)));
-    d.bm.cell_swapped = true;
     CB_SYNC();
+    if (tid == 0) d.bm.cell_swapped = true, d.set_fields();
+    __syncthreads();
     CB_PHASE((dir1 == 1 ? batch_advec_mom<T, 1>(cx, sm, d, 1, 2) : batch_advec_mom<T, 2>(cx, sm, d, 1, 2)));
-    d.bm.mom_swapped = true;
     CB_SYNC();
+    if (tid == 0) d.bm.mom_swapped = true, d.set_fields();
+    __syncthreads();
     CB_PHASE((dir2 == 1 ? batch_advec_cell<T, 1>(cx, sm, d, 2) : batch_advec_cell<T, 2>(cx, sm, d, 2)));
-    d.bm.cell_swapped = false;
     CB_SYNC();
+    if (tid == 0) d.bm.cell_swapped = false, d.set_fields();
+    __syncthreads();
     CB_PHASE((dir2 == 1 ? batch_advec_mom<T, 1>(cx, sm, d, 2, 0) : batch_advec_mom<T, 2>(cx, sm, d, 2, 0)));
-    d.bm.mom_swapped = false;
     CB_SYNC();
+    if (tid == 0) d.bm.mom_swapped = false, d.set_fields();
+    __syncthreads();
     {
-      const Fields<T> F = d.fields();
+      const Fields<T> &F = d.F;
       const int gx = ((m.nx + 1 + N - 1) / N + PW_X - 1) / PW_X, gy = (m.ny + 1 + PW_Y - 1) / PW_Y;
       for (int vb = rank; vb < gx * gy; vb += w) reset_field_block(F, m, 1, vb % gx, vb / gx, ptx, pty);
     }

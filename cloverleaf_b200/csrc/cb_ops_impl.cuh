@@ -163,12 +163,6 @@ template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fol
   return launched(c);
 }
 
-#ifndef CB_CELL_TY_X
-#define CB_CELL_TY_X 8 // rows per x-sweep tile of advec_cell
-#endif
-#ifndef CB_CELL_TY_Y
-#define CB_CELL_TY_Y 8 // rows per y-sweep tile of advec_cell
-#endif
 
 template <typename T, int DIR, int TY> cudaError_t launch_advec_cell(Chunk &c, int sweep, int fold, void *dd, void *de) {
   using L = CellLayout<T, DIR, TY>;
@@ -189,16 +183,10 @@ template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int di
     RingPair rp{{sd, se}, {dd, de}};
     if ((e = copy_ring<T>(c, rp, 2, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
   }
-  return dir == 1 ? launch_advec_cell<T, 1, CB_CELL_TY_X>(c, sweep, fold, dd, de)
-                  : launch_advec_cell<T, 2, CB_CELL_TY_Y>(c, sweep, fold, dd, de);
+  return dir == 1 ? launch_advec_cell<T, 1, AdvecTiles<T>::CELL_X>(c, sweep, fold, dd, de)
+                  : launch_advec_cell<T, 2, AdvecTiles<T>::CELL_Y>(c, sweep, fold, dd, de);
 }
 
-#ifndef CB_MOM_TY_X
-#define CB_MOM_TY_X 8 // rows per x-sweep tile of advec_mom
-#endif
-#ifndef CB_MOM_TY_Y
-#define CB_MOM_TY_Y 8 // rows per y-sweep tile of advec_mom
-#endif
 
 template <typename T, int DIR, int TY>
 cudaError_t launch_advec_mom(Chunk &c, int vel_mask, int sweep, int fold, void *du, void *dv) {
@@ -227,8 +215,8 @@ template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int 
     if (vel_mask & 2) rp.src[n] = sv, rp.dst[n++] = dv;
     if ((e = copy_ring<T>(c, rp, n, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
   }
-  return dir == 1 ? launch_advec_mom<T, 1, CB_MOM_TY_X>(c, vel_mask, sweep, fold, du, dv)
-                  : launch_advec_mom<T, 2, CB_MOM_TY_Y>(c, vel_mask, sweep, fold, du, dv);
+  return dir == 1 ? launch_advec_mom<T, 1, AdvecTiles<T>::MOM_X>(c, vel_mask, sweep, fold, du, dv)
+                  : launch_advec_mom<T, 2, AdvecTiles<T>::MOM_Y>(c, vel_mask, sweep, fold, du, dv);
 }
 
 template <typename T> cudaError_t Ops<T>::reset_field(Chunk &c, int fold) {

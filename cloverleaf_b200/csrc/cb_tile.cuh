@@ -560,6 +560,18 @@ __global__ void __launch_bounds__(256) kt_flux_calc(const __grid_constant__ Maps
 }
 
 // ---------------------------------------------------------------------------
+// Rows per tile of the advection kernels, x sweep and y sweep: 8 in FP64
+// (issue-bound; smaller boxes keep five blocks per SM), 16 in FP32 (half the
+// bytes per element: taller tiles halve the per-tile staging overhead and
+// the share of cells recomputed in the tile overlaps).
+template <typename T> struct AdvecTiles {
+  static constexpr int CELL_X = 8, CELL_Y = 8, MOM_X = 8, MOM_Y = 8;
+};
+template <> struct AdvecTiles<float> {
+  static constexpr int CELL_X = 16, CELL_Y = 16, MOM_X = 16, MOM_Y = 16;
+};
+
+// ---------------------------------------------------------------------------
 // advec_cell: src/serial/advec_cell.cpp:28-220, one sweep in one pass.
 // pre_vol of the cells the faces need, then the face fluxes, then the
 // update, all through shared memory; each stage spreads its items evenly

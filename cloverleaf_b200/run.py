@@ -4,6 +4,7 @@ field summaries.
 
   python -m cloverleaf_b200.run --deck clover.in
   python -m cloverleaf_b200.run --bm 4608 --steps 2 [--precision fp32] [--no-fold]
+  python -m cloverleaf_b200.run --ensemble 512 [--precision fp32] [--runs 3]
 """
 from __future__ import annotations
 
@@ -20,11 +21,15 @@ def main(argv=None):
     g = ap.add_mutually_exclusive_group(required=True)
     g.add_argument("--deck", help="clover.in deck file")
     g.add_argument("--bm", type=int, help="benchmark problem on an N x N mesh")
+    g.add_argument("--ensemble", type=int, help="the seeded batched ensemble of N decks, one persistent launch per run")
     ap.add_argument("--steps", type=int, default=None, help="stop after this many steps (default: the deck's end)")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--no-fold", action="store_true", help="run every update_halo as its own pass")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--runs", type=int, default=1, help="ensemble runs after one warm-up run")
     args = ap.parse_args(argv)
+    if args.ensemble:
+        return ensemble(args)
 
     dk = read_deck(args.deck) if args.deck else nudged(benchmark_deck(args.bm, end_step=args.steps or 87))
     c = Chunk(dk.x_cells, dk.y_cells, precision=FP32 if args.precision == "fp32" else FP64, device=args.device)
@@ -42,6 +47,23 @@ def main(argv=None):
         qa = abs(100.0 * (run.summaries[-1].ke / 1.19316898756307) - 100.0)
         print(f" Test problem 2 is within {qa}% of the expected solution: {'PASSED' if qa < 0.001 else 'NOT PASSED'}")
     c.close()
+    return 0
+
+
+def ensemble(args):
+    from .batch import Batch, ensemble_decks
+    decks = ensemble_decks(args.ensemble)
+    b = Batch(decks, precision=FP32 if args.precision == "fp32" else FP64, device=args.device)
+    sched, lanes, ctas = b.schedule()
+    for k in range(args.runs + 1):
+        b.run()
+        ms = b.synchronize()
+        res = [b.result(q) for q in range(len(decks))]
+        cs = sum(d.x_cells * d.y_cells * r.steps for d, r in zip(decks, res))
+        print(f" {'warm-up' if k == 0 else 'run'}: {len(decks)} decks, {cs} cell-steps in {ms:.2f} ms "
+              f"({cs / ms * 1e3:.4e} cell-steps/s); {sum(r.status == 1 for r in res)} done; schedule {sched}, {lanes} lanes, "
+              f"{ctas} CTAs")
+    b.close()
     return 0
 
 
