@@ -13,6 +13,15 @@ driver's per-step dt read-back.  Every field array is 472 MB, far above the
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+Besides the headline FP64 line, the same JSON line carries: the FP32 form on
+the same deck and dt sequence (speed-up and errors against FP64), FP64 at
+15360^2, the batched ensemble of 512 seeded decks in one persistent launch
+(FP64 and FP32, autotuned, against the same decks run one after the other),
+the adjoint at 480^2 x 200 steps (timings, dot-product test, finite
+differences), the reference's own CUDA model on the same deck and GPU, the
+end-to-end figure through the C ABI with host buffers, and the reference
+OpenMP build on the host cores (cpu_baseline).
+
 N > 1 runs under torchrun: the path does not shard (one mesh per GPU, no
 decomposition, as in the north star), so each rank advances its own replica
 and value is the sum over ranks (weak scaling).  --impl reference times the
@@ -418,6 +427,30 @@ def run_reference_omp(cells, steps, threads, timeout=900):
         return [float(x) for x in re.findall(r"Step time per cell\s+([0-9.eE+-]+)", p.stdout)]
 
 
+def reference_cuda_leg(cells, steps=10, warm=2, timeout=900):
+    """The reference's own CUDA model (oracle/_ref/cuda: the unmodified driver
+    and src/cuda built for sm_100a with the model's nvcc flags) on the same
+    deck and the same B200, for comparison: cell-steps/s from the driver's
+    per-step "Step time per cell" lines (driver/hydro.cpp:209-220) after
+    `warm` steps, and its final kinetic energy."""
+    from cloverleaf_b200 import benchmark_deck, format_deck
+    exe = os.path.join(ROOT, "oracle", "_ref", "cuda")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/cuda was not built (needs the reference sources)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = os.path.join(tmp, "clover.in")
+        with open(deck, "w") as f:
+            f.write(format_deck(benchmark_deck(cells, end_step=warm + steps, end_time=1.0e30)))
+        p = subprocess.run([exe, "--file", deck, "--out", os.path.join(tmp, "clover.out")], cwd=tmp, capture_output=True, text=True,
+                           timeout=timeout)
+        if p.returncode != 0:
+            return {"error": f"exited {p.returncode}: {p.stdout[-300:]}"}
+        per_cell = [float(x) for x in re.findall(r"Step time per cell\s+([0-9.eE+-]+)", p.stdout)][warm:]
+        return {"value": 1.0 / statistics.mean(per_cell), "unit": UNIT, "steps": len(per_cell),
+                "sample": f"reference CUDA model (src/cuda, nvcc -O3 -extended-lambda -use_fast_math -restrict, sm_100a), "
+                          f"{cells}x{cells} benchmark deck, steps {warm + 1}-{warm + len(per_cell)}, driver's per-step timer"}
+
+
 def cpu_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -484,6 +517,7 @@ def main():
     ap.add_argument("--batch", type=int, default=512, help="decks of the batched-ensemble leg (0 to skip)")
     ap.add_argument("--adjoint", type=int, default=480, help="mesh side of the adjoint leg (0 to skip)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA model")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -583,6 +617,15 @@ def main():
         except Exception as e:
             adjoint = {"error": str(e)}
 
+    ref_cuda = None
+    if rank == 0 and world == 1 and not args.no_ref_cuda:
+        try:
+            ref_cuda = reference_cuda_leg(S)
+            if "value" in ref_cuda:
+                ref_cuda["b200_speedup"] = value / ref_cuda["value"]
+        except Exception as e:
+            ref_cuda = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -598,7 +641,7 @@ def main():
                            "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "halo": "folded into producers"},
-                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "cpu_baseline": cpu}
         print(json.dumps(line, default=_plain))
     if world > 1:
