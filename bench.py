@@ -53,6 +53,21 @@ PHASE_ARRAYS = {"ideal_gas": 4, "viscosity": 5, "calc_dt": 8, "pdv_predict": 11 
 STEP_ARRAYS = 105  # the step's phases, ideal_gas .. reset_field
 
 
+def max_over_ranks(ms, device):
+    """The slowest rank's time (ms) for the whole-job figure: one all_reduce(MAX)
+    of the device-timed elapsed time, the only collective of a replicas run."""
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(cells, steps, world, ms_max):
+    """Whole-job cell-steps/s of `world` replicas that each advanced `cells`
+    cells for `steps` steps, timed by the slowest."""
+    return cells * steps * world / (ms_max / 1e3)
+
+
 def _plain(o):
     """numpy scalars in the JSON line as plain numbers."""
     if hasattr(o, "item"):
@@ -543,19 +558,15 @@ def main():
                                                       world=world)
     clocks = clk.summary()
     if world > 1:
-        t = torch.tensor([ms64], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms64 = float(t.item())
-    value = S * S * args.steps * world / (ms64 / 1e3)
+        ms64 = max_over_ranks(ms64, "cuda")
+    value = replicas_value(S * S, args.steps, world, ms64)
 
     # FP32 form, replaying the FP64 run's dt sequence, errors against FP64 at the same time
     dts = list(run64.dt_trace)
     ms32, run32, c32, ph32, _ = run_form(FP32, S, args.warmup, args.steps, forced_dt=dts, with_phases=True, world=world)
     if world > 1:
-        t = torch.tensor([ms32], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms32 = float(t.item())
-    value32 = S * S * args.steps * world / (ms32 / 1e3)
+        ms32 = max_over_ranks(ms32, "cuda")
+    value32 = replicas_value(S * S, args.steps, world, ms32)
     errs = {}
     for name in ("density0", "energy0", "pressure", "xvel0", "yvel0"):
         a64 = c64.read(name)[2:-2, 2:-2]
@@ -580,13 +591,17 @@ def main():
         try:
             msl, _, cl, _, _ = run_form(FP64, args.large, 3, 20, world=world)
             cl.close()
-            large = {"cells": f"{args.large}x{args.large}", "steps": 20, "value": args.large ** 2 * 20 * world / (msl / 1e3),
+            if world > 1:
+                msl = max_over_ranks(msl, "cuda")
+            large = {"cells": f"{args.large}x{args.large}", "steps": 20, "value": replicas_value(args.large ** 2, 20, world, msl),
                      "unit": UNIT}
         except Exception as e:  # memory or other failure is reported, not hidden
             large = {"error": str(e)}
 
     ms_e2e, h2d, d2h = e2e_run(S, args.warmup, args.steps)
-    e2e = {"value": S * S * args.steps * world / (ms_e2e / 1e3), "unit": UNIT,
+    if world > 1:
+        ms_e2e = max_over_ranks(ms_e2e, "cuda")
+    e2e = {"value": replicas_value(S * S, args.steps, world, ms_e2e), "unit": UNIT,
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
 
     # roofline of the dominant kernel (largest total time over the timed steps)
