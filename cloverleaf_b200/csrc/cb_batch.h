@@ -22,7 +22,7 @@ namespace cb {
 
 constexpr int BATCH_MAX_STATES = 8;
 constexpr int BATCH_RECORD = 7;       // summary record: step, time, vol, mass, ie, ke, press
-constexpr int BATCH_MAX_LANE = 128;   // CTAs per lane at most
+constexpr int BATCH_MAX_LANE = 1024;  // CTAs per lane at most
 constexpr int BATCH_VARIANTS = 2;     // tile-shape variants of the kernel (BatchTune)
 
 // Deck status after a run.

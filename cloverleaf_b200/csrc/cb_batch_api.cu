@@ -125,8 +125,8 @@ Plan make_plan(const cb_batch *b, const cb_batch_schedule &s, int grid_max) {
     int wd = s.cells_per_cta > 0 ? next_pow2((cells + s.cells_per_cta - 1) / s.cells_per_cta) : 1;
     wd = std::min(wd, maxw);
     while (wd > 1 && wd > tiles_of(b->decks[d])) wd >>= 1;
-    while (wd > grid_max) wd >>= 1;
-    w[d] = std::max(wd, 1);
+    // a deck wider than the grid gets the whole grid (not the power of two below it)
+    w[d] = std::max(std::min(wd, grid_max), 1);
   }
   // classes by width: count, work
   std::vector<int> widths;
