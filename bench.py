@@ -243,7 +243,7 @@ def e2e_run(cells, warmup, steps):
     for _ in range(steps):
         run2.hydro_step()
     for n in names:
-        host[n][...] = c.read(n)
+        c.read_into(n, host[n])
     t1.record(ext)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
@@ -251,6 +251,42 @@ def e2e_run(cells, warmup, steps):
     d2h = sum(host[n].nbytes for n in names) + 8 * steps + 40 * len(run2.summaries)
     c.close()
     return ms, h2d, d2h
+
+
+def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
+    """The whole hydro loop as one device-resident CUDA graph (cb_run) against
+    the host-driven loop (dt read back every step), FP64, same deck, same
+    steps; ms per step from CUDA events on the chunk's stream around the
+    whole loop (the graph's capture and instantiation included)."""
+    import torch
+    from cloverleaf_b200 import Chunk, HydroRun
+    out = []
+    for cells, steps in sizes:
+        row = {"cells": f"{cells}x{cells}", "steps": steps}
+        for mode in ("host_loop", "device_graph"):
+            c = Chunk(cells, cells, device=torch.cuda.current_device())
+            r = HydroRun(c, bench_deck(cells))
+            r.start()
+            for _ in range(warmup):
+                r.hydro_step()
+            ext = torch.cuda.ExternalStream(c.stream())
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c.synchronize()
+            torch.cuda.synchronize()
+            t0.record(ext)
+            if mode == "device_graph":
+                r.run_steps_on_device(max_steps=r.step + steps)
+            else:
+                for _ in range(steps):
+                    r.hydro_step()
+            t1.record(ext)
+            torch.cuda.synchronize()
+            ms = t0.elapsed_time(t1)
+            row[mode] = {"ms_per_step": ms / steps, "value": cells * cells * steps / (ms / 1e3), "unit": UNIT}
+            c.close()
+        row["speedup"] = row["host_loop"]["ms_per_step"] / row["device_graph"]["ms_per_step"]
+        out.append(row)
+    return out
 
 
 def traffic_per_launch(kernel, cells):
@@ -533,6 +569,7 @@ def main():
     ap.add_argument("--adjoint", type=int, default=480, help="mesh side of the adjoint leg (0 to skip)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA model")
+    ap.add_argument("--no-resident", action="store_true", help="skip the device-resident loop leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -632,6 +669,13 @@ def main():
         except Exception as e:
             adjoint = {"error": str(e)}
 
+    resident = None
+    if not args.no_resident:
+        try:
+            resident = resident_leg(((960, 87), (S, 100)))
+        except Exception as e:
+            resident = {"error": str(e)}
+
     ref_cuda = None
     if rank == 0 and world == 1 and not args.no_ref_cuda:
         try:
@@ -656,7 +700,7 @@ def main():
                            "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "halo": "folded into producers"},
-                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "resident_loop": resident, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "cpu_baseline": cpu}
         print(json.dumps(line, default=_plain))
     if world > 1:

@@ -31,7 +31,7 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk",
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
-           "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_field_summary_noalloc",
+           "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_run", "cb_field_summary_noalloc",
            "cb_batch_create", "cb_batch_destroy", "cb_batch_set_schedule", "cb_batch_get_schedule", "cb_batch_autotune",
            "cb_batch_run", "cb_batch_synchronize", "cb_batch_deck_result", "cb_batch_read_summaries", "cb_batch_read_dt",
            "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count",
@@ -54,6 +54,18 @@ class State(ctypes.Structure):
 class DtParams(ctypes.Structure):
     _fields_ = [("dtmin", ctypes.c_double), ("dtc_safe", ctypes.c_double), ("dtu_safe", ctypes.c_double),
                 ("dtv_safe", ctypes.c_double), ("dtdiv_safe", ctypes.c_double)]
+
+
+class RunParams(ctypes.Structure):
+    _fields_ = [("dtmin", ctypes.c_double), ("dtmax", ctypes.c_double), ("dtrise", ctypes.c_double),
+                ("dtc_safe", ctypes.c_double), ("dtu_safe", ctypes.c_double), ("dtv_safe", ctypes.c_double),
+                ("dtdiv_safe", ctypes.c_double), ("end_time", ctypes.c_double), ("end_step", ctypes.c_int),
+                ("summary_frequency", ctypes.c_int), ("fold", ctypes.c_int)]
+
+
+class RunState(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_int), ("advect_x", ctypes.c_int), ("time", ctypes.c_double),
+                ("dtold", ctypes.c_double), ("dt", ctypes.c_double), ("done", ctypes.c_int)]
 
 
 _lib = None
@@ -88,6 +100,7 @@ def library() -> ctypes.CDLL:
         "cb_reset_field": ([P, i], i), "cb_update_halo": ([P, ip, i], i), "cb_field_summary": ([P, dp], i),
         "cb_synchronize": ([P], i), "cb_get_stream": ([P, ctypes.POINTER(P)], i),
         "cb_launch_count": ([P, ctypes.POINTER(ctypes.c_longlong)], i),
+        "cb_run": ([P, ctypes.POINTER(RunParams), ctypes.POINTER(RunState), i, dp, dp, i, ip], i),
         "cb_field_summary_noalloc": ([i, i, ctypes.c_longlong] + [P] * 8 + [d, P, P], i),
         "cb_selftest_width_ratio": ([ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong)], i),
     }
@@ -159,6 +172,16 @@ class Chunk:
         _check(self._L.cb_read_field(self._h, fid, _dptr(out), out.size, LAYOUT_XFAST))
         return out
 
+    def read_into(self, field, out: np.ndarray) -> np.ndarray:
+        """Whole field into `out` ((sy, sx) float64, C-contiguous), e.g. a pinned
+        host buffer, with no intermediate copy."""
+        fid = FIELD_ID[field] if isinstance(field, str) else int(field)
+        sx, sy = self.extent(fid)
+        if out.shape != (sy, sx) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise CloverError(f"read_into {field}: expected a C-contiguous float64 array of shape {(sy, sx)}")
+        _check(self._L.cb_read_field(self._h, fid, _dptr(out), out.size, LAYOUT_XFAST))
+        return out
+
     def write(self, field, arr: np.ndarray):
         fid = FIELD_ID[field] if isinstance(field, str) else int(field)
         sx, sy = self.extent(fid)
@@ -227,6 +250,19 @@ class Chunk:
         out = (ctypes.c_double * 5)()
         _check(self._L.cb_field_summary(self._h, out))
         return tuple(out)
+
+    def run(self, params: RunParams, state: RunState, max_steps: int, max_summaries: int = 0):
+        """cb_run: hydro steps on the device until the run completes or
+        max_steps steps were made; `state` is updated in place.  Returns
+        (dt of each step, summary records (n, 7), total summaries)."""
+        trace = np.zeros(max_steps, dtype=np.float64)
+        recs = np.zeros((max(max_summaries, 1), 7), dtype=np.float64)
+        n = ctypes.c_int()
+        step0 = state.step
+        rc = self._L.cb_run(self._h, ctypes.byref(params), ctypes.byref(state), max_steps, _dptr(trace), _dptr(recs),
+                            max_summaries, ctypes.byref(n))
+        _check(rc)
+        return trace[:state.step - step0], recs[:min(n.value, max_summaries)], n.value
 
     def synchronize(self): _check(self._L.cb_synchronize(self._h))
 

@@ -65,6 +65,9 @@ struct Chunk {
   bool reset_by_swap = false;  // reset_field swaps level buffers instead of copying
 
   long long launches = 0; // kernels launched for this chunk
+  // When set, the phases that take dt (PdV, accelerate, flux_calc) read it
+  // from this device address instead of their argument (cb_run's graph).
+  const double *dt_dev = nullptr;
 
   bool can_fold() const { return fold_enabled && nx >= 8 && ny >= 8; }
   void *base(int f) const { return (char *)buf[fbuf[f]] + off * esize; }

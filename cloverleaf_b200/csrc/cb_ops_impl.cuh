@@ -130,7 +130,7 @@ template <typename T> cudaError_t Ops<T>::pdv(Chunk &c, int predict, double dt, 
   PdvIn in{c.base(DENSITY0), c.base(ENERGY0), c.base(PRESSURE), c.base(VISCOSITY)};
   PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
   Maps mp = maps_of<B::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1});
-  kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, mesh<T>(c), (int)c.off, predict, (T)dt, mode, gm1<T>(c), fold, c.d_err);
+  kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, mesh<T>(c), (int)c.off, predict, (T)dt, c.dt_dev, mode, gm1<T>(c), fold, c.d_err);
   return launched(c);
 }
 
@@ -147,8 +147,8 @@ template <typename T> cudaError_t Ops<T>::accelerate(Chunk &c, double dt, int fo
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
   kt_accelerate<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0}),
-                                                       (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, (T)dt, fold,
-                                                       c.d_err);
+                                                       (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, (T)dt, c.dt_dev,
+                                                       fold, c.d_err);
   return launched(c);
 }
 
@@ -159,7 +159,7 @@ template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fol
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
   kt_flux_calc<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1}), (T *)c.base(VOL_FLUX_X),
-                                                      (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off, (T)dt, fold, c.d_err);
+                                                      (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, fold, c.d_err);
   return launched(c);
 }
 

@@ -425,12 +425,12 @@ __device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, c
 
 template <typename T>
 __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict, T dt,
-                                              int mode, T gm1, int fold, int *err) {
+                                              const double *dtp, int mode, T gm1, int fold, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   TileCtx cx = tile_ctx(&bar, err);
-  pdv_tile(cx, reinterpret_cast<T *>(smraw), map_set(maps, predict ? 2 : 4), in, out, m, off, predict, dt, mode, gm1, fold, blockIdx.x,
-           blockIdx.y);
+  pdv_tile(cx, reinterpret_cast<T *>(smraw), map_set(maps, predict ? 2 : 4), in, out, m, off, predict, dtp ? (T)*dtp : dt, mode, gm1, fold,
+           blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -491,11 +491,12 @@ __device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet
 
 template <typename T>
 __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Maps maps, T *u_out, T *v_out, Mesh<T> m, int off, T dt,
-                                                     int fold, int *err) {
+                                                     const double *dtp, int fold, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   TileCtx cx = tile_ctx(&bar, err);
-  accelerate_tile<T, ACC_TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 5), u_out, v_out, m, off, dt, fold, blockIdx.x, blockIdx.y);
+  accelerate_tile<T, ACC_TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 5), u_out, v_out, m, off, dtp ? (T)*dtp : dt, fold, blockIdx.x,
+                             blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -552,11 +553,12 @@ __device__ __forceinline__ bool flux_calc_tile(TileCtx &cx, T *sm, const MapSet 
 
 template <typename T>
 __global__ void __launch_bounds__(256) kt_flux_calc(const __grid_constant__ Maps maps, T *fx_out, T *fy_out, Mesh<T> m, int off, T dt,
-                                                    int fold, int *err) {
+                                                    const double *dtp, int fold, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   TileCtx cx = tile_ctx(&bar, err);
-  flux_calc_tile<T, FLUX_TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 4), fx_out, fy_out, m, off, dt, fold, blockIdx.x, blockIdx.y);
+  flux_calc_tile<T, FLUX_TY>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 4), fx_out, fy_out, m, off, dtp ? (T)*dtp : dt, fold, blockIdx.x,
+                             blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------

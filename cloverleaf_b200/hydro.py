@@ -15,7 +15,7 @@ from __future__ import annotations
 import dataclasses
 from typing import Callable, List, Optional
 
-from .chunk import Chunk
+from .chunk import Chunk, RunParams, RunState
 from .deck import G_SMALL, G_BIG, Deck
 
 D0, D1, E0, E1, P, Q, C, U0, U1, V0, V1, VFX, VFY, MFX, MFY = range(15)
@@ -141,6 +141,34 @@ class HydroRun:
             self.field_summary()
         self._mark("end")
         return done
+
+    # driver/hydro.cpp:53-111, the whole loop on the device (cb_run)
+    def run_steps_on_device(self, max_steps: Optional[int] = None, chunk_steps: int = 4096) -> bool:
+        """Makes the steps `hydro_step` would make, up to the end of the run or
+        up to step `max_steps`, as device-resident CUDA graphs of at most
+        `chunk_steps` steps each (the host waits once per graph).  Fields, dt
+        sequence and summaries are those of the `hydro_step` loop.  Returns
+        True when the run is complete."""
+        if self.forced_dt is not None or self.probe is not None:
+            raise ValueError("run_steps_on_device: forced_dt and probe need the host-driven loop")
+        d = self.deck
+        p = RunParams(d.dtmin, d.dtmax, d.dtrise, d.dtc_safe, d.dtu_safe, d.dtv_safe, d.dtdiv_safe, d.end_time,
+                      d.end_step, d.summary_frequency, int(self.fold))
+        st = RunState(self.step, int(self.advect_x), self.time, self.dtold, self.dt, 0)
+        last = d.end_step if max_steps is None else min(d.end_step, max_steps)
+        while self.step < last:
+            n = min(chunk_steps, last - self.step)
+            cap = n // d.summary_frequency + 2 if d.summary_frequency > 0 else 2
+            try:
+                trace, recs, _ = self.c.run(p, st, n, cap)
+            finally:
+                self.step, self.time, self.dt, self.dtold = st.step, st.time, st.dt, st.dtold
+                self.advect_x = bool(st.advect_x)
+            self.dt_trace.extend(float(x) for x in trace)
+            self.summaries.extend(Summary(int(r[0]), *(float(x) for x in r[1:])) for r in recs)
+            if st.done:
+                return True
+        return False
 
     def run(self, max_steps: Optional[int] = None, on_step: Optional[Callable[["HydroRun"], None]] = None):
         self.start()

@@ -144,6 +144,50 @@ int cb_get_stream(cb_chunk *c, void **stream);
 int cb_launch_count(const cb_chunk *c, long long *count);
 
 /* ------------------------------------------------------------------------
+ * Whole-run residency: the hydro loop of driver/hydro.cpp:53-111 (the
+ * while loop over hydro steps) run on the device as one CUDA graph, its
+ * host-side logic -- the dt clamp of driver/timestep.cpp:75-96, time, the
+ * end test and the summary schedule of driver/hydro.cpp:87-111 -- moved
+ * into small kernels, so the host waits once for the whole run.  Each step
+ * launches exactly the phases the calls above make for the driver's
+ * sequence (driver/timestep.cpp:37-109, driver/advection.cpp:29-105,
+ * src/serial/PdV.cpp:92-133), with the same halo bookkeeping, and the
+ * fields end bit-identical to that sequence's.  Call it after the start-up
+ * sequence of driver/start.cpp:43-138 (or after any number of steps made
+ * through the phase calls).
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  double dtmin, dtmax, dtrise;                       /* driver/definitions.h:246-249 */
+  double dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;   /* calc_dt's safety factors */
+  double end_time;
+  int end_step;
+  int summary_frequency;                             /* 0: a summary at the end only */
+  int fold;                                          /* 1: producers write the halos the next update_halo
+                                                        needs (halo_depth > 0 in the phase calls); 0: none do */
+} cb_run_params;
+
+/* The driver's loop state (driver/definitions.h:258-280). */
+typedef struct {
+  int step;         /* in: steps made so far; out: after the call */
+  int advect_x;     /* in/out: 1 when the next step sweeps x first */
+  double time;      /* in/out: simulated time */
+  double dtold;     /* in/out: dt of the last step (dtinit before the first) */
+  double dt;        /* out: dt of the last step */
+  int done;         /* out: 1 once time reached end_time or step reached end_step */
+} cb_run_state;
+
+/* Runs hydro steps until the run is complete or max_steps (>= 1) steps were
+ * made.  dt_trace (NULL, or max_steps doubles) receives each step's dt;
+ * summaries (NULL when max_summaries is 0; else 7 doubles per record: step,
+ * time, volume, mass, internal energy, kinetic energy, pressure*volume)
+ * receives the summaries of driver/hydro.cpp:95-111 in order, the first
+ * max_summaries of them; *nsummaries (may be NULL) counts all of them.  A dt
+ * below dtmin returns CB_ESTATE (the state then includes that step, as the
+ * driver's report does). */
+int cb_run(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_steps, double *dt_trace, double *summaries,
+           int max_summaries, int *nsummaries);
+
+/* ------------------------------------------------------------------------
  * Batched ensemble: many independent decks advanced by one persistent
  * kernel launch.  No counterpart in the reference, whose driver runs one
  * deck per process; each deck here follows exactly the per-chunk sequence
