@@ -659,8 +659,11 @@ template <typename T, int DIR, int TY> struct CellLayout {
   }
 };
 
-template <typename T, int DIR, int TY>
-__device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
+// EDGE = false: a tile whose every position lies inside the mesh's extents
+// (no edge_tile), so the extent checks, the upwind clamp and the halo fold
+// drop out.
+template <typename T, int DIR, int TY, bool EDGE>
+__device__ __forceinline__ bool advec_cell_body(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
                                                 int sweep, int fold, int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, YH = L::YH;
@@ -683,7 +686,7 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     L::item(t, L::NPV, LL, p, l);
     const int a = a0 - 1 + p, line = l0 + l;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-    if (i > m.nx + 3 || j > m.ny + 3) continue;
+    if (EDGE && (i > m.nx + 3 || j > m.ny + 3)) continue;
     const int b = bidx(i, j);
     const T vol = m.celldx_t[i] * m.celldy_t[j];
     T pv;
@@ -698,20 +701,20 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
   // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
   const double *vdx = DIR == 1 ? m.vertexdx : m.vertexdy;
   const double *rvdx = DIR == 1 ? m.rvertexdx : m.rvertexdy;
-  const bool edge = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+  const bool edge = EDGE && fold;
   for (int t = tid; t < L::NF * LL; t += 256) {
     int p, l;
     L::item(t, L::NF, LL, p, l);
     const int f = a0 + p, line = l0 + l; // position of the face along the sweep
     const int i = DIR == 1 ? f : line, j = DIR == 1 ? line : f;
-    if (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3)) continue;
+    if (EDGE && (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3))) continue;
     const int b = bidx(i, j);
     const T flux = DIR == 1 ? VFX[b] : VFY[b];
     int upwind, donor, downwind, dif;
     if (flux > T(0.0)) {
       upwind = f - 2; donor = f - 1; downwind = f; dif = donor;
     } else {
-      upwind = (f + 1 < na + 2) ? f + 1 : na + 2;
+      upwind = (!EDGE || f + 1 < na + 2) ? f + 1 : na + 2;
       donor = f; downwind = f - 1; dif = upwind;
     }
     const int bd = b + (donor - f) * ST, bu = b + (upwind - f) * ST, bw = b + (downwind - f) * ST;
@@ -727,7 +730,7 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     s_mf[L::fx(p, l)] = (double)mass_flux;
     s_ef[L::fx(p, l)] = (double)mass_flux * (double)(e_adv);
     T *mf = (T *)out.mass_flux;
-    const bool halo_face = fold && f == na + 3; // with a fold, face na+3 takes its halo value
+    const bool halo_face = EDGE && fold && f == na + 3; // with a fold, face na+3 takes its halo value
     if (!halo_face) mf[gidx(pitch, i, j)] = mass_flux;
     if (edge && f < na + 3) fold_halo(mf, m, halo_rule(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y), fold, i, j, mass_flux);
   }
@@ -738,7 +741,7 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     L::item(t, LA, LL, p, l);
     const int a = a0 + p, line = l0 + l;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-    if (i >= m.nx + 2 || j >= m.ny + 2) continue;
+    if (EDGE && (i >= m.nx + 2 || j >= m.ny + 2)) continue;
     const int b = bidx(i, j);
     const T pre_vol = s_pv[L::pv(p + 1, l)];
     const double mf_lo = s_mf[L::fx(p, l)], mf_hi = s_mf[L::fx(p + 1, l)];
@@ -770,6 +773,14 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     }
   }
   return true;
+}
+
+template <typename T, int DIR, int TY>
+__device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
+                                                int sweep, int fold, int bx, int by) {
+  if (edge_tile(m.nx, m.ny, 2 + bx * TILE_X, 2 + by * TY, TY))
+    return advec_cell_body<T, DIR, TY, true>(cx, sm, ms, out, m, off, sweep, fold, bx, by);
+  return advec_cell_body<T, DIR, TY, false>(cx, sm, ms, out, m, off, sweep, fold, bx, by);
 }
 
 // Five blocks per SM: the register budget that keeps the staged boxes of
@@ -877,8 +888,10 @@ template <typename T, int DIR, int TY> struct MomLayout {
   }
 };
 
-template <typename T, int DIR, int TY>
-__device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
+// EDGE = false: a tile whose every position lies inside the mesh's extents
+// (no edge_tile), so the extent checks and the halo fold drop out.
+template <typename T, int DIR, int TY, bool EDGE>
+__device__ __forceinline__ bool advec_mom_body(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
                                                int vel_mask, int sweep, int fold, int bx, int by) {
   using L = MomLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, NP = L::NP, YH = L::YH;
@@ -909,7 +922,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
       int p, lc;
       L::item(t, NP, LL + 1, p, lc);
       const int a = a0 - 2 + p, line = l0 - 1 + lc;
-      if (a >= 0 && a <= na + 3 && line >= 0 && line <= nlmax + 3) {
+      if (!EDGE || (a >= 0 && a <= na + 3 && line >= 0 && line <= nlmax + 3)) {
         const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
         const int b = bidx(i, j);
         const T vol = m.celldx_t[i] * m.celldy_t[j];
@@ -928,7 +941,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
       int p, l;
       L::item(t, NP, LL, p, l);
       const int a = a0 - 2 + p, line = l0 + l;
-      if (line < nlmax + 3 && a >= 0 && a <= na + 3) {
+      if (!EDGE || (line < nlmax + 3 && a >= 0 && a <= na + 3)) {
         const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
         // (:84-88 / :156-160) dir 1: mf(a, j-1) + mf(a, j) + mf(a+1, j-1) + mf(a+1, j); dir 2: mf(i-1, a) + mf(i, a) + mf(i-1, a+1) + mf(i, a+1)
         v = quarter_sum(MF[b - SL], MF[b], MF[b + ST - SL], MF[b + ST]);
@@ -970,7 +983,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
     p += 1;
     const int a = a0 - 2 + p, line = l0 + l;
     T nmpre = T(1.0);
-    if (line < nlmax + 3 && a >= 1 && a <= na + 3) nmpre = mom_node_mass_pre(node_mass_post(p, l), s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]);
+    if (!EDGE || (line < nlmax + 3 && a >= 1 && a <= na + 3)) nmpre = mom_node_mass_pre(node_mass_post(p, l), s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]);
     s_nmpre[L::w(p, l)] = nmpre;
   }
   __syncthreads();
@@ -982,7 +995,7 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
     L::item(t, LA + 1, LL, p, l);
     p += 1;
     const int a = a0 - 2 + p, line = l0 + l;
-    if (line >= nlmax + 3 || a < 1 || a > na + 2) continue;
+    if (EDGE && (line >= nlmax + 3 || a < 1 || a > na + 2)) continue;
     const T nfv = s_nf[L::w(p, l)];
     int upwind, donor, downwind, dif;
     if (nfv < T(0.0)) {
@@ -1001,13 +1014,13 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
   __syncthreads();
 
   // (4) velocity update (:139-144 / :211-216) over positions 2 .. LA+1
-  const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+  const bool do_fold = EDGE && fold;
   for (int t = tid; t < LA * LL; t += 256) {
     int p, l;
     L::item(t, LA, LL, p, l);
     p += 2;
     const int a = a0 - 2 + p, line = l0 + l;
-    if (line > nlmax + 2 || a > na + 2) continue;
+    if (EDGE && (line > nlmax + 2 || a > na + 2)) continue;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
     const int b = bidx(i, j);
     const T nmpre = s_nmpre[L::w(p, l)], nmpost = node_mass_post(p, l);
@@ -1024,6 +1037,14 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
     }
   }
   return true;
+}
+
+template <typename T, int DIR, int TY>
+__device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
+                                               int vel_mask, int sweep, int fold, int bx, int by) {
+  if (edge_tile(m.nx, m.ny, 2 + bx * TILE_X, 2 + by * TY, TY))
+    return advec_mom_body<T, DIR, TY, true>(cx, sm, ms, out, m, off, vel_mask, sweep, fold, bx, by);
+  return advec_mom_body<T, DIR, TY, false>(cx, sm, ms, out, m, off, vel_mask, sweep, fold, bx, by);
 }
 
 template <typename T, int DIR, int TY>
