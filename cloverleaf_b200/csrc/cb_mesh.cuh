@@ -9,6 +9,8 @@
 // boundary: element (i, j) lives at base[j * pitch + i].
 #pragma once
 
+#include <type_traits>
+
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -77,6 +79,22 @@ __host__ __device__ inline HaloRule halo_rule(int f) {
 // use the exact operator.
 template <typename T> __device__ __forceinline__ T lim_div(T a, T b) { return a / b; }
 template <> __device__ __forceinline__ float lim_div<float>(float a, float b) { return __fdividef(a, b); }
+
+// a / b where a is often exactly zero (the fluxes of faces and nodes the
+// flow has not reached): for a zero and b positive the quotient is a itself,
+// its sign included.  When that holds on every active lane of the warp the
+// division is skipped (a branch the warp takes together); otherwise each
+// lane takes a or the division operator's quotient, the same bits.  For
+// arithmetic types only: the tangent-linear number types divide with their
+// own operator.
+template <typename T> __device__ __forceinline__ T div_zero_num(T a, T b) {
+  if constexpr (std::is_floating_point<T>::value) {
+    const bool zero = a == T(0.0) && b > T(0.0);
+    if (__all_sync(__activemask(), zero)) return a; // a branch the warp takes together
+    return zero ? a : a / b;
+  }
+  return a / b;
+}
 
 // x / w for positive mesh widths x and w, given r = 1 / w rounded to nearest
 // (computed on the host), by correction steps q <- RN(q + (x - q w) r) with

@@ -605,13 +605,13 @@ template <typename T> __device__ __forceinline__ T cell_pre_vol2(T vol, T a_lo, 
 // flux is mass_flux * e_adv.
 template <typename T>
 __device__ __forceinline__ void cell_face_value(T flux, T pre_vol_d, T ratio, T dd, T du, T dw, T ed, T eu, T ew, T &mass_flux, T &e_adv) {
-  T sigmat = lim_div(fabs(flux), pre_vol_d);
+  T sigmat = sizeof(T) == sizeof(double) ? div_zero_num(fabs(flux), pre_vol_d) : lim_div(fabs(flux), pre_vol_d);
   T sigma3 = (T(1.0) + sigmat) * ratio;
   T sigma4 = T(2.0) - sigmat;
   T sigmav = sigmat;
   T limiter = cell_limiter_value(sigmav, sigma3, sigma4, dd - du, dw - dd);
   mass_flux = flux * (dd + limiter);
-  T sigmam = lim_div(fabs(mass_flux), dd * pre_vol_d);
+  T sigmam = sizeof(T) == sizeof(double) ? div_zero_num(fabs(mass_flux), dd * pre_vol_d) : lim_div(fabs(mass_flux), dd * pre_vol_d);
   limiter = cell_limiter_value(sigmam, sigma3, sigma4, ed - eu, ew - ed);
   e_adv = ed + limiter;
 }
@@ -843,7 +843,7 @@ template <typename T> __device__ __forceinline__ T mom_node_mass_pre(T post, T n
 
 // sigma of a node's momentum flux (:120 / :192).
 template <typename T> __device__ __forceinline__ T mom_sigma(T node_flux, T node_mass_pre_donor) {
-  return lim_div(fabs(node_flux), node_mass_pre_donor);
+  return sizeof(T) == sizeof(double) ? div_zero_num(fabs(node_flux), node_mass_pre_donor) : lim_div(fabs(node_flux), node_mass_pre_donor);
 }
 
 // Momentum flux of one velocity component (:121-133 / :193-205): vd, vu, vw
@@ -855,7 +855,7 @@ template <typename T> __device__ __forceinline__ T mom_flux_value(T sigma, T nod
 
 // Velocity update (:139-144 / :211-216).
 template <typename T> __device__ __forceinline__ T mom_update_value(T vel, T nm_pre, T nm_post, T mf_lo, T mf_hi) {
-  return (vel * nm_pre + mf_lo - mf_hi) / (nm_post);
+  return div_zero_num(vel * nm_pre + mf_lo - mf_hi, nm_post);
 }
 
 struct MomOut {
