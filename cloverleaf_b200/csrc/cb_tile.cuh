@@ -84,6 +84,9 @@ __device__ __forceinline__ bool stage(TileCtx &cx, T *sm, const MapSet &ms, int 
   if (cx.fresh && leader) mbar_init(cx.bar, 1);
   __syncthreads(); // barrier initialised; the previous tile's readers are done with the boxes
   if (leader) {
+    // the block's generic-proxy accesses to the boxes (reads, and the work
+    // arrays some tiles write over them) come before the copies' writes
+    if (!cx.fresh) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(cx.bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
     for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, ms.m[f], xs, ys, cx.bar);
   }
@@ -647,7 +650,8 @@ template <typename T, int DIR, int TY> struct CellLayout {
   static constexpr int BOX = BOX_X * BH;
   static constexpr int BOXS = (BOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
   static constexpr int NPV = LA + 2, NF = LA + 1;
-  static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + (size_t)2 * NF * LL * sizeof(double) + (size_t)NPV * LL * sizeof(T);
+  static constexpr size_t SCRATCH_BYTES = (size_t)2 * NF * LL * sizeof(double) + (size_t)NPV * LL * sizeof(T);
+  static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + SCRATCH_BYTES;
   __device__ static constexpr int pv(int p, int l) { return DIR == 1 ? l * NPV + p : p * LL + l; } // p = cell + 1
   __device__ static constexpr int fx(int p, int l) { return DIR == 1 ? l * NF + p : p * LL + l; }  // p = face
   __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
@@ -662,17 +666,18 @@ template <typename T, int DIR, int TY> struct CellLayout {
 // EDGE = false: a tile whose every position lies inside the mesh's extents
 // (no edge_tile), so the extent checks, the upwind clamp and the halo fold
 // drop out.
+// The tile's work once its boxes are staged at `sm` (density1, energy1,
+// vol_flux_x, vol_flux_y, L::BOXS elements apart); `scratch` holds the face
+// fluxes and pre_vol (L::SCRATCH_BYTES).
 template <typename T, int DIR, int TY, bool EDGE>
-__device__ __forceinline__ bool advec_cell_body(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
-                                                int sweep, int fold, int bx, int by) {
+__device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, const CellOut &out, const Mesh<T> &m, int sweep, int fold,
+                                                   int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, YH = L::YH;
-  double *s_mf = reinterpret_cast<double *>(sm + 4 * L::BOXS);
+  double *s_mf = reinterpret_cast<double *>(scratch);
   double *s_ef = s_mf + L::NF * LL;
   T *s_pv = reinterpret_cast<T *>(s_ef + L::NF * LL);
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  const int nf = (sweep == 1) ? 4 : (DIR == 1 ? 3 : 4); // sweep 2 of x needs no y fluxes
-  if (!stage(cx, sm, ms, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH)) return false;
   const T *D1 = sm, *E1 = sm + L::BOXS, *VFX = sm + 2 * L::BOXS, *VFY = sm + 3 * L::BOXS;
   const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
@@ -772,15 +777,23 @@ __device__ __forceinline__ bool advec_cell_body(TileCtx &cx, T *sm, const MapSet
       fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, enew);
     }
   }
-  return true;
 }
 
+// Fields the cell sweep stages: sweep 2 of x needs no y fluxes.
+template <int DIR> __device__ __forceinline__ int cell_staged(int sweep) { return (sweep == 1) ? 4 : (DIR == 1 ? 3 : 4); }
+
+// One tile: staging, then the work (an edge tile keeps the extent checks).
 template <typename T, int DIR, int TY>
 __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
                                                 int sweep, int fold, int bx, int by) {
-  if (edge_tile(m.nx, m.ny, 2 + bx * TILE_X, 2 + by * TY, TY))
-    return advec_cell_body<T, DIR, TY, true>(cx, sm, ms, out, m, off, sweep, fold, bx, by);
-  return advec_cell_body<T, DIR, TY, false>(cx, sm, ms, out, m, off, sweep, fold, bx, by);
+  using L = CellLayout<T, DIR, TY>;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  if (!stage(cx, sm, ms, cell_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH)) return false;
+  if (edge_tile(m.nx, m.ny, x0, y0, TY))
+    advec_cell_compute<T, DIR, TY, true>(sm, sm + 4 * L::BOXS, out, m, sweep, fold, bx, by);
+  else
+    advec_cell_compute<T, DIR, TY, false>(sm, sm + 4 * L::BOXS, out, m, sweep, fold, bx, by);
+  return true;
 }
 
 // Five blocks per SM: the register budget that keeps the staged boxes of
@@ -890,15 +903,15 @@ template <typename T, int DIR, int TY> struct MomLayout {
 
 // EDGE = false: a tile whose every position lies inside the mesh's extents
 // (no edge_tile), so the extent checks and the halo fold drop out.
+// The tile's work once its boxes are staged at `sm` (L::SMEM bytes: the
+// boxes, then the work arrays over the boxes the first stage consumes).
 template <typename T, int DIR, int TY, bool EDGE>
-__device__ __forceinline__ bool advec_mom_body(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
-                                               int vel_mask, int sweep, int fold, int bx, int by) {
+__device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, const Mesh<T> &m, int vel_mask, int sweep, int fold, int bx,
+                                                  int by) {
   using L = MomLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, NP = L::NP, YH = L::YH;
   const int mom_sweep = DIR + 2 * (sweep - 1);
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  const int nf = mom_sweep <= 2 ? 5 : 4;
-  if (!stage(cx, sm, ms, nf, L::BOXS, L::BH, off + x0 - HALO, y0 - YH)) return false;
   const T *U1 = sm, *V1 = sm + L::BOXS, *D1 = sm + 2 * L::BOXS, *MF = sm + 3 * L::BOXS, *VFO = sm + 4 * L::BOXS;
   T *region = sm + 2 * L::BOXS;
   T *s_cm = region, *s_nf = s_cm + L::N_CM, *s_nmpre = s_nf + L::N_W, *s_mfu = s_nmpre + L::N_W, *s_mfv = s_mfu + L::N_W;
@@ -1036,15 +1049,23 @@ __device__ __forceinline__ bool advec_mom_body(TileCtx &cx, T *sm, const MapSet 
       if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
     }
   }
-  return true;
 }
 
+// Fields the momentum sweep stages: the other direction's volume flux only for mom_sweep 1 and 2.
+template <int DIR> __device__ __forceinline__ int mom_staged(int sweep) { return DIR + 2 * (sweep - 1) <= 2 ? 5 : 4; }
+
+// One tile: staging, then the work (an edge tile keeps the extent checks).
 template <typename T, int DIR, int TY>
 __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
                                                int vel_mask, int sweep, int fold, int bx, int by) {
-  if (edge_tile(m.nx, m.ny, 2 + bx * TILE_X, 2 + by * TY, TY))
-    return advec_mom_body<T, DIR, TY, true>(cx, sm, ms, out, m, off, vel_mask, sweep, fold, bx, by);
-  return advec_mom_body<T, DIR, TY, false>(cx, sm, ms, out, m, off, vel_mask, sweep, fold, bx, by);
+  using L = MomLayout<T, DIR, TY>;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  if (!stage(cx, sm, ms, mom_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH)) return false;
+  if (edge_tile(m.nx, m.ny, x0, y0, TY))
+    advec_mom_compute<T, DIR, TY, true>(sm, out, m, vel_mask, sweep, fold, bx, by);
+  else
+    advec_mom_compute<T, DIR, TY, false>(sm, out, m, vel_mask, sweep, fold, bx, by);
+  return true;
 }
 
 template <typename T, int DIR, int TY>
