@@ -334,6 +334,21 @@ __device__ __forceinline__ void pdv_value(bool predict, T dt, T xa, T ya, T vol,
     top_flux = (ya_t * (v01 + v11 + z01 + z11)) * T(0.25) * dt;
   }
   T total_flux = right_flux - left_flux + top_flux - bottom_flux;
+  if constexpr (std::is_floating_point<T>::value) {
+    // A cell no flux crosses: volume_change = vol / vol = 1 exactly and
+    // energy_change is a signed zero, so density1 = d0 and energy1 = e0 to
+    // the bit -- given a finite positive vol, quotients p / d0 and q / d0
+    // that cannot overflow (bounds below) and a normal e0.  When that holds
+    // on every active lane of the warp, the four divisions are skipped.
+    const T lo = T(0x1p-60), hi = T(0x1p60);
+    const bool still = total_flux == T(0.0) && vol >= lo && vol <= hi && d0 >= lo && d0 <= hi && fabs(p) <= hi && fabs(q) <= hi &&
+                       fabs(e0) >= lo && fabs(e0) <= hi;
+    if (__all_sync(__activemask(), still)) {
+      density1 = d0;
+      energy1 = e0;
+      return;
+    }
+  }
   T volume_change_s = (vol) / (vol + total_flux);
   T recip_volume = (T(1.0)) / (vol);
   T energy_change = ((p) / (d0) + (q) / (d0)) * total_flux * recip_volume;
@@ -446,11 +461,31 @@ template <typename T>
 __device__ __forceinline__ void accel_value(T halfdt, T vol_mm, T vol_m0, T vol_00, T vol_0m, T xa, T xa_m, T ya, T ya_m, T d_mm, T d_m0,
                                             T d_00, T d_0m, T p_00, T p_m0, T p_0m, T p_mm, T q_00, T q_m0, T q_0m, T q_mm, T u0, T v0, T &u,
                                             T &v) {
-  T stepbymass_s = (halfdt) / (((d_mm * vol_mm + d_m0 * vol_m0 + d_00 * vol_00 + d_0m * vol_0m) * T(0.25)));
-  u = u0 - stepbymass_s * (xa * (p_00 - p_m0) + xa_m * (p_0m - p_mm));
-  v = v0 - stepbymass_s * (ya * (p_00 - p_0m) + ya_m * (p_m0 - p_mm));
-  u = u - stepbymass_s * (xa * (q_00 - q_m0) + xa_m * (q_0m - q_mm));
-  v = v - stepbymass_s * (ya * (q_00 - q_0m) + ya_m * (q_m0 - q_mm));
+  const T nodal_mass = (d_mm * vol_mm + d_m0 * vol_m0 + d_00 * vol_00 + d_0m * vol_0m) * T(0.25);
+  const T fu_p = xa * (p_00 - p_m0) + xa_m * (p_0m - p_mm), fv_p = ya * (p_00 - p_0m) + ya_m * (p_m0 - p_mm);
+  const T fu_q = xa * (q_00 - q_m0) + xa_m * (q_0m - q_mm), fv_q = ya * (q_00 - q_0m) + ya_m * (q_m0 - q_mm);
+  T stepbymass_s;
+  if constexpr (std::is_same<T, double>::value) {
+    // A node no force acts on (every pressure and viscosity term a signed
+    // zero): stepbymass times each term is that same signed zero for any
+    // positive finite stepbymass (the bounds below keep it finite), so 1
+    // stands in for it -- the velocities come out to the bit -- and, when
+    // that holds on every active lane of the warp, the division is skipped.
+    // (FP64 only: the single-precision quotient is cheaper than the test.)
+    const T lo = T(0x1p-60), hi = T(0x1p60);
+    const bool still = fu_p == T(0.0) && fv_p == T(0.0) && fu_q == T(0.0) && fv_q == T(0.0) && halfdt > T(0.0) && halfdt <= hi &&
+                       nodal_mass >= lo;
+    if (__all_sync(__activemask(), still))
+      stepbymass_s = T(1.0);
+    else
+      stepbymass_s = (halfdt) / (nodal_mass);
+  } else {
+    stepbymass_s = (halfdt) / (nodal_mass);
+  }
+  u = u0 - stepbymass_s * fu_p;
+  v = v0 - stepbymass_s * fv_p;
+  u = u - stepbymass_s * fu_q;
+  v = v - stepbymass_s * fv_q;
 }
 
 // One tile of TY node rows; the one-launch kernel uses TY = ACC_TY.
