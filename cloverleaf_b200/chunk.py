@@ -60,7 +60,7 @@ class RunParams(ctypes.Structure):
     _fields_ = [("dtmin", ctypes.c_double), ("dtmax", ctypes.c_double), ("dtrise", ctypes.c_double),
                 ("dtc_safe", ctypes.c_double), ("dtu_safe", ctypes.c_double), ("dtv_safe", ctypes.c_double),
                 ("dtdiv_safe", ctypes.c_double), ("end_time", ctypes.c_double), ("end_step", ctypes.c_int),
-                ("summary_frequency", ctypes.c_int), ("fold", ctypes.c_int)]
+                ("summary_frequency", ctypes.c_int), ("fold", ctypes.c_int), ("fuse", ctypes.c_int)]
 
 
 class RunState(ctypes.Structure):

@@ -35,11 +35,15 @@ template <typename T> struct Ops {
   static cudaError_t revert(Chunk &c);
   static cudaError_t accelerate(Chunk &c, double dt, int fold);
   static cudaError_t flux_calc(Chunk &c, double dt, int fold);
-  static cudaError_t advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de);
-  static cudaError_t advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv);
+  // reset_fold >= 0: the sweep also does reset_field's copy of what it writes (fold depth reset_fold)
+  static cudaError_t advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de, int reset_fold = -1);
+  static cudaError_t advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv, int reset_fold = -1);
   static cudaError_t reset_field(Chunk &c, int fold);
   static cudaError_t update_halo(Chunk &c, const HaloJob &job, int depth);
   static cudaError_t field_summary(Chunk &c);
+  // fused passes of the resident loop: viscosity + calc_dt, PdV corrector + flux_calc
+  static cudaError_t visc_dt(Chunk &c, const DtConsts &k, int fold);
+  static cudaError_t pdv_flux(Chunk &c, double dt, int fold, int flux_fold);
 };
 
 extern template struct Ops<double>;

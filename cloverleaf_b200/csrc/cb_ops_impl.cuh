@@ -164,9 +164,14 @@ template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fol
 }
 
 
-template <typename T, int DIR, int TY> cudaError_t launch_advec_cell(Chunk &c, int sweep, int fold, void *dd, void *de) {
+template <typename T, int DIR, int TY> cudaError_t launch_advec_cell(Chunk &c, int sweep, int fold, void *dd, void *de, int reset_fold) {
   using L = CellLayout<T, DIR, TY>;
   CellOut out{dd, de, c.base(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
+  if (reset_fold >= 0) {
+    out.density0 = c.base(DENSITY0);
+    out.energy0 = c.base(ENERGY0);
+    out.rfold = reset_fold;
+  }
   Maps mp = maps_of<L::BH>(c, {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y});
   cudaError_t e = allow_smem(kt_advec_cell<T, DIR, TY>, L::SMEM);
   if (e != cudaSuccess) return e;
@@ -176,20 +181,20 @@ template <typename T, int DIR, int TY> cudaError_t launch_advec_cell(Chunk &c, i
 }
 
 // dir 1 = x, 2 = y.  The updated density/energy go to (dd, de); the caller swaps buffers.
-template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de) {
+template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de, int reset_fold) {
   const T *sd = (const T *)c.base(DENSITY1), *se = (const T *)c.base(ENERGY1);
   cudaError_t e;
   if (fold != 2) { // keep the halo ring exactly as the in-place reference leaves it
     RingPair rp{{sd, se}, {dd, de}};
     if ((e = copy_ring<T>(c, rp, 2, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
   }
-  return dir == 1 ? launch_advec_cell<T, 1, AdvecTiles<T>::CELL_X>(c, sweep, fold, dd, de)
-                  : launch_advec_cell<T, 2, AdvecTiles<T>::CELL_Y>(c, sweep, fold, dd, de);
+  return dir == 1 ? launch_advec_cell<T, 1, AdvecTiles<T>::CELL_X>(c, sweep, fold, dd, de, reset_fold)
+                  : launch_advec_cell<T, 2, AdvecTiles<T>::CELL_Y>(c, sweep, fold, dd, de, reset_fold);
 }
 
 
 template <typename T, int DIR, int TY>
-cudaError_t launch_advec_mom(Chunk &c, int vel_mask, int sweep, int fold, void *du, void *dv) {
+cudaError_t launch_advec_mom(Chunk &c, int vel_mask, int sweep, int fold, void *du, void *dv, int reset_fold) {
   using L = MomLayout<T, DIR, TY>;
   const int mom_sweep = DIR + 2 * (sweep - 1);
   const int mf = DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y;
@@ -200,12 +205,18 @@ cudaError_t launch_advec_mom(Chunk &c, int vel_mask, int sweep, int fold, void *
   if (e != cudaSuccess) return e;
   // nodes [2, n+2] along both axes: n+1 of them
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  kt_advec_mom<T, DIR, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(mp, MomOut{du, dv}, mesh<T>(c), (int)c.off, vel_mask, sweep, fold,
-                                                                  c.d_err);
+  MomOut out{du, dv};
+  if (reset_fold >= 0) {
+    out.xvel0 = (vel_mask & 1) ? c.base(XVEL0) : nullptr;
+    out.yvel0 = (vel_mask & 2) ? c.base(YVEL0) : nullptr;
+    out.rfold = reset_fold;
+  }
+  kt_advec_mom<T, DIR, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(mp, out, mesh<T>(c), (int)c.off, vel_mask, sweep, fold, c.d_err);
   return launched(c);
 }
 
-template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv) {
+template <typename T>
+cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv, int reset_fold) {
   const T *su = (const T *)c.base(XVEL1), *sv = (const T *)c.base(YVEL1);
   cudaError_t e;
   if (fold != 2) {
@@ -215,8 +226,8 @@ template <typename T> cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int 
     if (vel_mask & 2) rp.src[n] = sv, rp.dst[n++] = dv;
     if ((e = copy_ring<T>(c, rp, n, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
   }
-  return dir == 1 ? launch_advec_mom<T, 1, AdvecTiles<T>::MOM_X>(c, vel_mask, sweep, fold, du, dv)
-                  : launch_advec_mom<T, 2, AdvecTiles<T>::MOM_Y>(c, vel_mask, sweep, fold, du, dv);
+  return dir == 1 ? launch_advec_mom<T, 1, AdvecTiles<T>::MOM_X>(c, vel_mask, sweep, fold, du, dv, reset_fold)
+                  : launch_advec_mom<T, 2, AdvecTiles<T>::MOM_Y>(c, vel_mask, sweep, fold, du, dv, reset_fold);
 }
 
 template <typename T> cudaError_t Ops<T>::reset_field(Chunk &c, int fold) {
@@ -235,6 +246,38 @@ template <typename T> cudaError_t Ops<T>::update_halo(Chunk &c, const HaloJob &j
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+template <typename T> cudaError_t Ops<T>::visc_dt(Chunk &c, const DtConsts &k, int fold) {
+  constexpr int TY = VISC_TY;
+  using B = Box1<T, TY>;
+  const size_t smem = 3 * B::BOXS * sizeof(T);
+  cudaError_t e = allow_smem(kt_visc_dt<T>, smem);
+  if (e != cudaSuccess) return e;
+  const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt_visc_dt<T>, 256, smem)) != cudaSuccess) return e;
+  const int grid = std::min(nt, c.sms * std::max(per_sm, 1));
+  DtIn in{c.base(SOUNDSPEED), c.base(VISCOSITY), c.base(DENSITY0)};
+  kt_visc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {PRESSURE, XVEL0, YVEL0}), in, (T *)c.base(VISCOSITY), mesh<T>(c),
+                                                       (int)c.off, k, fold, tx, nt, c.d_dt_bits, c.d_err);
+  return launched(c);
+}
+
+template <typename T> cudaError_t Ops<T>::pdv_flux(Chunk &c, double dt, int fold, int flux_fold) {
+  constexpr int TY = PDV_TY;
+  using B = Box1<T, TY>;
+  const size_t smem = 4 * B::BOXS * sizeof(T);
+  cudaError_t e = allow_smem(kt_pdv_flux<T>, smem);
+  if (e != cudaSuccess) return e;
+  // the faces reach one column and one row past the cells
+  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
+  PdvIn in{c.base(DENSITY0), c.base(ENERGY0), c.base(PRESSURE), c.base(VISCOSITY)};
+  PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
+  Maps mp = maps_of<B::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1});
+  kt_pdv_flux<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, (T *)c.base(VOL_FLUX_X), (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off,
+                                                     (T)dt, c.dt_dev, fold, flux_fold, c.d_err);
+  return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::field_summary(Chunk &c) {

@@ -158,6 +158,10 @@ template <typename T> struct Seq {
   unsigned written = 0;
   std::vector<Pass> passes;
   cudaError_t err = cudaSuccess;
+  // fused emission (only with every producer folding): viscosity + calc_dt
+  // in one pass, the PdV corrector + flux_calc in one pass, and reset_field
+  // done by the second sweeps; the freshness moves exactly as unfused
+  bool fuse = false;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
 
@@ -195,10 +199,10 @@ template <typename T> struct Seq {
     wrote({SS}, 0);
     halo({P, E0, D0, U0, V0}, 1);
     const int fv = eff(dep(1));
-    if (emit) run(Ops<T>::viscosity(c, fv));
+    if (emit && !fuse) run(Ops<T>::viscosity(c, fv));
     wrote({Q}, fv);
-    halo({Q}, 1);
-    if (emit) run(Ops<T>::calc_dt(c, dk));
+    halo({Q}, 1); // (no pass when fused: q is fresh to depth 1)
+    if (emit) run(fuse ? Ops<T>::visc_dt(c, dk, fv) : Ops<T>::calc_dt(c, dk));
     ++pos;
   }
   // driver/hydro.cpp:69-75 and src/serial/PdV.cpp:92-133, dt from the device
@@ -219,24 +223,26 @@ template <typename T> struct Seq {
     if (emit) run(Ops<T>::accelerate(c, 0.0, fa));
     wrote({U1, V1}, fa);
     const int fc = eff(dep(2));
-    if (emit) run(Ops<T>::pdv(c, 0, 0.0, 0, fc));
-    wrote({D1, E1}, fc);
     const int ff = eff(dep(2));
-    if (emit) run(Ops<T>::flux_calc(c, 0.0, ff));
+    if (emit) run(fuse ? Ops<T>::pdv_flux(c, 0.0, fc, ff) : Ops<T>::pdv(c, 0, 0.0, 0, fc));
+    wrote({D1, E1}, fc);
+    if (emit && !fuse) run(Ops<T>::flux_calc(c, 0.0, ff));
     wrote({VFX, VFY}, ff);
   }
+  // fold depth of reset_field, which a fused second sweep does
+  int reset_tail(bool last) const { return fuse && last ? eff(dep(1)) : -1; }
   // cb_advec_cell with its buffer swap
-  void cell(int sweep, int dir) {
+  void cell(int sweep, int dir, bool last = false) {
     const int f = eff(dep(2));
-    if (emit) run(Ops<T>::advec_cell(c, sweep, dir, f, c.spare_base(0), c.spare_base(1)));
+    if (emit) run(Ops<T>::advec_cell(c, sweep, dir, f, c.spare_base(0), c.spare_base(1), reset_tail(last)));
     std::swap(c.fbuf[DENSITY1], c.sbuf[0]);
     std::swap(c.fbuf[ENERGY1], c.sbuf[1]);
     wrote({D1, E1, dir == 1 ? MFX : MFY}, f);
   }
   // cb_advec_mom of both velocities with its buffer swaps
-  void mom(int sweep, int dir, int depth) {
+  void mom(int sweep, int dir, int depth, bool last = false) {
     const int f = eff(depth);
-    if (emit) run(Ops<T>::advec_mom(c, 3, sweep, dir, f, c.spare_base(2), c.spare_base(3)));
+    if (emit) run(Ops<T>::advec_mom(c, 3, sweep, dir, f, c.spare_base(2), c.spare_base(3), reset_tail(last)));
     std::swap(c.fbuf[XVEL1], c.sbuf[2]);
     std::swap(c.fbuf[YVEL1], c.sbuf[3]);
     wrote({U1, V1}, f);
@@ -248,13 +254,13 @@ template <typename T> struct Seq {
     cell(1, d1);
     halo({D1, E1, U1, V1, MFX, MFY}, 2);
     mom(1, d1, dep(2));
-    cell(2, d2);
+    cell(2, d2, true);
     halo({D1, E1, U1, V1, MFX, MFY}, 2);
-    mom(2, d2, 0);
+    mom(2, d2, 0, true);
   }
   void reset() {
     const int f = eff(dep(1));
-    if (emit) run(Ops<T>::reset_field(c, f));
+    if (emit && !fuse) run(Ops<T>::reset_field(c, f));
     wrote({D0, E0, U0, V0}, f);
   }
   // cb_field_summary
@@ -494,6 +500,7 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
     return cuda_fail(e, "cb_run");
   }
   Seq<T> q(*c, true, fold, dk);
+  q.fuse = p->fuse != 0 && fold && c->can_fold();
   std::memcpy(q.fresh, settled[3], sizeof q.fresh);
   const cudaStream_t user = c->stream;
   const long long launches0 = c->launches;

@@ -314,6 +314,83 @@ __global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Map
 }
 
 // ---------------------------------------------------------------------------
+// viscosity and calc_dt in one pass (the resident loop): a tile's q is
+// computed and stored as viscosity_tile does, then used for the tile's dt as
+// calc_dt_tile uses the stored q -- the same values and the same minimum as
+// the two phases one after the other, with one staging of xvel0 / yvel0 and
+// one read of density0.  Staged: ms 0 pressure, 1 xvel0, 2 yvel0.
+static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height");
+
+template <typename T>
+__device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, T *q_out, const Mesh<T> &m, int off,
+                                             const DtConsts &k, int fold, int bx, int by, double &vmin) {
+  constexpr int TY = VISC_TY;
+  using B = Box1<T, TY>;
+  const T *S = (const T *)in.soundspeed, *R = (const T *)in.density0;
+  const int pitch = (int)m.pitch;
+  constexpr int RPT = TY / 4;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  const int i = x0 + threadIdx.x;
+  T ss[RPT], dd[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
+    const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
+    const int g = gidx(pitch, i, j);
+    ss[r] = in_mesh ? S[g] : T(0);
+    dd[r] = in_mesh ? R[g] : T(1);
+  }
+  if (!stage(cx, sm, ms, 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  const T *P = sm, *U = sm + B::BOXS, *V = sm + 2 * B::BOXS;
+  const double thr = sizeof(T) == sizeof(double) ? warp_min(vmin) * DT_SKIP : 0.0;
+  if (i < m.nx + 2) {
+    const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+    const T cdx = m.celldx_t[i], cdx1 = m.celldx_t[i + 1];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const int j = y0 + threadIdx.y + 4 * r;
+      if (j >= m.ny + 2) break;
+      const int b = B::at(i, j, x0, y0);
+      const T cdy = m.celldy_t[j];
+      const T q = viscosity_value(U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1], P[b - 1],
+                                  P[b + 1], P[b - BOX_X], P[b + BOX_X], dd[r], cdx, cdx1, cdy, m.celldy_t[j + 2]);
+      q_out[gidx(pitch, i, j)] = q;
+      if (do_fold) fold_halo(q_out, m, halo_rule(VISCOSITY), fold, i, j, q);
+      if constexpr (sizeof(T) == sizeof(double)) {
+        const double est = dt_estimate(ss[r], q, dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
+                                       V[b + BOX_X + 1], cdx, cdy, k);
+        if (est > thr) continue; // NaN estimates fall through to the exact value
+      }
+      const double c = (double)dt_value(ss[r], q, dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
+                                        V[b + BOX_X + 1], cdx, cdy, k);
+      vmin = fmin(c, vmin);
+    }
+  }
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 4) kt_visc_dt(const __grid_constant__ Maps maps, DtIn in, T *q_out, Mesh<T> m, int off, DtConsts k,
+                                                  int fold, int tiles_x, int ntiles, unsigned long long *dt_bits, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  T *sm = reinterpret_cast<T *>(smraw);
+  TileCtx cx = tile_ctx(&bar, err);
+  const MapSet ms = map_set(maps, 3);
+  double vmin = g_big;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    if (!visc_dt_tile(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin)) return;
+  block_min_to(vmin, dt_bits);
+}
+
+// Volume flux through a face (src/serial/flux_calc.cpp:33-40): width is
+// xarea (celldy) for x faces, yarea (celldx) for y faces; a0, a1 the level-0
+// velocities of the face's two nodes, b0, b1 the level-1 ones.
+template <typename T> __device__ __forceinline__ T flux_value(T dt, T width, T a0, T a1, T b0, T b1) {
+  return T(0.25) * dt * width * (a0 + a1 + b0 + b1);
+}
+
+// ---------------------------------------------------------------------------
 // PdV: src/serial/PdV.cpp:36-87; mode 1 also does the predictor's
 // ideal_gas, pressure halo and revert (:92-133) in the same pass.
 template <typename T>
@@ -378,9 +455,14 @@ struct PdvOut {
 constexpr int PDV_TY = 8;
 template <typename T> constexpr size_t pdv_smem() { return 4 * Box1<T, PDV_TY>::BOXS * sizeof(T); }
 
-template <typename T>
+// FLUX: the corrector (mode 0) also does flux_calc (src/serial/flux_calc.cpp:27-43)
+// from the same staged velocities -- faces [2, nx+2] x [2, ny+2], so the grid
+// covers one more column and row than the cells -- with fold depth
+// flux_fold, as flux_calc_tile writes them.
+template <typename T, bool FLUX = false>
 __device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, const PdvIn &in, const PdvOut &out, const Mesh<T> &m, int off,
-                                         int predict, T dt, int mode, T gm1, int fold, int bx, int by) {
+                                         int predict, T dt, int mode, T gm1, int fold, int bx, int by, T *fx_out = nullptr,
+                                         T *fy_out = nullptr, int flux_fold = 0) {
   constexpr int TY = PDV_TY;
   using B = Box1<T, TY>;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
@@ -402,40 +484,61 @@ __device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, c
   const int nf = predict ? 2 : 4;
   if (!stage(cx, sm, ms, nf, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
   const T *U0 = sm, *V0 = sm + B::BOXS, *U1 = sm + 2 * B::BOXS, *V1 = sm + 3 * B::BOXS;
-  if (i >= m.nx + 2) return true;
-  const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+  if (i >= m.nx + (FLUX ? 3 : 2)) return true;
+  const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
+  const bool do_fold = fold && near;
   const T cdx = m.celldx_t[i];
 #pragma unroll
   for (int r = 0; r < RPT; ++r) {
     const int j = y0 + threadIdx.y + 4 * r;
-    if (j >= m.ny + 2) break;
+    if (j >= m.ny + (FLUX ? 3 : 2)) break;
     const int b = B::at(i, j, x0, y0);
-    const T cdy = m.celldy_t[j];
-    const T vol = cdx * cdy;
-    T w00 = T(0), w01 = T(0), w10 = T(0), w11 = T(0), z00 = T(0), z10 = T(0), z01 = T(0), z11 = T(0);
-    if (!predict) {
-      w00 = U1[b], w01 = U1[b + BOX_X], w10 = U1[b + 1], w11 = U1[b + BOX_X + 1];
-      z00 = V1[b], z10 = V1[b + 1], z01 = V1[b + BOX_X], z11 = V1[b + BOX_X + 1];
-    }
-    T d1, e1;
-    pdv_value(predict != 0, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
-              V0[b + BOX_X + 1], w00, w01, w10, w11, z00, z10, z01, z11, rd[r], re[r], rp[r], rq[r], d1, e1);
     const int g = gidx(pitch, i, j);
-    if (mode == 0) {
-      ((T *)out.density1)[g] = d1;
-      ((T *)out.energy1)[g] = e1;
-      if (do_fold) {
-        fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, d1);
-        fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, e1);
+    if (!FLUX || (i < m.nx + 2 && j < m.ny + 2)) {
+      const T cdy = m.celldy_t[j];
+      const T vol = cdx * cdy;
+      T w00 = T(0), w01 = T(0), w10 = T(0), w11 = T(0), z00 = T(0), z10 = T(0), z01 = T(0), z11 = T(0);
+      if (!predict) {
+        w00 = U1[b], w01 = U1[b + BOX_X], w10 = U1[b + 1], w11 = U1[b + BOX_X + 1];
+        z00 = V1[b], z10 = V1[b + 1], z01 = V1[b + BOX_X], z11 = V1[b + BOX_X + 1];
       }
-    } else {
-      T p, c;
-      eos_value(d1, e1, gm1, p, c);
-      ((T *)out.pressure)[g] = p;
-      ((T *)out.soundspeed)[g] = c;
-      if (do_fold) fold_halo((T *)out.pressure, m, halo_rule(PRESSURE), fold, i, j, p);
-      ((T *)out.density1)[g] = rd[r];
-      ((T *)out.energy1)[g] = re[r];
+      T d1, e1;
+      pdv_value(predict != 0, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
+                V0[b + BOX_X + 1], w00, w01, w10, w11, z00, z10, z01, z11, rd[r], re[r], rp[r], rq[r], d1, e1);
+      if (mode == 0) {
+        ((T *)out.density1)[g] = d1;
+        ((T *)out.energy1)[g] = e1;
+        if (do_fold) {
+          fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, d1);
+          fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, e1);
+        }
+      } else {
+        T p, c;
+        eos_value(d1, e1, gm1, p, c);
+        ((T *)out.pressure)[g] = p;
+        ((T *)out.soundspeed)[g] = c;
+        if (do_fold) fold_halo((T *)out.pressure, m, halo_rule(PRESSURE), fold, i, j, p);
+        ((T *)out.density1)[g] = rd[r];
+        ((T *)out.energy1)[g] = re[r];
+      }
+    }
+    if constexpr (FLUX) {
+      // flux_calc_tile's face values and writes
+      const T fx = flux_value(dt, m.celldy_t[j], U0[b], U0[b + BOX_X], U1[b], U1[b + BOX_X]);
+      const T fy = flux_value(dt, cdx, V0[b], V0[b + 1], V1[b], V1[b + 1]);
+      if (!flux_fold) {
+        fx_out[g] = fx;
+        fy_out[g] = fy;
+        continue;
+      }
+      if (j < m.ny + 2) {
+        fx_out[g] = fx;
+        if (near) fold_halo(fx_out, m, halo_rule(VOL_FLUX_X), flux_fold, i, j, fx);
+      }
+      if (i < m.nx + 2) {
+        fy_out[g] = fy;
+        if (near) fold_halo(fy_out, m, halo_rule(VOL_FLUX_Y), flux_fold, i, j, fy);
+      }
     }
   }
   return true;
@@ -449,6 +552,17 @@ __global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps,
   TileCtx cx = tile_ctx(&bar, err);
   pdv_tile(cx, reinterpret_cast<T *>(smraw), map_set(maps, predict ? 2 : 4), in, out, m, off, predict, dtp ? (T)*dtp : dt, mode, gm1, fold,
            blockIdx.x, blockIdx.y);
+}
+
+// The PdV corrector and flux_calc in one pass (the resident loop).
+template <typename T>
+__global__ void __launch_bounds__(256) kt_pdv_flux(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, T *fx_out, T *fy_out, Mesh<T> m,
+                                                   int off, T dt, const double *dtp, int fold, int flux_fold, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  TileCtx cx = tile_ctx(&bar, err);
+  pdv_tile<T, true>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 4), in, out, m, off, 0, dtp ? (T)*dtp : dt, 0, T(0), fold, blockIdx.x,
+                    blockIdx.y, fx_out, fy_out, flux_fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -542,12 +656,6 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 // With a fold, the extra row of x faces and column of y faces (overwritten
 // by update_halo) take their halo values.
 // fields: 0 xvel0, 1 yvel0, 2 xvel1, 3 yvel1
-// Volume flux through a face (src/serial/flux_calc.cpp:33-40): width is
-// xarea (celldy) for x faces, yarea (celldx) for y faces; a0, a1 the level-0
-// velocities of the face's two nodes, b0, b1 the level-1 ones.
-template <typename T> __device__ __forceinline__ T flux_value(T dt, T width, T a0, T a1, T b0, T b1) {
-  return T(0.25) * dt * width * (a0 + a1 + b0 + b1);
-}
 
 constexpr int FLUX_TY = 16;
 template <typename T, int TY> constexpr size_t flux_smem() { return 4 * Tile<TY>::BOX * sizeof(T); }
@@ -669,8 +777,13 @@ __device__ __forceinline__ void cell_update_value(S d1, S e1, S pre_vol, S mf_lo
   enew = post_ener_s;
 }
 
+// density0 / energy0 set: the sweep also does reset_field's cell copy
+// (src/serial/reset_field.cpp:33-40) of the values it writes, with its fold
+// depth rfold -- the resident loop's second sweep.
 struct CellOut {
   void *density1, *energy1, *mass_flux;
+  void *density0 = nullptr, *energy0 = nullptr;
+  int rfold = 0;
 };
 
 // Tile of the cell sweep: LA cells along the sweep x LL lines across.
@@ -811,6 +924,14 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
       fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, dnew);
       fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, enew);
     }
+    if (out.density0) {
+      ((T *)out.density0)[g] = dnew;
+      ((T *)out.energy0)[g] = enew;
+      if (EDGE && out.rfold) {
+        fold_halo((T *)out.density0, m, halo_rule(DENSITY0), out.rfold, i, j, dnew);
+        fold_halo((T *)out.energy0, m, halo_rule(ENERGY0), out.rfold, i, j, enew);
+      }
+    }
   }
 }
 
@@ -906,8 +1027,13 @@ template <typename T> __device__ __forceinline__ T mom_update_value(T vel, T nm_
   return div_zero_num(vel * nm_pre + mf_lo - mf_hi, nm_post);
 }
 
+// xvel0 / yvel0 set: the sweep also does reset_field's node copy
+// (src/serial/reset_field.cpp:42-49) of the velocities it writes, with its
+// fold depth rfold -- the resident loop's second sweep.
 struct MomOut {
   void *xvel1, *yvel1;
+  void *xvel0 = nullptr, *yvel0 = nullptr;
+  int rfold = 0;
 };
 
 template <typename T, int DIR, int TY> struct MomLayout {
@@ -1077,11 +1203,19 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
       T v = mom_update_value(U1[b], nmpre, nmpost, s_mfu[L::w(p - 1, l)], s_mfu[L::w(p, l)]);
       ((T *)out.xvel1)[g] = v;
       if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
+      if (out.xvel0) {
+        ((T *)out.xvel0)[g] = v;
+        if (EDGE && out.rfold) fold_halo((T *)out.xvel0, m, halo_rule(XVEL0), out.rfold, i, j, v);
+      }
     }
     if (vel_mask & 2) {
       T v = mom_update_value(V1[b], nmpre, nmpost, s_mfv[L::w(p - 1, l)], s_mfv[L::w(p, l)]);
       ((T *)out.yvel1)[g] = v;
       if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
+      if (out.yvel0) {
+        ((T *)out.yvel0)[g] = v;
+        if (EDGE && out.rfold) fold_halo((T *)out.yvel0, m, halo_rule(YVEL0), out.rfold, i, j, v);
+      }
     }
   }
 }

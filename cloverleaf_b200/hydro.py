@@ -143,17 +143,19 @@ class HydroRun:
         return done
 
     # driver/hydro.cpp:53-111, the whole loop on the device (cb_run)
-    def run_steps_on_device(self, max_steps: Optional[int] = None, chunk_steps: int = 4096) -> bool:
+    def run_steps_on_device(self, max_steps: Optional[int] = None, chunk_steps: int = 4096, fuse: bool = False) -> bool:
         """Makes the steps `hydro_step` would make, up to the end of the run or
         up to step `max_steps`, as device-resident CUDA graphs of at most
         `chunk_steps` steps each (the host waits once per graph).  Fields, dt
-        sequence and summaries are those of the `hydro_step` loop.  Returns
-        True when the run is complete."""
+        sequence and summaries are those of the `hydro_step` loop.  With
+        `fuse`, phases that share inputs run as one pass (FP64 results
+        unchanged to the bit, FP32 within its rounding).  Returns True when
+        the run is complete."""
         if self.forced_dt is not None or self.probe is not None:
             raise ValueError("run_steps_on_device: forced_dt and probe need the host-driven loop")
         d = self.deck
         p = RunParams(d.dtmin, d.dtmax, d.dtrise, d.dtc_safe, d.dtu_safe, d.dtv_safe, d.dtdiv_safe, d.end_time,
-                      d.end_step, d.summary_frequency, int(self.fold))
+                      d.end_step, d.summary_frequency, int(self.fold), int(fuse))
         st = RunState(self.step, int(self.advect_x), self.time, self.dtold, self.dt, 0)
         last = d.end_step if max_steps is None else min(d.end_step, max_steps)
         while self.step < last:

@@ -7,6 +7,12 @@ record and every state field (halos included) are bit-identical, in both
 precisions, with and without halo folding, on meshes too small to fold, when
 the run ends on its time or on its step count, when the loop is split into
 several graphs, and when the graph takes over a run the host started.
+
+With fuse = 1 the graph runs viscosity with calc_dt, the PdV corrector with
+flux_calc and reset_field inside the second sweeps: FP64 stays bit-identical;
+FP32 is compared within 1e-5 (relative to each field's largest magnitude),
+because the fused kernels may contract single-precision products and sums
+differently.
 """
 import numpy as np
 import pytest
@@ -45,13 +51,13 @@ def host_run(dk, precision, fold=True, steps=None):
     return c, r
 
 
-def device_run(dk, precision, fold=True, host_steps=0, chunk_steps=4096, steps=None):
+def device_run(dk, precision, fold=True, host_steps=0, chunk_steps=4096, steps=None, fuse=False):
     c = Chunk(dk.x_cells, dk.y_cells, precision=precision, gamma=dk.gamma)
     r = HydroRun(c, dk, fold=fold)
     r.start()
     for _ in range(host_steps):
         r.hydro_step()
-    done = r.run_steps_on_device(max_steps=steps, chunk_steps=chunk_steps)
+    done = r.run_steps_on_device(max_steps=steps, chunk_steps=chunk_steps, fuse=fuse)
     return c, r, done
 
 
@@ -122,7 +128,7 @@ def test_run_small_timestep_reports():
 
 def test_run_arguments_rejected():
     c = Chunk(16, 16)
-    p = RunParams(1e-7, 0.04, 1.5, 0.7, 0.5, 0.5, 0.7, 1.0, 10, 0, 1)
+    p = RunParams(1e-7, 0.04, 1.5, 0.7, 0.5, 0.5, 0.7, 1.0, 10, 0, 1, 0)
     st = RunState(0, 1, 0.0, 0.04, 0.04, 0)
     with pytest.raises(CloverError, match="max_steps"):
         c.run(p, st, 0)
@@ -150,3 +156,58 @@ def test_run_launch_count():
         counts.append(c.launch_count() - n0)
         assert r.step == 12 and len(r.summaries) == 4
     assert counts[1] == counts[0] + 1 + 3 * 12 + 3
+
+
+@pytest.mark.parametrize("deck", ["a", "b"])
+def test_run_fused_fp64_bit_identical(deck):
+    dk = deck_a() if deck == "a" else deck_b()
+    c1, r1 = host_run(dk, FP64)
+    c2, r2, done = device_run(dk, FP64, fuse=True)
+    assert done
+    assert_same(c1, r1, c2, r2)
+
+
+def test_run_fused_fp64_split_and_taken_over():
+    dk = deck_b()
+    c1, r1 = host_run(dk, FP64)
+    c2, r2, _ = device_run(dk, FP64, host_steps=3, chunk_steps=5, fuse=True)
+    assert_same(c1, r1, c2, r2)
+
+
+def test_run_fused_fp32_close():
+    dk = deck_a()  # ends on its step count
+    c1, r1 = host_run(dk, FP32)
+    c2, r2, done = device_run(dk, FP32, fuse=True)
+    assert done and r2.step == r1.step == 40
+    assert np.allclose(r2.dt_trace, r1.dt_trace, rtol=1e-5, atol=0)
+    for a, b in zip(r1.summaries, r2.summaries):
+        assert a.step == b.step
+        for q in ("vol", "mass", "ie", "ke", "press"):
+            assert abs(getattr(a, q) - getattr(b, q)) <= 1e-5 * abs(getattr(a, q)), (q, a, b)
+    for f in STATE_FIELDS:
+        x, y = c1.read(f), c2.read(f)
+        scale = max(np.abs(x).max(), 1e-30)
+        assert np.abs(x - y).max() <= 1e-5 * scale, f
+
+
+@pytest.mark.parametrize("nx,ny,fold", [(6, 5, True), (64, 48, False)])
+def test_run_fused_falls_back(nx, ny, fold):
+    """Without folding producers (small meshes, or fold off) fuse = 1 runs the unfused step."""
+    dk = deck_a(nx, ny, end_step=12, freq=4)
+    c1, r1 = host_run(dk, FP64, fold=fold)
+    c2, r2, _ = device_run(dk, FP64, fold=fold, fuse=True)
+    assert_same(c1, r1, c2, r2)
+
+
+def test_run_fused_launch_count():
+    """Fused, a step launches three kernels fewer (viscosity, flux_calc and reset_field run inside others)."""
+    dk = deck_a(48, 48, end_step=12, freq=5)
+    counts = []
+    for fuse in (False, True):
+        c = Chunk(48, 48)
+        r = HydroRun(c, dk)
+        r.start()
+        n0 = c.launch_count()
+        r.run_steps_on_device(fuse=fuse)
+        counts.append(c.launch_count() - n0)
+    assert counts[1] == counts[0] - 3 * 12
