@@ -7,9 +7,14 @@ background rho=0.2 e=1.0, rectangle [0,5]x[0,2] rho=1.0 e=2.5 on [0,10]^2,
 gamma 1.4, reflective) on a 7680x7680 mesh.  One "step" is one hydro
 timestep of the reference driver (timestep, PdV predictor, accelerate, PdV
 corrector, flux_calc, advection, reset_field, and field_summary every 10
-steps), enqueued through the C ABI in the driver's call order, with the
-driver's per-step dt read-back.  Every field array is 472 MB, far above the
-126 MB L2, so no flush is needed between steps.
+steps).  The headline runs the timed steps as one device-resident CUDA graph
+through the C ABI's cb_run with fuse = 1 (dt on the device, viscosity with
+calc_dt, the PdV corrector with flux_calc and reset_field inside the second
+sweeps: FP64 results identical to the bit to the phase-by-phase calls).  The
+same steps enqueued phase by phase in the driver's call order, with the
+driver's per-step dt read-back, are timed too (host_loop), with CUDA events
+at every phase boundary for the per-kernel roofline.  Every field array is
+472 MB, far above the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -205,6 +210,36 @@ def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False,
     return ms, run, c, phases, n1 - n0
 
 
+def resident_form(precision, cells, warmup, steps, rank=0, world=1, fuse=True):
+    """Sets up a chunk, runs `warmup` steps as one device-resident graph, then
+    times `steps` steps as another (cb_run; the graph's capture and
+    instantiation inside the timed region); returns (ms, run, chunk, launches
+    in the timed region)."""
+    import torch
+    from cloverleaf_b200 import Chunk, HydroRun
+    dk = bench_deck(cells)
+    c = Chunk(cells, cells, precision=precision, device=torch.cuda.current_device())
+    run = HydroRun(c, dk)
+    run.start()
+    run.run_steps_on_device(max_steps=run.step + warmup, fuse=fuse)
+    ext = torch.cuda.ExternalStream(c.stream())
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    n0 = c.launch_count()
+    t0.record(ext)
+    run.run_steps_on_device(max_steps=run.step + steps, fuse=fuse)
+    t1.record(ext)
+    c.synchronize()
+    torch.cuda.synchronize()
+    n1 = c.launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    return t0.elapsed_time(t1), run, c, n1 - n0
+
+
 def rel_errors(a64, a32):
     import numpy as np
     d = np.abs(a32 - a64)
@@ -216,8 +251,9 @@ def rel_errors(a64, a32):
 def e2e_run(cells, warmup, steps):
     """The same metric through the public C ABI with host buffers: the timed
     region uploads the step-0 state (density0, energy0, xvel0, yvel0) from
-    pinned host memory, advances `steps` steps (dt read back every step, the
-    summaries every 10) and reads the final state back to pinned host memory."""
+    pinned host memory, advances `steps` steps as the headline does (cb_run,
+    fused; its dt trace and summaries come back to the host) and reads the
+    final state back to pinned host memory."""
     import numpy as np
     import torch
     from cloverleaf_b200 import Chunk, HydroRun
@@ -229,8 +265,7 @@ def e2e_run(cells, warmup, steps):
     host = {n: torch.empty(tuple(reversed(c.extent(n))), dtype=torch.float64, pin_memory=True).numpy() for n in names}
     for n in names:
         host[n][...] = c.read(n)
-    for _ in range(warmup):
-        run.hydro_step()
+    run.run_steps_on_device(max_steps=warmup, fuse=True)
     run2 = HydroRun(c, dk)
     run2.summaries = []
     ext = torch.cuda.ExternalStream(c.stream())
@@ -240,8 +275,7 @@ def e2e_run(cells, warmup, steps):
     t0.record(ext)
     for n in names:
         c.write(n, host[n])
-    for _ in range(steps):
-        run2.hydro_step()
+    run2.run_steps_on_device(max_steps=steps, fuse=True)
     for n in names:
         c.read_into(n, host[n])
     t1.record(ext)
@@ -254,16 +288,17 @@ def e2e_run(cells, warmup, steps):
 
 
 def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
-    """The whole hydro loop as one device-resident CUDA graph (cb_run) against
-    the host-driven loop (dt read back every step), FP64, same deck, same
-    steps; ms per step from CUDA events on the chunk's stream around the
-    whole loop (the graph's capture and instantiation included)."""
+    """The whole hydro loop as one device-resident CUDA graph (cb_run, without
+    and with fused passes) against the host-driven loop (dt read back every
+    step), FP64, same deck, same steps; ms per step from CUDA events on the
+    chunk's stream around the whole loop (the graph's capture and
+    instantiation included)."""
     import torch
     from cloverleaf_b200 import Chunk, HydroRun
     out = []
     for cells, steps in sizes:
         row = {"cells": f"{cells}x{cells}", "steps": steps}
-        for mode in ("host_loop", "device_graph"):
+        for mode in ("host_loop", "device_graph", "device_graph_fused"):
             c = Chunk(cells, cells, device=torch.cuda.current_device())
             r = HydroRun(c, bench_deck(cells))
             r.start()
@@ -274,8 +309,8 @@ def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
             c.synchronize()
             torch.cuda.synchronize()
             t0.record(ext)
-            if mode == "device_graph":
-                r.run_steps_on_device(max_steps=r.step + steps)
+            if mode != "host_loop":
+                r.run_steps_on_device(max_steps=r.step + steps, fuse=mode == "device_graph_fused")
             else:
                 for _ in range(steps):
                     r.hydro_step()
@@ -285,6 +320,7 @@ def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
             row[mode] = {"ms_per_step": ms / steps, "value": cells * cells * steps / (ms / 1e3), "unit": UNIT}
             c.close()
         row["speedup"] = row["host_loop"]["ms_per_step"] / row["device_graph"]["ms_per_step"]
+        row["speedup_fused"] = row["host_loop"]["ms_per_step"] / row["device_graph_fused"]["ms_per_step"]
         out.append(row)
     return out
 
@@ -590,43 +626,62 @@ def main():
 
     S = args.size
     peak, peak_kind = peaks()
+    # headline: the steps as one device-resident graph (cb_run, fused passes)
     with ClockSampler(local) as clk:
-        ms64, run64, c64, phases, launches = run_form(FP64, S, args.warmup, args.steps, with_phases=True, rank=rank,
-                                                      world=world)
+        ms64, run64r, c64r, launches = resident_form(FP64, S, args.warmup, args.steps, rank=rank, world=world)
     clocks = clk.summary()
     if world > 1:
         ms64 = max_over_ranks(ms64, "cuda")
     value = replicas_value(S * S, args.steps, world, ms64)
+    ms32r, run32r, c32r, _ = resident_form(FP32, S, args.warmup, args.steps, rank=rank, world=world)
+    if world > 1:
+        ms32r = max_over_ranks(ms32r, "cuda")
+    value32 = replicas_value(S * S, args.steps, world, ms32r)
 
-    # FP32 form, replaying the FP64 run's dt sequence, errors against FP64 at the same time
+    def field_errors(ca, cb):
+        errs = {}
+        for name in ("density0", "energy0", "pressure", "xvel0", "yvel0"):
+            l1, mx = rel_errors(ca.read(name)[2:-2, 2:-2], cb.read(name)[2:-2, 2:-2])
+            errs[name] = {"l1_rel": l1, "max_rel": mx}
+        return errs
+
+    errs_resident = field_errors(c64r, c32r)
+    c64r.close()
+    c32r.close()
+
+    # the same steps phase by phase (host loop): per-phase CUDA events for the kernel roofline
+    ms64h, run64, c64, phases, _ = run_form(FP64, S, args.warmup, args.steps, with_phases=True, rank=rank, world=world)
+    if world > 1:
+        ms64h = max_over_ranks(ms64h, "cuda")
+    # FP32 form phase by phase, replaying the FP64 run's dt sequence: errors against FP64 at the same time
     dts = list(run64.dt_trace)
     ms32, run32, c32, ph32, _ = run_form(FP32, S, args.warmup, args.steps, forced_dt=dts, with_phases=True, world=world)
     if world > 1:
         ms32 = max_over_ranks(ms32, "cuda")
-    value32 = replicas_value(S * S, args.steps, world, ms32)
-    errs = {}
-    for name in ("density0", "energy0", "pressure", "xvel0", "yvel0"):
-        a64 = c64.read(name)[2:-2, 2:-2]
-        a32 = c32.read(name)[2:-2, 2:-2]
-        l1, mx = rel_errors(a64, a32)
-        errs[name] = {"l1_rel": l1, "max_rel": mx}
+    errs = field_errors(c64, c32)
 
     def drift(run):
         s0, s1 = run.summaries[0], run.summaries[-1]
         return {"mass": (s1.mass - s0.mass) / s0.mass,
                 "total_energy": ((s1.ie + s1.ke) - (s0.ie + s0.ke)) / (s0.ie + s0.ke)}
 
-    fp32 = {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
-            "errors_vs_fp64": errs, "drift_fp64": drift(run64), "drift_fp32": drift(run32),
-            "dt_sequence": "the FP64 run's, replayed",
+    fp32 = {"value": value32, "unit": UNIT, "ms_per_step": ms32r / args.steps, "speedup_vs_fp64": value32 / value,
+            "path": "cb_run fused, its own dt sequence",
+            "errors_vs_fp64": errs, "errors_dt_sequence": "FP32 phase by phase replaying the FP64 run's dt sequence",
+            "errors_vs_fp64_resident": errs_resident,
+            "errors_resident_dt_sequence": "each form's own dt, compared after the same number of steps",
+            "drift_fp64": drift(run64), "drift_fp32": drift(run32),
+            "host_loop": {"value": replicas_value(S * S, args.steps, world, ms32), "ms_per_step": ms32 / args.steps},
             "phase_ms_per_step": {k: ph32[0][k] / args.steps for k in sorted(ph32[0])}}
+    host_loop = {"value": replicas_value(S * S, args.steps, world, ms64h), "unit": UNIT, "ms_per_step": ms64h / args.steps,
+                 "path": "phase-by-phase C ABI calls in the driver's order, dt read back every step"}
     c64.close()
     c32.close()
 
     large = None
     if args.large:
         try:
-            msl, _, cl, _, _ = run_form(FP64, args.large, 3, 20, world=world)
+            msl, _, cl, _ = resident_form(FP64, args.large, 3, 20, world=world)
             cl.close()
             if world > 1:
                 msl = max_over_ranks(msl, "cuda")
@@ -649,7 +704,7 @@ def main():
     alg = PHASE_ARRAYS[dom] * 8 * S * S
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = traffic_per_launch(dom, S)
-    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roof = {"kernel": dom, "timed_in": "host_loop (the same kernel runs in the graph)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6.65 TB/s", "traffic": traffic, "alg_bytes_per_launch": alg,
             "step_frac": value / world * STEP_ARRAYS * 8 / 1e9 / peak,
@@ -699,8 +754,9 @@ def main():
                 "config": {"workload": f"clover_bm FP64 {S}x{S} hydro steps (InputDecks/clover_bm64_300.in physics)",
                            "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "path": "cb_run: the timed steps as one device-resident CUDA graph, fused passes",
                            "halo": "folded into producers"},
-                "roofline": roof, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "resident_loop": resident, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "host_loop": host_loop, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "resident_loop": resident, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "cpu_baseline": cpu}
         print(json.dumps(line, default=_plain))
     if world > 1:
