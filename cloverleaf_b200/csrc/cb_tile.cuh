@@ -78,8 +78,12 @@ __device__ __forceinline__ TileCtx tile_ctx(uint64_t *bar, int *err) { return Ti
 // memory (stride * sizeof(T) a multiple of 128 bytes).  Called by every
 // thread of the block; returns false in every thread if the copies did not
 // arrive within the wait limit.
+// stage() in two halves, for tiles that fill other shared memory while the
+// copies are in flight: stage_issue (every thread; the previous tile's
+// readers are done when it returns) and stage_wait (every thread; the boxes
+// and whatever the block wrote in between are visible when it returns).
 template <typename T>
-__device__ __forceinline__ bool stage(TileCtx &cx, T *sm, const MapSet &ms, int nf, int stride, int bh, int xs, int ys) {
+__device__ __forceinline__ void stage_issue(TileCtx &cx, T *sm, const MapSet &ms, int nf, int stride, int bh, int xs, int ys) {
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
   if (cx.fresh && leader) mbar_init(cx.bar, 1);
   __syncthreads(); // barrier initialised; the previous tile's readers are done with the boxes
@@ -90,11 +94,43 @@ __device__ __forceinline__ bool stage(TileCtx &cx, T *sm, const MapSet &ms, int 
     mbar_expect_tx(cx.bar, (unsigned)(nf * BOX_X * bh * sizeof(T)));
     for (int f = 0; f < nf; ++f) tma_load_2d(sm + f * stride, ms.m[f], xs, ys, cx.bar);
   }
+}
+
+__device__ __forceinline__ bool stage_wait(TileCtx &cx) {
   bool ok = mbar_wait(cx.bar, cx.phase, cx.err);
   if (!ok) mbar_wait(cx.bar, cx.phase, nullptr); // a second bounded wait for copies still in flight
   cx.phase ^= 1u;
   cx.fresh = false;
   return __syncthreads_and(ok) != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ bool stage(TileCtx &cx, T *sm, const MapSet &ms, int nf, int stride, int bh, int xs, int ys) {
+  stage_issue(cx, sm, ms, nf, stride, bh, xs, ys);
+  return stage_wait(cx);
+}
+
+// The 1-D widths a tile reads, copied to shared memory while its boxes are
+// in flight: gx[k] = celldx of column x0 - HALO + k (BOX_X of them), gy[r] =
+// celldy of row y0 - yh + r (bh of them), and -- when gv is given -- the
+// sweep direction's vertex widths and their reciprocals, indexed like gx
+// (x sweep) or gy (y sweep).  Indices past the arrays' ends are clamped:
+// those entries belong to positions no extent check lets through.
+template <typename T>
+__device__ __forceinline__ void fill_widths(const Mesh<T> &m, int x0, int y0, int yh, int bh, int dir, T *gx, T *gy, double *gv,
+                                            double *grv) {
+  const int tid = threadIdx.y * 64 + threadIdx.x;
+  if (tid < BOX_X) {
+    gx[tid] = m.celldx_t[min(max(x0 - HALO + tid, 0), m.nx + 3)];
+  } else if (tid < BOX_X + bh) {
+    const int r = tid - BOX_X;
+    gy[r] = m.celldy_t[min(max(y0 - yh + r, 0), m.ny + 3)];
+  } else if (gv && tid >= 128 && tid < 128 + (dir == 1 ? BOX_X : bh)) {
+    const int k = tid - 128;
+    const int idx = dir == 1 ? min(max(x0 - HALO + k, 0), m.nx + 4) : min(max(y0 - yh + k, 0), m.ny + 4);
+    gv[k] = dir == 1 ? m.vertexdx[idx] : m.vertexdy[idx];
+    grv[k] = dir == 1 ? m.rvertexdx[idx] : m.rvertexdy[idx];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -798,8 +834,11 @@ template <typename T, int DIR, int TY> struct CellLayout {
   static constexpr int BOX = BOX_X * BH;
   static constexpr int BOXS = (BOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
   static constexpr int NPV = LA + 2, NF = LA + 1;
-  static constexpr size_t SCRATCH_BYTES = (size_t)2 * NF * LL * sizeof(double) + (size_t)NPV * LL * sizeof(T);
-  static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + SCRATCH_BYTES;
+  static constexpr size_t SCRATCH_BYTES = ((size_t)2 * NF * LL * sizeof(double) + (size_t)NPV * LL * sizeof(T) + 15) / 16 * 16;
+  // then the widths (fill_widths): vertex widths and reciprocals along the sweep, celldx, celldy
+  static constexpr int LV = DIR == 1 ? BOX_X : BH;
+  static constexpr size_t GEO_BYTES = (size_t)2 * LV * sizeof(double) + (size_t)(BOX_X + BH) * sizeof(T);
+  static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + SCRATCH_BYTES + GEO_BYTES;
   __device__ static constexpr int pv(int p, int l) { return DIR == 1 ? l * NPV + p : p * LL + l; } // p = cell + 1
   __device__ static constexpr int fx(int p, int l) { return DIR == 1 ? l * NF + p : p * LL + l; }  // p = face
   __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
@@ -825,7 +864,11 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   double *s_mf = reinterpret_cast<double *>(scratch);
   double *s_ef = s_mf + L::NF * LL;
   T *s_pv = reinterpret_cast<T *>(s_ef + L::NF * LL);
+  const double *g_vd = reinterpret_cast<const double *>(reinterpret_cast<char *>(scratch) + L::SCRATCH_BYTES);
+  const double *g_rvd = g_vd + L::LV;
+  const T *g_x = reinterpret_cast<const T *>(g_rvd + L::LV), *g_y = g_x + BOX_X;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
+  const int vo = DIR == 1 ? HALO - x0 : YH - y0; // index of the sweep's vertex width of position a: a + vo
   const T *D1 = sm, *E1 = sm + L::BOXS, *VFX = sm + 2 * L::BOXS, *VFY = sm + 3 * L::BOXS;
   const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
@@ -841,7 +884,7 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
     if (EDGE && (i > m.nx + 3 || j > m.ny + 3)) continue;
     const int b = bidx(i, j);
-    const T vol = m.celldx_t[i] * m.celldy_t[j];
+    const T vol = g_x[i - x0 + HALO] * g_y[j - y0 + YH];
     T pv;
     if (DIR == 1) {
       pv = sweep == 1 ? cell_pre_vol1(vol, VFX[b], VFX[b + 1], VFY[b], VFY[b + BOX_X]) : cell_pre_vol2(vol, VFX[b], VFX[b + 1]);
@@ -852,8 +895,6 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   }
   __syncthreads();
   // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
-  const double *vdx = DIR == 1 ? m.vertexdx : m.vertexdy;
-  const double *rvdx = DIR == 1 ? m.rvertexdx : m.rvertexdy;
   const bool edge = EDGE && fold;
   for (int t = tid; t < L::NF * LL; t += 256) {
     int p, l;
@@ -875,9 +916,9 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
     T mass_flux, e_adv;
     T ratio;
     if constexpr (sizeof(T) == sizeof(double)) {
-      ratio = width_ratio(vdx[f], vdx[dif], rvdx[dif]); // = vdx[f] / vdx[dif]
+      ratio = width_ratio(g_vd[f + vo], g_vd[dif + vo], g_rvd[dif + vo]); // = vertexdx[f] / vertexdx[dif]
     } else {
-      ratio = lim_div((T)vdx[f], (T)vdx[dif]);
+      ratio = lim_div((T)g_vd[f + vo], (T)g_vd[dif + vo]);
     }
     cell_face_value(flux, pre_vol_d, ratio, D1[bd], D1[bu], D1[bw], E1[bd], E1[bu], E1[bw], mass_flux, e_adv);
     s_mf[L::fx(p, l)] = (double)mass_flux;
@@ -944,7 +985,14 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
                                                 int sweep, int fold, int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  if (!stage(cx, sm, ms, cell_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH)) return false;
+  stage_issue(cx, sm, ms, cell_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH);
+  {
+    char *geo = reinterpret_cast<char *>(sm + 4 * L::BOXS) + L::SCRATCH_BYTES;
+    double *gv = reinterpret_cast<double *>(geo), *grv = gv + L::LV;
+    T *gx = reinterpret_cast<T *>(grv + L::LV);
+    fill_widths(m, x0, y0, L::YH, L::BH, DIR, gx, gx + BOX_X, gv, grv);
+  }
+  if (!stage_wait(cx)) return false;
   if (edge_tile(m.nx, m.ny, x0, y0, TY))
     advec_cell_compute<T, DIR, TY, true>(sm, sm + 4 * L::BOXS, out, m, sweep, fold, bx, by);
   else
@@ -1048,7 +1096,8 @@ template <typename T, int DIR, int TY> struct MomLayout {
   static constexpr int N_W = NP * LL;                // node arrays
   static constexpr int SCRATCH = N_CM + 4 * N_W;    // cell masses, node flux, node_mass_pre, two momentum fluxes
   static constexpr int REGION = SCRATCH > 3 * BOXS ? SCRATCH : 3 * BOXS;
-  static constexpr size_t SMEM = (size_t)(2 * BOXS + REGION) * sizeof(T);
+  static constexpr int GEO = 2 * BOXS + REGION; // the widths (fill_widths): celldx, then celldy
+  static constexpr size_t SMEM = (size_t)(GEO + BOX_X + BH) * sizeof(T);
   // work-array indices: the thread-fastest coordinate is the contiguous one
   __device__ static constexpr int cm(int p, int lc) { return DIR == 1 ? lc * NP + p : p * (LL + 1) + lc; }
   __device__ static constexpr int w(int p, int l) { return DIR == 1 ? l * NP + p : p * LL + l; }
@@ -1099,7 +1148,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
       if (!EDGE || (a >= 0 && a <= na + 3 && line >= 0 && line <= nlmax + 3)) {
         const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
         const int b = bidx(i, j);
-        const T vol = m.celldx_t[i] * m.celldy_t[j];
+        const T vol = sm[L::GEO + i - x0 + HALO] * sm[L::GEO + BOX_X + j - y0 + YH];
         // post_vol (:42-77): mom_sweep 1 vol + vfy difference, 2 vol + vfx difference, 3/4 vol
         const T pv = mom_sweep == 1 ? mom_post_vol(1, vol, VFO[b], VFO[b + BOX_X]) : mom_sweep == 2 ? mom_post_vol(2, vol, VFO[b], VFO[b + 1]) : vol;
         v = D1[b] * pv;
@@ -1163,7 +1212,8 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
   __syncthreads();
 
   // (3) mom_flux (:108-133 / :180-205) over positions 1 .. LA+1
-  const T *celld = DIR == 1 ? m.celldx_t : m.celldy_t;
+  // the sweep direction's cell widths: position a at celld[a]
+  const T *celld = DIR == 1 ? sm + L::GEO + HALO - x0 : sm + L::GEO + BOX_X + YH - y0;
   for (int t = tid; t < (LA + 1) * LL; t += 256) {
     int p, l;
     L::item(t, LA + 1, LL, p, l);
@@ -1229,7 +1279,9 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
                                                int vel_mask, int sweep, int fold, int bx, int by) {
   using L = MomLayout<T, DIR, TY>;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  if (!stage(cx, sm, ms, mom_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH)) return false;
+  stage_issue(cx, sm, ms, mom_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH);
+  fill_widths<T>(m, x0, y0, L::YH, L::BH, DIR, sm + L::GEO, sm + L::GEO + BOX_X, nullptr, nullptr);
+  if (!stage_wait(cx)) return false;
   if (edge_tile(m.nx, m.ny, x0, y0, TY))
     advec_mom_compute<T, DIR, TY, true>(sm, out, m, vel_mask, sweep, fold, bx, by);
   else
