@@ -348,7 +348,8 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
       const DtIn in{d.field(SOUNDSPEED), d.field(VISCOSITY), d.field(DENSITY0)};
       const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + DT_TY - 1) / DT_TY);
       double vmin = g_big;
-      for (int t = rank; t < nt; t += w) CB_PHASE(calc_dt_tile(cx, sm, ms, in, m, off, D->k, t % tx, t / tx, vmin));
+      RestMemo<T> memo;
+      for (int t = rank; t < nt; t += w) CB_PHASE(calc_dt_tile(cx, sm, ms, in, m, off, D->k, t % tx, t / tx, vmin, memo));
       block_min_to(vmin, slot);
     }
     CB_SYNC();

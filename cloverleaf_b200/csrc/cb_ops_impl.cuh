@@ -124,13 +124,15 @@ template <typename T> cudaError_t Ops<T>::pdv(Chunk &c, int predict, double dt, 
   constexpr int TY = 8;
   using B = Box1<T, TY>;
   const size_t smem = (predict ? 2 : 4) * B::BOXS * sizeof(T);
-  cudaError_t e = allow_smem(kt_pdv<T>, 4 * B::BOXS * sizeof(T));
+  // FP64: the four-blocks-per-SM form; FP32: the compiler's register choice
+  auto kern = sizeof(T) == sizeof(double) ? kt_pdv4<T> : kt_pdv<T>;
+  cudaError_t e = allow_smem(kern, 4 * B::BOXS * sizeof(T));
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + TILE_X - 1) / TILE_X, (c.ny + TY - 1) / TY);
   PdvIn in{c.base(DENSITY0), c.base(ENERGY0), c.base(PRESSURE), c.base(VISCOSITY)};
   PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
   Maps mp = maps_of<B::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1});
-  kt_pdv<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, mesh<T>(c), (int)c.off, predict, (T)dt, c.dt_dev, mode, gm1<T>(c), fold, c.d_err);
+  kern<<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, mesh<T>(c), (int)c.off, predict, (T)dt, c.dt_dev, mode, gm1<T>(c), fold, c.d_err);
   return launched(c);
 }
 

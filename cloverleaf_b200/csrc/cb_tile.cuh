@@ -279,6 +279,28 @@ __device__ __forceinline__ double dt_estimate(double ss, double q, double d0, do
 // factor cannot hold the minimum (the estimate's error is below 1e-6).
 constexpr double DT_SKIP = 1.0 + 1e-4;
 
+// The dt of a cell at rest (viscosity and the eight corner velocities zero,
+// of either sign) is a function of its sound speed, density and two widths
+// alone.  A thread that meets a cell at rest with the same four values as
+// the last one it evaluated skips it: that value is already in the thread's
+// minimum, or the filter showed it cannot lower it.
+template <typename T> struct RestMemo {
+  T ss, d0, dx, dy;
+  bool valid = false;
+  __device__ __forceinline__ bool seen(bool rest, T s, T d, T x, T y) {
+    if (!rest) return false;
+    if (valid && s == ss && d == d0 && x == dx && y == dy) return true;
+    ss = s, d0 = d, dx = x, dy = y, valid = true;
+    return false;
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ bool at_rest(T q, T u00, T u10, T u01, T u11, T v00, T v10, T v01, T v11) {
+  return q == T(0) && u00 == T(0) && u10 == T(0) && u01 == T(0) && u11 == T(0) && v00 == T(0) && v10 == T(0) && v01 == T(0) &&
+         v11 == T(0);
+}
+
 struct DtIn {
   const void *soundspeed, *viscosity, *density0;
 };
@@ -290,7 +312,7 @@ template <typename T> constexpr size_t dt_smem() { return 2 * Box1<T, DT_TY>::BO
 
 template <typename T>
 __device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, const Mesh<T> &m, int off,
-                                             const DtConsts &k, int bx, int by, double &vmin) {
+                                             const DtConsts &k, int bx, int by, double &vmin, RestMemo<T> &memo) {
   constexpr int TY = DT_TY;
   using B = Box1<T, TY>;
   const T *U = sm, *V = sm + B::BOXS;
@@ -320,6 +342,11 @@ __device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
       const int j = y0 + threadIdx.y + 4 * r;
       if (j >= m.ny + 2) break;
       const int b = B::at(i, j, x0, y0);
+      // (FP32 only here: the FP64 kernel's registers are spent on the estimate filter)
+      if (sizeof(T) == sizeof(float) &&
+          memo.seen(at_rest(qq[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1]), ss[r],
+                    dd[r], dsx, m.celldy_t[j]))
+        continue;
       if constexpr (sizeof(T) == sizeof(double)) {
         const double est = dt_estimate(ss[r], qq[r], dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
                                        V[b + BOX_X + 1], dsx, m.celldy_t[j], k);
@@ -344,8 +371,9 @@ __global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Map
   TileCtx cx = tile_ctx(&bar, err);
   const MapSet ms = map_set(maps, 2);
   double vmin = g_big;
+  RestMemo<T> memo;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!calc_dt_tile(cx, sm, ms, in, m, off, k, t % tiles_x, t / tiles_x, vmin)) return;
+    if (!calc_dt_tile(cx, sm, ms, in, m, off, k, t % tiles_x, t / tiles_x, vmin, memo)) return;
   block_min_to(vmin, dt_bits);
 }
 
@@ -359,7 +387,7 @@ static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height"
 
 template <typename T>
 __device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, T *q_out, const Mesh<T> &m, int off,
-                                             const DtConsts &k, int fold, int bx, int by, double &vmin) {
+                                             const DtConsts &k, int fold, int bx, int by, double &vmin, RestMemo<T> &memo) {
   constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
   const T *S = (const T *)in.soundspeed, *R = (const T *)in.density0;
@@ -392,6 +420,9 @@ __device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
                                   P[b + 1], P[b - BOX_X], P[b + BOX_X], dd[r], cdx, cdx1, cdy, m.celldy_t[j + 2]);
       q_out[gidx(pitch, i, j)] = q;
       if (do_fold) fold_halo(q_out, m, halo_rule(VISCOSITY), fold, i, j, q);
+      if (memo.seen(at_rest(q, U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1]), ss[r], dd[r],
+                    cdx, cdy))
+        continue;
       if constexpr (sizeof(T) == sizeof(double)) {
         const double est = dt_estimate(ss[r], q, dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
                                        V[b + BOX_X + 1], cdx, cdy, k);
@@ -414,8 +445,9 @@ __global__ void __launch_bounds__(256, 4) kt_visc_dt(const __grid_constant__ Map
   TileCtx cx = tile_ctx(&bar, err);
   const MapSet ms = map_set(maps, 3);
   double vmin = g_big;
+  RestMemo<T> memo;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!visc_dt_tile(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin)) return;
+    if (!visc_dt_tile(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin, memo)) return;
   block_min_to(vmin, dt_bits);
 }
 
@@ -581,13 +613,27 @@ __device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict, T dt,
-                                              const double *dtp, int mode, T gm1, int fold, int *err) {
+__device__ __forceinline__ void pdv_kernel(const Maps &maps, const PdvIn &in, const PdvOut &out, const Mesh<T> &m, int off, int predict, T dt,
+                                           const double *dtp, int mode, T gm1, int fold, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   TileCtx cx = tile_ctx(&bar, err);
   pdv_tile(cx, reinterpret_cast<T *>(smraw), map_set(maps, predict ? 2 : 4), in, out, m, off, predict, dtp ? (T)*dtp : dt, mode, gm1, fold,
            blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kt_pdv(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict, T dt,
+                                              const double *dtp, int mode, T gm1, int fold, int *err) {
+  pdv_kernel<T>(maps, in, out, m, off, predict, dt, dtp, mode, gm1, fold, err);
+}
+
+// The FP64 launch: four blocks per SM (the registers of the quiescent-cell
+// test would otherwise leave three).
+template <typename T>
+__global__ void __launch_bounds__(256, 4) kt_pdv4(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict,
+                                                  T dt, const double *dtp, int mode, T gm1, int fold, int *err) {
+  pdv_kernel<T>(maps, in, out, m, off, predict, dt, dtp, mode, gm1, fold, err);
 }
 
 // The PdV corrector and flux_calc in one pass (the resident loop).
