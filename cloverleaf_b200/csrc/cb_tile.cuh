@@ -880,7 +880,11 @@ template <typename T, int DIR, int TY> struct CellLayout {
   static constexpr int BOX = BOX_X * BH;
   static constexpr int BOXS = (BOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
   static constexpr int NPV = LA + 2, NF = LA + 1;
-  static constexpr size_t SCRATCH_BYTES = ((size_t)2 * NF * LL * sizeof(double) + (size_t)NPV * LL * sizeof(T) + 15) / 16 * 16;
+  // face scratch: FP64 keeps each face's mass flux and energy flux; FP32
+  // keeps the mass flux and e_adv as they were computed (single precision)
+  // and forms the FP64 energy flux, an exact product, where it is used
+  using FS = std::conditional_t<sizeof(T) == sizeof(double), double, float>;
+  static constexpr size_t SCRATCH_BYTES = ((size_t)2 * NF * LL * sizeof(FS) + (size_t)NPV * LL * sizeof(T) + 15) / 16 * 16;
   // then the widths (fill_widths): vertex widths and reciprocals along the sweep, celldx, celldy
   static constexpr int LV = DIR == 1 ? BOX_X : BH;
   static constexpr size_t GEO_BYTES = (size_t)2 * LV * sizeof(double) + (size_t)(BOX_X + BH) * sizeof(T);
@@ -907,8 +911,9 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
                                                    int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
   constexpr int LA = L::LA, LL = L::LL, YH = L::YH;
-  double *s_mf = reinterpret_cast<double *>(scratch);
-  double *s_ef = s_mf + L::NF * LL;
+  using FS = typename L::FS;
+  FS *s_mf = reinterpret_cast<FS *>(scratch);
+  FS *s_ef = s_mf + L::NF * LL; // FP64: mass_flux * e_adv; FP32: e_adv
   T *s_pv = reinterpret_cast<T *>(s_ef + L::NF * LL);
   const double *g_vd = reinterpret_cast<const double *>(reinterpret_cast<char *>(scratch) + L::SCRATCH_BYTES);
   const double *g_rvd = g_vd + L::LV;
@@ -967,8 +972,11 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
       ratio = lim_div((T)g_vd[f + vo], (T)g_vd[dif + vo]);
     }
     cell_face_value(flux, pre_vol_d, ratio, D1[bd], D1[bu], D1[bw], E1[bd], E1[bu], E1[bw], mass_flux, e_adv);
-    s_mf[L::fx(p, l)] = (double)mass_flux;
-    s_ef[L::fx(p, l)] = (double)mass_flux * (double)(e_adv);
+    s_mf[L::fx(p, l)] = mass_flux;
+    if constexpr (sizeof(T) == sizeof(double))
+      s_ef[L::fx(p, l)] = mass_flux * e_adv;
+    else
+      s_ef[L::fx(p, l)] = e_adv;
     T *mf = (T *)out.mass_flux;
     const bool halo_face = EDGE && fold && f == na + 3; // with a fold, face na+3 takes its halo value
     if (!halo_face) mf[gidx(pitch, i, j)] = mass_flux;
@@ -985,7 +993,12 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
     const int b = bidx(i, j);
     const T pre_vol = s_pv[L::pv(p + 1, l)];
     const double mf_lo = s_mf[L::fx(p, l)], mf_hi = s_mf[L::fx(p + 1, l)];
-    const double ef_lo = s_ef[L::fx(p, l)], ef_hi = s_ef[L::fx(p + 1, l)];
+    double ef_lo, ef_hi;
+    if constexpr (sizeof(T) == sizeof(double)) {
+      ef_lo = s_ef[L::fx(p, l)], ef_hi = s_ef[L::fx(p + 1, l)];
+    } else {
+      ef_lo = mf_lo * (double)s_ef[L::fx(p, l)], ef_hi = mf_hi * (double)s_ef[L::fx(p + 1, l)];
+    }
     const T vf_lo = DIR == 1 ? VFX[b] : VFY[b];
     const T vf_hi = DIR == 1 ? VFX[b + 1] : VFY[b + BOX_X];
     T dnew, enew;
