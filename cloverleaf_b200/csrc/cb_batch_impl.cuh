@@ -379,7 +379,7 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
     CB_SYNC();
     {
       const int fl[5] = {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0};
-      if (tid == 0) d.template set_maps<Tile<BT::ACC>::BH>(5, fl);
+      if (tid == 0) d.template set_maps<Box1<T, BT::ACC>::BH>(5, fl);
       const MapSet &ms = d.ms;
       const int tx = (m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + 1 + BT::ACC - 1) / BT::ACC);
       for (int t = rank; t < nt; t += w)
@@ -398,7 +398,7 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
     CB_SYNC();
     {
       const int fl[4] = {XVEL0, YVEL0, XVEL1, YVEL1};
-      if (tid == 0) d.template set_maps<Tile<BT::FLUX>::BH>(4, fl);
+      if (tid == 0) d.template set_maps<Box1<T, BT::FLUX>::BH>(4, fl);
       const MapSet &ms = d.ms;
       const int tx = (m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + 1 + BT::FLUX - 1) / BT::FLUX);
       for (int t = rank; t < nt; t += w)

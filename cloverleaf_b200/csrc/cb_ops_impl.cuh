@@ -144,11 +144,11 @@ template <typename T> cudaError_t Ops<T>::revert(Chunk &c) {
 
 template <typename T> cudaError_t Ops<T>::accelerate(Chunk &c, double dt, int fold) {
   constexpr int TY = 16;
-  const size_t smem = 5 * Tile<TY>::BOX * sizeof(T);
+  const size_t smem = acc_smem<T, TY>();
   cudaError_t e = allow_smem(kt_accelerate<T>, smem);
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  kt_accelerate<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0}),
+  kt_accelerate<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Box1<T, TY>::BH>(c, {DENSITY0, PRESSURE, VISCOSITY, XVEL0, YVEL0}),
                                                        (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, (T)dt, c.dt_dev,
                                                        fold, c.d_err);
   return launched(c);
@@ -156,11 +156,11 @@ template <typename T> cudaError_t Ops<T>::accelerate(Chunk &c, double dt, int fo
 
 template <typename T> cudaError_t Ops<T>::flux_calc(Chunk &c, double dt, int fold) {
   constexpr int TY = 16;
-  const size_t smem = 4 * Tile<TY>::BOX * sizeof(T);
+  const size_t smem = flux_smem<T, TY>();
   cudaError_t e = allow_smem(kt_flux_calc<T>, smem);
   if (e != cudaSuccess) return e;
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  kt_flux_calc<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Tile<TY>::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1}), (T *)c.base(VOL_FLUX_X),
+  kt_flux_calc<T><<<g, dim3(64, 4), smem, c.stream>>>(maps_of<Box1<T, TY>::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1}), (T *)c.base(VOL_FLUX_X),
                                                       (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, fold, c.d_err);
   return launched(c);
 }

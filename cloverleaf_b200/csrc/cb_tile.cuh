@@ -686,15 +686,17 @@ __device__ __forceinline__ void accel_value(T halfdt, T vol_mm, T vol_m0, T vol_
 
 // One tile of TY node rows; the one-launch kernel uses TY = ACC_TY.
 constexpr int ACC_TY = 16;
-template <typename T, int TY> constexpr size_t acc_smem() { return 5 * Tile<TY>::BOX * sizeof(T); }
+// Staged boxes start one row above the tile (the nodes' lower cells): Box1.
+template <typename T, int TY> constexpr size_t acc_smem() { return 5 * Box1<T, TY>::BOXS * sizeof(T); }
 
 template <typename T, int TY>
 __device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet &ms, T *u_out, T *v_out, const Mesh<T> &m, int off, T dt,
                                                 int fold, int bx, int by) {
-  using C = Tile<TY>;
+  using B = Box1<T, TY>;
+  constexpr int RPT = TY / 4;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  if (!stage(cx, sm, ms, 5, C::BOX, C::BH, off + x0 - HALO, y0 - HALO)) return false;
-  const T *D0 = sm, *P = sm + C::BOX, *Q = sm + 2 * C::BOX, *U0 = sm + 3 * C::BOX, *V0 = sm + 4 * C::BOX;
+  if (!stage(cx, sm, ms, 5, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  const T *D0 = sm, *P = sm + B::BOXS, *Q = sm + 2 * B::BOXS, *U0 = sm + 3 * B::BOXS, *V0 = sm + 4 * B::BOXS;
   const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
   if (i >= m.nx + 3) return true;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
@@ -702,8 +704,8 @@ __device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet
   const T halfdt = T(0.5) * dt;
   const T cdx = m.celldx_t[i], cdxm = m.celldx_t[i - 1];
 #pragma unroll
-  for (int r = 0; r < C::RPT; ++r) {
-    const int j = y0 + threadIdx.y + 4 * r, ly = HALO + threadIdx.y + 4 * r;
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r, ly = 1 + threadIdx.y + 4 * r;
     if (j >= m.ny + 3) break;
     const int b = ly * BOX_X + lx;
     const T cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
@@ -740,23 +742,25 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 // fields: 0 xvel0, 1 yvel0, 2 xvel1, 3 yvel1
 
 constexpr int FLUX_TY = 16;
-template <typename T, int TY> constexpr size_t flux_smem() { return 4 * Tile<TY>::BOX * sizeof(T); }
+// Staged boxes start one row above the tile: Box1 (the faces need rows j and j + 1).
+template <typename T, int TY> constexpr size_t flux_smem() { return 4 * Box1<T, TY>::BOXS * sizeof(T); }
 
 template <typename T, int TY>
 __device__ __forceinline__ bool flux_calc_tile(TileCtx &cx, T *sm, const MapSet &ms, T *fx_out, T *fy_out, const Mesh<T> &m, int off, T dt,
                                                int fold, int bx, int by) {
-  using C = Tile<TY>;
+  using B = Box1<T, TY>;
+  constexpr int RPT = TY / 4;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  if (!stage(cx, sm, ms, 4, C::BOX, C::BH, off + x0 - HALO, y0 - HALO)) return false;
-  const T *U0 = sm, *V0 = sm + C::BOX, *U1 = sm + 2 * C::BOX, *V1 = sm + 3 * C::BOX;
+  if (!stage(cx, sm, ms, 4, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  const T *U0 = sm, *V0 = sm + B::BOXS, *U1 = sm + 2 * B::BOXS, *V1 = sm + 3 * B::BOXS;
   const int i = x0 + threadIdx.x, lx = HALO + threadIdx.x;
   if (i >= m.nx + 3) return true;
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const int pitch = (int)m.pitch;
   const T cdx = m.celldx_t[i];
 #pragma unroll
-  for (int r = 0; r < C::RPT; ++r) {
-    const int j = y0 + threadIdx.y + 4 * r, ly = HALO + threadIdx.y + 4 * r;
+  for (int r = 0; r < RPT; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r, ly = 1 + threadIdx.y + 4 * r;
     if (j >= m.ny + 3) break;
     const int b = ly * BOX_X + lx;
     T fx = flux_value(dt, m.celldy_t[j], U0[b], U0[b + BOX_X], U1[b], U1[b + BOX_X]);
