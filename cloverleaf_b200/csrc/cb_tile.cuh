@@ -1080,14 +1080,15 @@ __global__ void __launch_bounds__(256, 5) kt_advec_cell(const __grid_constant__ 
 // A block updates the nodes of a tile: LA nodes along the sweep (a) times LL
 // lines across it.  Positions p = 0 .. LA+2 along the sweep map to nodes
 // a = a0 - 2 + p; the stages cover only the positions the tile's outputs
-// need (node flux and cell mass p = 0..LA+2, node masses 1..LA+2, momentum
-// fluxes 1..LA+1, updates 2..LA+1), and every stage spreads its
-// (position, line) items evenly over the block's 256 threads.
+// need (node flux and cell mass p = 0..LA+2, momentum fluxes 1..LA+1,
+// updates 2..LA+1), and every stage spreads its (position, line) items
+// evenly over the block's 256 threads.
 //
 // Cell masses density1 * post_vol are formed once per cell (the reference
 // forms each four times inside node_mass_post, :93-102 / :165-174, with the
 // same products and the same order of the sum, so the bits agree);
-// node_mass_post is re-formed from them where the update needs it.
+// node_mass_post and node_mass_pre are re-formed from them and the node
+// fluxes where a momentum flux or an update reads them.
 //
 // Staged boxes (BOX_X x BH, tensor rows from y0 - YH): xvel1, yvel1, then
 // density1, the sweep's mass flux and (sweep 1) the other direction's volume
@@ -1157,7 +1158,7 @@ template <typename T, int DIR, int TY> struct MomLayout {
   static constexpr int NP = LA + 3;                  // positions 0 .. LA+2
   static constexpr int N_CM = NP * (LL + 1);         // cell masses: lines -1 .. LL-1
   static constexpr int N_W = NP * LL;                // node arrays
-  static constexpr int SCRATCH = N_CM + 4 * N_W;    // cell masses, node flux, node_mass_pre, two momentum fluxes
+  static constexpr int SCRATCH = N_CM + 3 * N_W;    // cell masses, node flux, two momentum fluxes
   static constexpr int REGION = SCRATCH > 3 * BOXS ? SCRATCH : 3 * BOXS;
   static constexpr int GEO = 2 * BOXS + REGION; // the widths (fill_widths): celldx, then celldy
   static constexpr size_t SMEM = (size_t)(GEO + BOX_X + BH) * sizeof(T);
@@ -1187,7 +1188,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const T *U1 = sm, *V1 = sm + L::BOXS, *D1 = sm + 2 * L::BOXS, *MF = sm + 3 * L::BOXS, *VFO = sm + 4 * L::BOXS;
   T *region = sm + 2 * L::BOXS;
-  T *s_cm = region, *s_nf = s_cm + L::N_CM, *s_nmpre = s_nf + L::N_W, *s_mfu = s_nmpre + L::N_W, *s_mfv = s_mfu + L::N_W;
+  T *s_cm = region, *s_nf = s_cm + L::N_CM, *s_mfu = s_nf + L::N_W, *s_mfv = s_mfu + L::N_W;
   const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
   const int a0 = DIR == 1 ? x0 : y0, l0 = DIR == 1 ? y0 : x0;
@@ -1262,17 +1263,10 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
     return quarter_sum(s_cm[L::cm(p - 1, l + 1)], s_cm[L::cm(p, l + 1)], s_cm[L::cm(p - 1, l)], s_cm[L::cm(p, l)]);
   };
 
-  // (2) node_mass_pre (:97-102 / :169-174) over positions 1 .. LA+2
-  for (int t = tid; t < (NP - 1) * LL; t += 256) {
-    int p, l;
-    L::item(t, NP - 1, LL, p, l);
-    p += 1;
-    const int a = a0 - 2 + p, line = l0 + l;
-    T nmpre = T(1.0);
-    if (!EDGE || (line < nlmax + 3 && a >= 1 && a <= na + 3)) nmpre = mom_node_mass_pre(node_mass_post(p, l), s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]);
-    s_nmpre[L::w(p, l)] = nmpre;
-  }
-  __syncthreads();
+  // node_mass_pre (:97-102 / :169-174) of node (p, l), formed where it is
+  // read (the donor of a momentum flux, the node of an update) rather than
+  // stored: one barrier and one work array fewer
+  auto node_mass_pre = [&](int p, int l) -> T { return mom_node_mass_pre(node_mass_post(p, l), s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]); };
 
   // (3) mom_flux (:108-133 / :180-205) over positions 1 .. LA+1
   // the sweep direction's cell widths: position a at celld[a]
@@ -1290,7 +1284,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
     } else {
       upwind = a - 1; donor = a; downwind = a + 1; dif = upwind;
     }
-    const T sigma = mom_sigma(nfv, s_nmpre[L::w(p + (donor - a), l)]);
+    const T sigma = mom_sigma(nfv, node_mass_pre(p + (donor - a), l));
     const T width = celld[a];
     const T dxd = celld[dif];
     const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
@@ -1310,7 +1304,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
     if (EDGE && (line > nlmax + 2 || a > na + 2)) continue;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
     const int b = bidx(i, j);
-    const T nmpre = s_nmpre[L::w(p, l)], nmpost = node_mass_post(p, l);
+    const T nmpost = node_mass_post(p, l), nmpre = mom_node_mass_pre(nmpost, s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]);
     const int g = gidx(pitch, i, j);
     if (vel_mask & 1) {
       T v = mom_update_value(U1[b], nmpre, nmpost, s_mfu[L::w(p - 1, l)], s_mfu[L::w(p, l)]);
