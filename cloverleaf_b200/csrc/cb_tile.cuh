@@ -806,10 +806,10 @@ template <> struct AdvecTiles<float> {
 };
 
 // ---------------------------------------------------------------------------
-// advec_cell: src/serial/advec_cell.cpp:28-220, one sweep in one pass.
-// pre_vol of the cells the faces need, then the face fluxes, then the
-// update, all through shared memory; each stage spreads its items evenly
-// over the block's 256 threads.
+// advec_cell: src/serial/advec_cell.cpp:28-220, one sweep in one pass: the
+// face fluxes into shared memory, then the update; each stage spreads its
+// items evenly over the block's 256 threads, and pre_vol is formed from the
+// staged volume fluxes where a face or an update reads it.
 template <typename T>
 __device__ __forceinline__ T cell_limiter_value(T sigma, T sigma3, T sigma4, T diffuw, T diffdw) {
   const T one_by_six = T(1.0 / 6.0);
@@ -874,8 +874,8 @@ struct CellOut {
 
 // Tile of the cell sweep: LA cells along the sweep x LL lines across.
 // Staged boxes (BOX_X x BH, tensor rows from y0 - YH): density1, energy1,
-// vol_flux_x, vol_flux_y.  pre_vol covers cells -1 .. LA along the sweep
-// (the donors of the tile's faces), fluxes faces 0 .. LA.
+// vol_flux_x, vol_flux_y.  The faces are 0 .. LA along the sweep (their
+// donors reach cells -1 .. LA).
 template <typename T, int DIR, int TY> struct CellLayout {
   static constexpr int LA = DIR == 1 ? TILE_X : TY;
   static constexpr int LL = DIR == 1 ? TY : TILE_X;
@@ -883,17 +883,16 @@ template <typename T, int DIR, int TY> struct CellLayout {
   static constexpr int BH = DIR == 1 ? TY + 2 : TY + 4;
   static constexpr int BOX = BOX_X * BH;
   static constexpr int BOXS = (BOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
-  static constexpr int NPV = LA + 2, NF = LA + 1;
+  static constexpr int NF = LA + 1;
   // face scratch: FP64 keeps each face's mass flux and energy flux; FP32
   // keeps the mass flux and e_adv as they were computed (single precision)
   // and forms the FP64 energy flux, an exact product, where it is used
   using FS = std::conditional_t<sizeof(T) == sizeof(double), double, float>;
-  static constexpr size_t SCRATCH_BYTES = ((size_t)2 * NF * LL * sizeof(FS) + (size_t)NPV * LL * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t SCRATCH_BYTES = ((size_t)2 * NF * LL * sizeof(FS) + 15) / 16 * 16;
   // then the widths (fill_widths): vertex widths and reciprocals along the sweep, celldx, celldy
   static constexpr int LV = DIR == 1 ? BOX_X : BH;
   static constexpr size_t GEO_BYTES = (size_t)2 * LV * sizeof(double) + (size_t)(BOX_X + BH) * sizeof(T);
   static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + SCRATCH_BYTES + GEO_BYTES;
-  __device__ static constexpr int pv(int p, int l) { return DIR == 1 ? l * NPV + p : p * LL + l; } // p = cell + 1
   __device__ static constexpr int fx(int p, int l) { return DIR == 1 ? l * NF + p : p * LL + l; }  // p = face
   __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
     if (DIR == 1) {
@@ -918,7 +917,6 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   using FS = typename L::FS;
   FS *s_mf = reinterpret_cast<FS *>(scratch);
   FS *s_ef = s_mf + L::NF * LL; // FP64: mass_flux * e_adv; FP32: e_adv
-  T *s_pv = reinterpret_cast<T *>(s_ef + L::NF * LL);
   const double *g_vd = reinterpret_cast<const double *>(reinterpret_cast<char *>(scratch) + L::SCRATCH_BYTES);
   const double *g_rvd = g_vd + L::LV;
   const T *g_x = reinterpret_cast<const T *>(g_rvd + L::LV), *g_y = g_x + BOX_X;
@@ -931,24 +929,15 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   const int pitch = (int)m.pitch;
   constexpr int ST = DIR == 1 ? 1 : BOX_X; // box stride along the sweep
   auto bidx = [&](int i, int j) { return (j - y0 + YH) * BOX_X + (i - x0 + HALO); };
-  // (1) pre_vol (advec_cell.cpp:42-61 / :134-153) of cells a0-1 .. a0+LA
-  for (int t = tid; t < L::NPV * LL; t += 256) {
-    int p, l;
-    L::item(t, L::NPV, LL, p, l);
-    const int a = a0 - 1 + p, line = l0 + l;
-    const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-    if (EDGE && (i > m.nx + 3 || j > m.ny + 3)) continue;
+  // pre_vol (advec_cell.cpp:42-61 / :134-153) of cell (i, j), formed where
+  // it is read (a face's donor, a cell's update) rather than stored
+  auto pre_vol_of = [&](int i, int j) -> T {
     const int b = bidx(i, j);
     const T vol = g_x[i - x0 + HALO] * g_y[j - y0 + YH];
-    T pv;
-    if (DIR == 1) {
-      pv = sweep == 1 ? cell_pre_vol1(vol, VFX[b], VFX[b + 1], VFY[b], VFY[b + BOX_X]) : cell_pre_vol2(vol, VFX[b], VFX[b + 1]);
-    } else {
-      pv = sweep == 1 ? cell_pre_vol1(vol, VFY[b], VFY[b + BOX_X], VFX[b], VFX[b + 1]) : cell_pre_vol2(vol, VFY[b], VFY[b + BOX_X]);
-    }
-    s_pv[L::pv(p, l)] = pv;
-  }
-  __syncthreads();
+    if (DIR == 1)
+      return sweep == 1 ? cell_pre_vol1(vol, VFX[b], VFX[b + 1], VFY[b], VFY[b + BOX_X]) : cell_pre_vol2(vol, VFX[b], VFX[b + 1]);
+    return sweep == 1 ? cell_pre_vol1(vol, VFY[b], VFY[b + BOX_X], VFX[b], VFX[b + 1]) : cell_pre_vol2(vol, VFY[b], VFY[b + BOX_X]);
+  };
   // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
   const bool edge = EDGE && fold;
   for (int t = tid; t < L::NF * LL; t += 256) {
@@ -967,7 +956,7 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
       donor = f; downwind = f - 1; dif = upwind;
     }
     const int bd = b + (donor - f) * ST, bu = b + (upwind - f) * ST, bw = b + (downwind - f) * ST;
-    const T pre_vol_d = s_pv[L::pv(donor - a0 + 1, l)];
+    const T pre_vol_d = DIR == 1 ? pre_vol_of(donor, line) : pre_vol_of(line, donor);
     T mass_flux, e_adv;
     T ratio;
     if constexpr (sizeof(T) == sizeof(double)) {
@@ -995,7 +984,7 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
     if (EDGE && (i >= m.nx + 2 || j >= m.ny + 2)) continue;
     const int b = bidx(i, j);
-    const T pre_vol = s_pv[L::pv(p + 1, l)];
+    const T pre_vol = pre_vol_of(i, j);
     const double mf_lo = s_mf[L::fx(p, l)], mf_hi = s_mf[L::fx(p + 1, l)];
     double ef_lo, ef_hi;
     if constexpr (sizeof(T) == sizeof(double)) {
