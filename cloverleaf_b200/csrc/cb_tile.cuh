@@ -37,6 +37,52 @@ __device__ __forceinline__ bool edge_tile(int nx, int ny, int x0, int y0, int ty
   return x0 < 12 || x0 + TILE_X > nx - 8 || y0 < 12 || y0 + ty > ny - 8;
 }
 
+// The (p, l) items of a stage of NP positions along a sweep times NL lines
+// across it that the calling thread owns, for 256 threads as 64 x 4: the
+// coordinate along x (p for the x sweep, DIR = 1; l for the y sweep) on
+// threadIdx.x, the other on threadIdx.y + 4 k, and the items past lane 63
+// (a few positions or one line) spread over the block's first threads.  A
+// thread's main items share one x coordinate, so their addresses differ by
+// constants.  f(k, p, l) gets the item's slot k < K, the same for every
+// thread's k-th item.
+template <int DIR, int NP, int NL> struct Items {
+  static constexpr int NA = DIR == 1 ? NP : NL; // along threadIdx.x
+  static constexpr int NB = DIR == 1 ? NL : NP; // along threadIdx.y
+  static constexpr int KB = (NB + 3) / 4;
+  static constexpr int TAIL = NA > 64 ? (NA - 64) * NB : 0;
+  static constexpr int KT = (TAIL + 255) / 256;
+  static constexpr int K = KB + KT;
+  template <typename F> __device__ __forceinline__ static void each(F &&f) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (NA >= 64 || tx < NA) {
+#pragma unroll
+      for (int kb = 0; kb < KB; ++kb) {
+        const int b = ty + 4 * kb;
+        if (NB % 4 == 0 || b < NB) {
+          if constexpr (DIR == 1)
+            f(kb, tx, b);
+          else
+            f(kb, b, tx);
+        }
+      }
+    }
+    if constexpr (TAIL > 0) {
+      const int tid = ty * 64 + tx;
+#pragma unroll
+      for (int kt = 0; kt < KT; ++kt) {
+        const int t = tid + 256 * kt;
+        if (t < TAIL) {
+          const int a = 64 + t % (NA - 64), b = t / (NA - 64);
+          if constexpr (DIR == 1)
+            f(KB + kt, a, b);
+          else
+            f(KB + kt, b, a);
+        }
+      }
+    }
+  }
+};
+
 // Staged boxes whose first row is y0 - 1: BH = rows + 2 (a one-row halo
 // above and below the tile), stride rounded to 128 bytes.
 template <typename T, int TY> struct Box1 {
@@ -807,8 +853,8 @@ template <> struct AdvecTiles<float> {
 
 // ---------------------------------------------------------------------------
 // advec_cell: src/serial/advec_cell.cpp:28-220, one sweep in one pass: the
-// face fluxes into shared memory, then the update; each stage spreads its
-// items evenly over the block's 256 threads, and pre_vol is formed from the
+// face fluxes into shared memory, then the update; each stage's items are
+// dealt to the threads as Items<> deals them, and pre_vol is formed from the
 // staged volume fluxes where a face or an update reads it.
 template <typename T>
 __device__ __forceinline__ T cell_limiter_value(T sigma, T sigma3, T sigma4, T diffuw, T diffdw) {
@@ -894,13 +940,6 @@ template <typename T, int DIR, int TY> struct CellLayout {
   static constexpr size_t GEO_BYTES = (size_t)2 * LV * sizeof(double) + (size_t)(BOX_X + BH) * sizeof(T);
   static constexpr size_t SMEM = (size_t)4 * BOXS * sizeof(T) + SCRATCH_BYTES + GEO_BYTES;
   __device__ static constexpr int fx(int p, int l) { return DIR == 1 ? l * NF + p : p * LL + l; }  // p = face
-  __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
-    if (DIR == 1) {
-      p = k % np, l = k / np;
-    } else {
-      l = k % nl, p = k / nl;
-    }
-  }
 };
 
 // EDGE = false: a tile whose every position lies inside the mesh's extents
@@ -923,7 +962,6 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const int vo = DIR == 1 ? HALO - x0 : YH - y0; // index of the sweep's vertex width of position a: a + vo
   const T *D1 = sm, *E1 = sm + L::BOXS, *VFX = sm + 2 * L::BOXS, *VFY = sm + 3 * L::BOXS;
-  const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
   const int a0 = DIR == 1 ? x0 : y0, l0 = DIR == 1 ? y0 : x0;
   const int pitch = (int)m.pitch;
@@ -940,12 +978,10 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   };
   // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
   const bool edge = EDGE && fold;
-  for (int t = tid; t < L::NF * LL; t += 256) {
-    int p, l;
-    L::item(t, L::NF, LL, p, l);
+  Items<DIR, L::NF, LL>::each([&](int, int p, int l) {
     const int f = a0 + p, line = l0 + l; // position of the face along the sweep
     const int i = DIR == 1 ? f : line, j = DIR == 1 ? line : f;
-    if (EDGE && (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3))) continue;
+    if (EDGE && (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3))) return;
     const int b = bidx(i, j);
     const T flux = DIR == 1 ? VFX[b] : VFY[b];
     int upwind, donor, downwind, dif;
@@ -974,15 +1010,13 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
     const bool halo_face = EDGE && fold && f == na + 3; // with a fold, face na+3 takes its halo value
     if (!halo_face) mf[gidx(pitch, i, j)] = mass_flux;
     if (edge && f < na + 3) fold_halo(mf, m, halo_rule(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y), fold, i, j, mass_flux);
-  }
+  });
   __syncthreads();
   // (3) the update (:117-129 / :209-221), mass/energy accumulation in FP64
-  for (int t = tid; t < LA * LL; t += 256) {
-    int p, l;
-    L::item(t, LA, LL, p, l);
+  Items<DIR, LA, LL>::each([&](int, int p, int l) {
     const int a = a0 + p, line = l0 + l;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-    if (EDGE && (i >= m.nx + 2 || j >= m.ny + 2)) continue;
+    if (EDGE && (i >= m.nx + 2 || j >= m.ny + 2)) return;
     const int b = bidx(i, j);
     const T pre_vol = pre_vol_of(i, j);
     const double mf_lo = s_mf[L::fx(p, l)], mf_hi = s_mf[L::fx(p + 1, l)];
@@ -1025,7 +1059,7 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
         fold_halo((T *)out.energy0, m, halo_rule(ENERGY0), out.rfold, i, j, enew);
       }
     }
-  }
+  });
 }
 
 // Fields the cell sweep stages: sweep 2 of x needs no y fluxes.
@@ -1070,8 +1104,8 @@ __global__ void __launch_bounds__(256, 5) kt_advec_cell(const __grid_constant__ 
 // lines across it.  Positions p = 0 .. LA+2 along the sweep map to nodes
 // a = a0 - 2 + p; the stages cover only the positions the tile's outputs
 // need (node flux and cell mass p = 0..LA+2, momentum fluxes 1..LA+1,
-// updates 2..LA+1), and every stage spreads its (position, line) items
-// evenly over the block's 256 threads.
+// updates 2..LA+1), and every stage deals its (position, line) items to the
+// threads as Items<> deals them.
 //
 // Cell masses density1 * post_vol are formed once per cell (the reference
 // forms each four times inside node_mass_post, :93-102 / :165-174, with the
@@ -1154,14 +1188,6 @@ template <typename T, int DIR, int TY> struct MomLayout {
   // work-array indices: the thread-fastest coordinate is the contiguous one
   __device__ static constexpr int cm(int p, int lc) { return DIR == 1 ? lc * NP + p : p * (LL + 1) + lc; }
   __device__ static constexpr int w(int p, int l) { return DIR == 1 ? l * NP + p : p * LL + l; }
-  // the k-th item of an np x nl stage: (p, l) with the contiguous coordinate fastest
-  __device__ static constexpr void item(int k, int np, int nl, int &p, int &l) {
-    if (DIR == 1) {
-      p = k % np, l = k / np;
-    } else {
-      l = k % nl, p = k / nl;
-    }
-  }
 };
 
 // EDGE = false: a tile whose every position lies inside the mesh's extents
@@ -1178,7 +1204,6 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
   const T *U1 = sm, *V1 = sm + L::BOXS, *D1 = sm + 2 * L::BOXS, *MF = sm + 3 * L::BOXS, *VFO = sm + 4 * L::BOXS;
   T *region = sm + 2 * L::BOXS;
   T *s_cm = region, *s_nf = s_cm + L::N_CM, *s_mfu = s_nf + L::N_W, *s_mfv = s_mfu + L::N_W;
-  const int tid = threadIdx.y * 64 + threadIdx.x;
   const int na = DIR == 1 ? m.nx : m.ny, nlmax = DIR == 1 ? m.ny : m.nx;
   const int a0 = DIR == 1 ? x0 : y0, l0 = DIR == 1 ? y0 : x0;
   const int pitch = (int)m.pitch;
@@ -1188,62 +1213,31 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
   auto bidx = [&](int i, int j) { return (j - y0 + YH) * BOX_X + (i - x0 + HALO); };
 
   // (1) cell masses and node fluxes into registers, then into the region
-  constexpr int K_CM = (L::N_CM + 255) / 256, K_NF = (L::N_W + 255) / 256;
-  T r_cm[K_CM], r_nf[K_NF];
-#pragma unroll
-  for (int k = 0; k < K_CM; ++k) {
-    const int t = tid + 256 * k;
-    T v = T(0.0);
-    if (t < L::N_CM) {
-      int p, lc;
-      L::item(t, NP, LL + 1, p, lc);
-      const int a = a0 - 2 + p, line = l0 - 1 + lc;
-      if (!EDGE || (a >= 0 && a <= na + 3 && line >= 0 && line <= nlmax + 3)) {
-        const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
-        const int b = bidx(i, j);
-        const T vol = sm[L::GEO + i - x0 + HALO] * sm[L::GEO + BOX_X + j - y0 + YH];
-        // post_vol (:42-77): mom_sweep 1 vol + vfy difference, 2 vol + vfx difference, 3/4 vol
-        const T pv = mom_sweep == 1 ? mom_post_vol(1, vol, VFO[b], VFO[b + BOX_X]) : mom_sweep == 2 ? mom_post_vol(2, vol, VFO[b], VFO[b + 1]) : vol;
-        v = D1[b] * pv;
-      }
+  using ICM = Items<DIR, NP, LL + 1>; // cell masses: positions 0 .. LA+2, cell lines -1 .. LL-1
+  using INF = Items<DIR, NP, LL>;     // node fluxes: positions 0 .. LA+2
+  T r_cm[ICM::K] = {}, r_nf[INF::K] = {};
+  ICM::each([&](int k, int p, int lc) {
+    const int a = a0 - 2 + p, line = l0 - 1 + lc;
+    if (!EDGE || (a >= 0 && a <= na + 3 && line >= 0 && line <= nlmax + 3)) {
+      const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
+      const int b = bidx(i, j);
+      const T vol = sm[L::GEO + i - x0 + HALO] * sm[L::GEO + BOX_X + j - y0 + YH];
+      // post_vol (:42-77): mom_sweep 1 vol + vfy difference, 2 vol + vfx difference, 3/4 vol
+      const T pv = mom_sweep == 1 ? mom_post_vol(1, vol, VFO[b], VFO[b + BOX_X]) : mom_sweep == 2 ? mom_post_vol(2, vol, VFO[b], VFO[b + 1]) : vol;
+      r_cm[k] = D1[b] * pv;
     }
-    r_cm[k] = v;
-  }
-#pragma unroll
-  for (int k = 0; k < K_NF; ++k) {
-    const int t = tid + 256 * k;
-    T v = T(0.0);
-    if (t < L::N_W) {
-      int p, l;
-      L::item(t, NP, LL, p, l);
-      const int a = a0 - 2 + p, line = l0 + l;
-      if (!EDGE || (line < nlmax + 3 && a >= 0 && a <= na + 3)) {
-        const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
-        // (:84-88 / :156-160) dir 1: mf(a, j-1) + mf(a, j) + mf(a+1, j-1) + mf(a+1, j); dir 2: mf(i-1, a) + mf(i, a) + mf(i-1, a+1) + mf(i, a+1)
-        v = quarter_sum(MF[b - SL], MF[b], MF[b + ST - SL], MF[b + ST]);
-      }
+  });
+  INF::each([&](int k, int p, int l) {
+    const int a = a0 - 2 + p, line = l0 + l;
+    if (!EDGE || (line < nlmax + 3 && a >= 0 && a <= na + 3)) {
+      const int b = DIR == 1 ? bidx(a, line) : bidx(line, a);
+      // (:84-88 / :156-160) dir 1: mf(a, j-1) + mf(a, j) + mf(a+1, j-1) + mf(a+1, j); dir 2: mf(i-1, a) + mf(i, a) + mf(i-1, a+1) + mf(i, a+1)
+      r_nf[k] = quarter_sum(MF[b - SL], MF[b], MF[b + ST - SL], MF[b + ST]);
     }
-    r_nf[k] = v;
-  }
+  });
   __syncthreads(); // density1, mass flux and volume flux boxes are dead from here on
-#pragma unroll
-  for (int k = 0; k < K_CM; ++k) {
-    const int t = tid + 256 * k;
-    if (t < L::N_CM) {
-      int p, lc;
-      L::item(t, NP, LL + 1, p, lc);
-      s_cm[L::cm(p, lc)] = r_cm[k];
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < K_NF; ++k) {
-    const int t = tid + 256 * k;
-    if (t < L::N_W) {
-      int p, l;
-      L::item(t, NP, LL, p, l);
-      s_nf[L::w(p, l)] = r_nf[k];
-    }
-  }
+  ICM::each([&](int k, int p, int lc) { s_cm[L::cm(p, lc)] = r_cm[k]; });
+  INF::each([&](int k, int p, int l) { s_nf[L::w(p, l)] = r_nf[k]; });
   __syncthreads();
 
   // node_mass_post (:93-96 / :165-168) of node (p, l): cells (i, j-1), (i, j), (i-1, j-1), (i-1, j)
@@ -1260,12 +1254,10 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
   // (3) mom_flux (:108-133 / :180-205) over positions 1 .. LA+1
   // the sweep direction's cell widths: position a at celld[a]
   const T *celld = DIR == 1 ? sm + L::GEO + HALO - x0 : sm + L::GEO + BOX_X + YH - y0;
-  for (int t = tid; t < (LA + 1) * LL; t += 256) {
-    int p, l;
-    L::item(t, LA + 1, LL, p, l);
+  Items<DIR, LA + 1, LL>::each([&](int, int p, int l) {
     p += 1;
     const int a = a0 - 2 + p, line = l0 + l;
-    if (EDGE && (line >= nlmax + 3 || a < 1 || a > na + 2)) continue;
+    if (EDGE && (line >= nlmax + 3 || a < 1 || a > na + 2)) return;
     const T nfv = s_nf[L::w(p, l)];
     int upwind, donor, downwind, dif;
     if (nfv < T(0.0)) {
@@ -1280,17 +1272,15 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
     const int bd = b + (donor - a) * ST, bu = b + (upwind - a) * ST, bw = b + (downwind - a) * ST;
     if (vel_mask & 1) s_mfu[L::w(p, l)] = mom_flux_value(sigma, nfv, width, dxd, U1[bd], U1[bu], U1[bw]);
     if (vel_mask & 2) s_mfv[L::w(p, l)] = mom_flux_value(sigma, nfv, width, dxd, V1[bd], V1[bu], V1[bw]);
-  }
+  });
   __syncthreads();
 
   // (4) velocity update (:139-144 / :211-216) over positions 2 .. LA+1
   const bool do_fold = EDGE && fold;
-  for (int t = tid; t < LA * LL; t += 256) {
-    int p, l;
-    L::item(t, LA, LL, p, l);
+  Items<DIR, LA, LL>::each([&](int, int p, int l) {
     p += 2;
     const int a = a0 - 2 + p, line = l0 + l;
-    if (EDGE && (line > nlmax + 2 || a > na + 2)) continue;
+    if (EDGE && (line > nlmax + 2 || a > na + 2)) return;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
     const int b = bidx(i, j);
     const T nmpost = node_mass_post(p, l), nmpre = mom_node_mass_pre(nmpost, s_nf[L::w(p - 1, l)], s_nf[L::w(p, l)]);
@@ -1313,7 +1303,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
         if (EDGE && out.rfold) fold_halo((T *)out.yvel0, m, halo_rule(YVEL0), out.rfold, i, j, v);
       }
     }
-  }
+  });
 }
 
 // Fields the momentum sweep stages: the other direction's volume flux only for mom_sweep 1 and 2.
