@@ -1086,10 +1086,12 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
   return true;
 }
 
-// Five blocks per SM: the register budget that keeps the staged boxes of
-// five tiles resident.
+// Blocks per SM the register budget must allow: five in FP64 (the staged
+// boxes of five tiles), six in FP32.
+template <typename T> constexpr int cell_min_blocks() { return sizeof(T) == sizeof(double) ? 5 : 6; }
+
 template <typename T, int DIR, int TY>
-__global__ void __launch_bounds__(256, 5) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
+__global__ void __launch_bounds__(256, cell_min_blocks<T>()) kt_advec_cell(const __grid_constant__ Maps maps, CellOut out, Mesh<T> m, int off, int sweep,
                                                      int fold, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
