@@ -705,7 +705,9 @@ def main():
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = traffic_per_launch(dom, S)
     roof = {"kernel": dom, "timed_in": "host_loop (the same kernel runs in the graph)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            "frac": achieved / peak,
+            "traffic_frac": (traffic / (avg_ms / 1e3) / 1e9 / peak) if traffic else None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6.65 TB/s", "traffic": traffic, "alg_bytes_per_launch": alg,
             "step_frac": value / world * STEP_ARRAYS * 8 / 1e9 / peak,
             "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)}}
