@@ -43,6 +43,7 @@ template <typename T> struct Ops {
   static cudaError_t field_summary(Chunk &c);
   // fused passes of the resident loop: viscosity + calc_dt, PdV corrector + flux_calc
   static cudaError_t visc_dt(Chunk &c, const DtConsts &k, int fold);
+  static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold); // ideal_gas too
   static cudaError_t pdv_flux(Chunk &c, double dt, int fold, int flux_fold);
 };
 

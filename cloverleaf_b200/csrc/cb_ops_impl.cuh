@@ -266,6 +266,22 @@ template <typename T> cudaError_t Ops<T>::visc_dt(Chunk &c, const DtConsts &k, i
   return launched(c);
 }
 
+template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold) {
+  constexpr int TY = VISC_TY;
+  using B = Box1<T, TY>;
+  const size_t smem = 4 * B::BOXS * sizeof(T);
+  cudaError_t e = allow_smem(kt_ig_visc_dt<T>, smem);
+  if (e != cudaSuccess) return e;
+  const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt_ig_visc_dt<T>, 256, smem)) != cudaSuccess) return e;
+  const int grid = std::min(nt, c.sms * std::max(per_sm, 1));
+  kt_ig_visc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {DENSITY0, ENERGY0, XVEL0, YVEL0}), (T *)c.base(PRESSURE),
+                                                          (T *)c.base(SOUNDSPEED), (T *)c.base(VISCOSITY), mesh<T>(c), (int)c.off, k,
+                                                          gm1<T>(c), ig_fold, fold, tx, nt, c.d_dt_bits, c.d_err);
+  return launched(c);
+}
+
 template <typename T> cudaError_t Ops<T>::pdv_flux(Chunk &c, double dt, int fold, int flux_fold) {
   constexpr int TY = PDV_TY;
   using B = Box1<T, TY>;

@@ -158,9 +158,10 @@ template <typename T> struct Seq {
   unsigned written = 0;
   std::vector<Pass> passes;
   cudaError_t err = cudaSuccess;
-  // fused emission (only with every producer folding): viscosity + calc_dt
-  // in one pass, the PdV corrector + flux_calc in one pass, and reset_field
-  // done by the second sweeps; the freshness moves exactly as unfused
+  // fused emission (only with every producer folding): ideal_gas +
+  // viscosity + calc_dt in one pass, the PdV corrector + flux_calc in one
+  // pass, and reset_field done by the second sweeps; the freshness moves
+  // exactly as unfused
   bool fuse = false;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
@@ -194,7 +195,7 @@ template <typename T> struct Seq {
   // driver/timestep.cpp:37-73 up to calc_dt
   void timestep_front() {
     const int fi = eff(dep(1));
-    if (emit) run(Ops<T>::ideal_gas(c, 0, fi));
+    if (emit && !fuse) run(Ops<T>::ideal_gas(c, 0, fi));
     wrote({P}, fi);
     wrote({SS}, 0);
     halo({P, E0, D0, U0, V0}, 1);
@@ -202,7 +203,9 @@ template <typename T> struct Seq {
     if (emit && !fuse) run(Ops<T>::viscosity(c, fv));
     wrote({Q}, fv);
     halo({Q}, 1); // (no pass when fused: q is fresh to depth 1)
-    if (emit) run(fuse ? Ops<T>::visc_dt(c, dk, fv) : Ops<T>::calc_dt(c, dk));
+    // fused: ideal_gas, viscosity and calc_dt in one pass here (the halo
+    // passes between them are none: density0 / energy0 and q are fresh)
+    if (emit) run(fuse ? Ops<T>::ig_visc_dt(c, dk, fi, fv) : Ops<T>::calc_dt(c, dk));
     ++pos;
   }
   // driver/hydro.cpp:69-75 and src/serial/PdV.cpp:92-133, dt from the device

@@ -423,6 +423,17 @@ __global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Map
   block_min_to(vmin, dt_bits);
 }
 
+// The ideal-gas law of one cell (src/serial/ideal_gas.cpp:28-48).
+template <typename T>
+__device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressure, T &soundspeed) {
+  T v = lim_div(T(1.0), density); // feeds the sound speed only
+  pressure = gm1 * density * energy;
+  T pressurebyenergy = gm1 * density;
+  T pressurebyvolume = -density * pressure;
+  T sound_speed_squared = v * v * (pressure * pressurebyenergy - pressurebyvolume);
+  soundspeed = sqrt(sound_speed_squared);
+}
+
 // ---------------------------------------------------------------------------
 // viscosity and calc_dt in one pass (the resident loop): a tile's q is
 // computed and stored as viscosity_tile does, then used for the tile's dt as
@@ -431,9 +442,16 @@ __global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Map
 // one read of density0.  Staged: ms 0 pressure, 1 xvel0, 2 yvel0.
 static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height");
 
-template <typename T>
+// IG: ideal_gas (the step's first phase) in the same pass as well: the tile
+// stages density0 / energy0 instead of pressure, forms each cell's pressure
+// and sound speed as k_ideal_gas does (written, the pressure with its halo of
+// depth ig_fold) and the neighbours' pressures viscosity reads from the
+// staged density0 / energy0 (their halos hold the mirrored values, so the
+// mirrored pressures come out as ideal_gas's fold writes them).
+template <typename T, bool IG = false>
 __device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, T *q_out, const Mesh<T> &m, int off,
-                                             const DtConsts &k, int fold, int bx, int by, double &vmin, RestMemo<T> &memo) {
+                                             const DtConsts &k, int fold, int bx, int by, double &vmin, RestMemo<T> &memo, T gm1 = T(0),
+                                             T *p_out = nullptr, T *c_out = nullptr, int ig_fold = 0) {
   constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
   const T *S = (const T *)in.soundspeed, *R = (const T *)in.density0;
@@ -442,29 +460,52 @@ __device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const int i = x0 + threadIdx.x;
   T ss[RPT], dd[RPT];
+  if constexpr (!IG) {
 #pragma unroll
-  for (int r = 0; r < RPT; ++r) {
-    const int j = y0 + threadIdx.y + 4 * r;
-    const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
-    const int g = gidx(pitch, i, j);
-    ss[r] = in_mesh ? S[g] : T(0);
-    dd[r] = in_mesh ? R[g] : T(1);
+    for (int r = 0; r < RPT; ++r) {
+      const int j = y0 + threadIdx.y + 4 * r;
+      const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
+      const int g = gidx(pitch, i, j);
+      ss[r] = in_mesh ? S[g] : T(0);
+      dd[r] = in_mesh ? R[g] : T(1);
+    }
   }
-  if (!stage(cx, sm, ms, 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
-  const T *P = sm, *U = sm + B::BOXS, *V = sm + 2 * B::BOXS;
+  if (!stage(cx, sm, ms, IG ? 4 : 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  // staged: pressure, xvel0, yvel0 -- or (IG) density0, energy0, xvel0, yvel0
+  const T *P = sm, *D = sm, *E = sm + B::BOXS;
+  const T *U = sm + (IG ? 2 : 1) * B::BOXS, *V = sm + (IG ? 3 : 2) * B::BOXS;
   const double thr = sizeof(T) == sizeof(double) ? warp_min(vmin) * DT_SKIP : 0.0;
   if (i < m.nx + 2) {
-    const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
+    const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
+    const bool do_fold = fold && near;
     const T cdx = m.celldx_t[i], cdx1 = m.celldx_t[i + 1];
 #pragma unroll
     for (int r = 0; r < RPT; ++r) {
       const int j = y0 + threadIdx.y + 4 * r;
       if (j >= m.ny + 2) break;
       const int b = B::at(i, j, x0, y0);
+      const int g = gidx(pitch, i, j);
       const T cdy = m.celldy_t[j];
-      const T q = viscosity_value(U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1], P[b - 1],
-                                  P[b + 1], P[b - BOX_X], P[b + BOX_X], dd[r], cdx, cdx1, cdy, m.celldy_t[j + 2]);
-      q_out[gidx(pitch, i, j)] = q;
+      T pl, pr, pb, pt;
+      if constexpr (IG) {
+        // src/serial/ideal_gas.cpp:28-48 for the cell; pressure alone for its neighbours
+        T p, c;
+        eos_value(D[b], E[b], gm1, p, c);
+        p_out[g] = p;
+        c_out[g] = c;
+        if (ig_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), ig_fold, i, j, p);
+        ss[r] = c;
+        dd[r] = D[b];
+        pl = gm1 * D[b - 1] * E[b - 1];
+        pr = gm1 * D[b + 1] * E[b + 1];
+        pb = gm1 * D[b - BOX_X] * E[b - BOX_X];
+        pt = gm1 * D[b + BOX_X] * E[b + BOX_X];
+      } else {
+        pl = P[b - 1], pr = P[b + 1], pb = P[b - BOX_X], pt = P[b + BOX_X];
+      }
+      const T q = viscosity_value(U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1], pl, pr, pb,
+                                  pt, dd[r], cdx, cdx1, cdy, m.celldy_t[j + 2]);
+      q_out[g] = q;
       if (do_fold) fold_halo(q_out, m, halo_rule(VISCOSITY), fold, i, j, q);
       if (memo.seen(at_rest(q, U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1]), ss[r], dd[r],
                     cdx, cdy))
@@ -494,6 +535,25 @@ __global__ void __launch_bounds__(256, 4) kt_visc_dt(const __grid_constant__ Map
   RestMemo<T> memo;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     if (!visc_dt_tile(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin, memo)) return;
+  block_min_to(vmin, dt_bits);
+}
+
+// ideal_gas, viscosity and calc_dt in one pass (the resident loop).
+template <typename T>
+__global__ void __launch_bounds__(256, 4) kt_ig_visc_dt(const __grid_constant__ Maps maps, T *p_out, T *c_out, T *q_out, Mesh<T> m, int off,
+                                                     DtConsts k, T gm1, int ig_fold, int fold, int tiles_x, int ntiles,
+                                                     unsigned long long *dt_bits, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  T *sm = reinterpret_cast<T *>(smraw);
+  TileCtx cx = tile_ctx(&bar, err);
+  const MapSet ms = map_set(maps, 4);
+  const DtIn in{nullptr, nullptr, nullptr};
+  double vmin = g_big;
+  RestMemo<T> memo;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    if (!visc_dt_tile<T, true>(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin, memo, gm1, p_out, c_out, ig_fold))
+      return;
   block_min_to(vmin, dt_bits);
 }
 
@@ -547,15 +607,6 @@ __device__ __forceinline__ void pdv_value(bool predict, T dt, T xa, T ya, T vol,
   density1 = d0 * volume_change_s;
 }
 
-template <typename T>
-__device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressure, T &soundspeed) {
-  T v = lim_div(T(1.0), density); // feeds the sound speed only
-  pressure = gm1 * density * energy;
-  T pressurebyenergy = gm1 * density;
-  T pressurebyvolume = -density * pressure;
-  T sound_speed_squared = v * v * (pressure * pressurebyenergy - pressurebyvolume);
-  soundspeed = sqrt(sound_speed_squared);
-}
 
 struct PdvIn {
   const void *density0, *energy0, *pressure, *viscosity;
