@@ -38,8 +38,8 @@ struct BatchDeck {
   // layout (as cb_create lays out one chunk)
   int nx, ny, off, pitch;
   size_t buf_bytes;           // bytes of each buffer (a multiple of 256)
-  void *buf[NUM_BUF];         // the 15 state fields in field order, then the 4 spares
-  const CUtensorMap *maps;    // [NUM_BUF][NUM_BOX_H], in global memory
+  void *buf[BATCH_BUF];        // the 15 state fields in field order, then the 4 spares
+  const CUtensorMap *maps;     // [BATCH_BUF][NUM_BOX_H], in global memory
   const double *geom_d[NUM_GEOM];
   const void *geom_t[NUM_GEOM];
   const double *rgeom;        // 1 / celldx, 1 / celldy, 1 / vertexdx, 1 / vertexdy

@@ -41,7 +41,7 @@ struct cb_batch {
   double *geom = nullptr;           // FP64 geometry of every deck
   double *rgeom = nullptr;          // reciprocal widths of every deck
   void *geom_t = nullptr;           // geometry in the storage type (FP32 form)
-  CUtensorMap *maps = nullptr;      // [deck][NUM_BUF][NUM_BOX_H]
+  CUtensorMap *maps = nullptr;      // [deck][BATCH_BUF][NUM_BOX_H]
   double *records = nullptr;        // summaries, dt traces, partials
   unsigned long long *slots = nullptr;
   BatchDeck *d_desc = nullptr;
@@ -309,7 +309,7 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
     const size_t elems = (size_t)D.off + (size_t)D.pitch * (size_t)(d.ny + 6) + (size_t)align;
     D.buf_bytes = round_up(elems * b->esize, 256);
     pool_off[k] = pool_bytes;
-    pool_bytes += D.buf_bytes * NUM_BUF;
+    pool_bytes += D.buf_bytes * BATCH_BUF;
     geom_off[k] = geom_elems;
     geom_elems += (size_t)NUM_GEOM * (std::max(d.nx, d.ny) + 6);
     b->work[k] = estimate_steps(d) * (double)d.nx * d.ny;
@@ -324,19 +324,19 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
   if ((e = cudaMalloc(&b->geom, geom_elems * sizeof(double))) != cudaSuccess) return bail(e, "geometry");
   if ((e = cudaMalloc(&b->rgeom, geom_elems / 2 * sizeof(double))) != cudaSuccess) return bail(e, "geometry");
   if (precision == CB_FP32 && (e = cudaMalloc(&b->geom_t, geom_elems * sizeof(float))) != cudaSuccess) return bail(e, "geometry");
-  if ((e = cudaMalloc(&b->maps, sizeof(CUtensorMap) * NUM_BUF * NUM_BOX_H * ndecks)) != cudaSuccess) return bail(e, "tensor maps");
+  if ((e = cudaMalloc(&b->maps, sizeof(CUtensorMap) * BATCH_BUF * NUM_BOX_H * ndecks)) != cudaSuccess) return bail(e, "tensor maps");
   if ((e = cudaMalloc(&b->records, sizeof(double) * rec_elems)) != cudaSuccess) return bail(e, "records");
   if ((e = cudaMalloc(&b->slots, sizeof(unsigned long long) * 4 * ndecks)) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&b->d_desc, sizeof(BatchDeck) * ndecks)) != cudaSuccess) return bail(e, "descriptors");
   if ((e = cudaMallocHost(&b->h_desc, sizeof(BatchDeck) * ndecks)) != cudaSuccess) return bail(e, "descriptors");
   if ((e = cudaMalloc(&b->d_flags, sizeof(int) * 2)) != cudaSuccess) return bail(e, "scratch");
   std::vector<double> gh(geom_elems, 0.0), rh(geom_elems / 2, 0.0);
-  std::vector<CUtensorMap> maps((size_t)NUM_BUF * NUM_BOX_H * ndecks);
+  std::vector<CUtensorMap> maps((size_t)BATCH_BUF * NUM_BOX_H * ndecks);
   for (int k = 0; k < ndecks; ++k) {
     const cb_deck &d = decks[k];
     BatchDeck &D = b->desc[k];
     const int glen = std::max(d.nx, d.ny) + 6;
-    for (int bb = 0; bb < NUM_BUF; ++bb) D.buf[bb] = (char *)b->pool + pool_off[k] + (size_t)bb * D.buf_bytes;
+    for (int bb = 0; bb < BATCH_BUF; ++bb) D.buf[bb] = (char *)b->pool + pool_off[k] + (size_t)bb * D.buf_bytes;
     double *g[NUM_GEOM];
     for (int q = 0; q < NUM_GEOM; ++q) {
       g[q] = gh.data() + geom_off[k] + (size_t)q * glen;
@@ -352,13 +352,13 @@ int cb_batch_create(int ndecks, const cb_deck *decks, int precision, int device,
     D.rgeom = b->rgeom + geom_off[k] / 2;
     D.geom_len = glen;
     std::string err;
-    if (!encode_buffer_maps(D.buf, NUM_BUF, D.pitch, d.ny, precision,
-                            reinterpret_cast<CUtensorMap(*)[NUM_BOX_H]>(&maps[(size_t)k * NUM_BUF * NUM_BOX_H]), &err)) {
+    if (!encode_buffer_maps(D.buf, BATCH_BUF, D.pitch, d.ny, precision,
+                            reinterpret_cast<CUtensorMap(*)[NUM_BOX_H]>(&maps[(size_t)k * BATCH_BUF * NUM_BOX_H]), &err)) {
       release(b);
       delete b;
       return fail(CB_ECUDA, "cb_batch_create: " + err);
     }
-    D.maps = b->maps + (size_t)k * NUM_BUF * NUM_BOX_H;
+    D.maps = b->maps + (size_t)k * BATCH_BUF * NUM_BOX_H;
     D.gm1 = d.gamma - 1.0;
     D.nstates = d.nstates;
     for (int s = 0; s < d.nstates; ++s) {

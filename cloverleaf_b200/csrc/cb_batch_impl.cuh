@@ -282,7 +282,7 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
   // build_field (src/serial/build_field.cpp:29-180): every buffer to zero
   {
     const size_t nv = D->buf_bytes / 16;
-    for (int b = 0; b < NUM_BUF; ++b) {
+    for (int b = 0; b < BATCH_BUF; ++b) {
       uint4 *p = (uint4 *)D->buf[b];
       for (size_t e = lt; e < nv; e += lstride) p[e] = make_uint4(0u, 0u, 0u, 0u);
     }

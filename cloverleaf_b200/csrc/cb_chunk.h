@@ -12,8 +12,11 @@
 
 namespace cb {
 
-constexpr int NUM_SPARE = 4;            // second buffers of the double-buffered phases
+// second buffers of the double-buffered phases: 0 density1, 1 energy1,
+// 2 xvel1, 3 yvel1 (advection), 4 pressure (the resident loop's fused step)
+constexpr int NUM_SPARE = 5;
 constexpr int NUM_BUF = 15 + NUM_SPARE; // device buffers of the 15 state fields + spares
+constexpr int BATCH_BUF = 15 + 4;       // a batch deck's buffers: the state fields + the advection spares
 constexpr int NUM_BOX_H = 6;            // staged box heights (rows) with a tensor map each
 constexpr int BOX_HEIGHTS[NUM_BOX_H] = {10, 12, 16, 18, 20, 24};
 

@@ -298,6 +298,19 @@ template <typename T> cudaError_t Ops<T>::pdv_flux(Chunk &c, double dt, int fold
   return launched(c);
 }
 
+template <typename T> cudaError_t Ops<T>::pdvp_accelerate(Chunk &c, void *p_out, int p_fold, int acc_fold) {
+  constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 16;
+  using L = PdvAccLayout<T, TY>;
+  cudaError_t e = allow_smem(kt_pdvp_acc<T, TY>, L::SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
+  kt_pdvp_acc<T, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(
+      maps_of<L::B::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, PRESSURE, VISCOSITY}), (T *)p_out, (T *)c.base(SOUNDSPEED),
+      (T *)c.base(DENSITY1), (T *)c.base(ENERGY1), (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, T(0), c.dt_dev,
+      gm1<T>(c), p_fold, acc_fold, c.d_err);
+  return launched(c);
+}
+
 template <typename T> cudaError_t Ops<T>::field_summary(Chunk &c) {
   dim3 b(32, 8);
   const int tx = (c.nx + 31) / 32, ty = (c.ny + 7) / 8;

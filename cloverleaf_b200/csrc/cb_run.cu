@@ -159,9 +159,9 @@ template <typename T> struct Seq {
   std::vector<Pass> passes;
   cudaError_t err = cudaSuccess;
   // fused emission (only with every producer folding): ideal_gas +
-  // viscosity + calc_dt in one pass, the PdV corrector + flux_calc in one
-  // pass, and reset_field done by the second sweeps; the freshness moves
-  // exactly as unfused
+  // viscosity + calc_dt in one pass, the PdV predictor + accelerate in one
+  // pass, the PdV corrector + flux_calc in one pass, and reset_field done by
+  // the second sweeps; the freshness moves exactly as unfused
   bool fuse = false;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
@@ -204,14 +204,25 @@ template <typename T> struct Seq {
     wrote({Q}, fv);
     halo({Q}, 1); // (no pass when fused: q is fresh to depth 1)
     // fused: ideal_gas, viscosity and calc_dt in one pass here (the halo
-    // passes between them are none: density0 / energy0 and q are fresh)
+    // passes between them are none: density0 / energy0 and q are fresh),
+    // the pressure written to its second buffer (see lagrange)
+    if (fuse) swap_pressure();
     if (emit) run(fuse ? Ops<T>::ig_visc_dt(c, dk, fi, fv) : Ops<T>::calc_dt(c, dk));
     ++pos;
   }
+  // Fused, the predicted pressure goes to the other of two buffers: the pass
+  // that makes it reads the previous pressure of cells other tiles predict.
+  // ideal_gas swaps as well, so a step leaves the buffer map as it found it.
+  void swap_pressure() { std::swap(c.fbuf[P], c.sbuf[4]); }
   // driver/hydro.cpp:69-75 and src/serial/PdV.cpp:92-133, dt from the device
   void lagrange() {
     const int fp = eff(1); // the predictor makes its own pressure halo
-    if (emit) {
+    const int fa = eff(dep(2));
+    if (fuse) {
+      // fused: the predictor and accelerate in one pass
+      if (emit) run(Ops<T>::pdvp_accelerate(c, c.spare_base(4), fp, fa));
+      swap_pressure();
+    } else if (emit) {
       run(Ops<T>::pdv(c, 1, 0.0, 1, fp));
       if (fp == 0) {
         HaloJob job{};
@@ -222,8 +233,7 @@ template <typename T> struct Seq {
     }
     wrote({P}, fp);
     wrote({SS, D1, E1}, 0);
-    const int fa = eff(dep(2));
-    if (emit) run(Ops<T>::accelerate(c, 0.0, fa));
+    if (emit && !fuse) run(Ops<T>::accelerate(c, 0.0, fa));
     wrote({U1, V1}, fa);
     const int fc = eff(dep(2));
     const int ff = eff(dep(2));

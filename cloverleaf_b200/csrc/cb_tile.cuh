@@ -833,6 +833,93 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 }
 
 // ---------------------------------------------------------------------------
+// The PdV predictor and accelerate in one pass (the resident loop).  A tile
+// of accelerate's nodes reads the predicted pressure of the cells around
+// them, a ring one cell wider than the tile's own cells on their low sides:
+// the tile evaluates the predictor there as pdv_tile mode 1 does -- a halo
+// cell through its mirror interior cell (its index clamped: the depth-1
+// reflection that the predictor's fold writes) -- keeps the pressures in
+// shared memory, writes the predictor's outputs for its own cells, then
+// accelerates its nodes.  The predicted pressure goes to p_out, a buffer
+// other than the pressure's current one, because other tiles still read the
+// old pressure of their ring cells; the caller swaps the two.
+// Staged (Box1): 0 xvel0, 1 yvel0, 2 density0, 3 energy0, 4 pressure, 5 viscosity.
+template <typename T, int TY> struct PdvAccLayout {
+  using B = Box1<T, TY>;
+  static constexpr int NCX = TILE_X + 1, NCY = TY + 1; // ring cells along x and y
+  static constexpr size_t SMEM = (size_t)(6 * B::BOXS + NCX * NCY) * sizeof(T);
+};
+template <typename T, int TY>
+__global__ void __launch_bounds__(256) kt_pdvp_acc(const __grid_constant__ Maps maps, T *p_out, T *c_out, T *d1_out, T *e1_out, T *u_out,
+                                                   T *v_out, Mesh<T> m, int off, T dt, const double *dtp, T gm1, int p_fold, int acc_fold,
+                                                   int *err) {
+  using L = PdvAccLayout<T, TY>;
+  using B = typename L::B;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  T *sm = reinterpret_cast<T *>(smraw);
+  TileCtx cx = tile_ctx(&bar, err);
+  if (dtp) dt = (T)*dtp;
+  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
+  if (!stage(cx, sm, map_set(maps, 6), 6, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return;
+  const T *U0 = sm, *V0 = sm + B::BOXS, *D0 = sm + 2 * B::BOXS, *E0 = sm + 3 * B::BOXS, *P = sm + 4 * B::BOXS, *Q = sm + 5 * B::BOXS;
+  T *sp = sm + 6 * B::BOXS; // predicted pressure of ring cell (x0 - 1 + p, y0 - 1 + l) at sp[l * NCX + p]
+  const int pitch = (int)m.pitch;
+  const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
+  // (1) the predictor (src/serial/PdV.cpp:92-133) over the ring cells
+  Items<1, L::NCX, L::NCY>::each([&](int, int p, int l) {
+    const int i = x0 - 1 + p, j = y0 - 1 + l;
+    if (i > m.nx + 2 || j > m.ny + 2) return; // no node of the mesh reads it
+    const int ic = min(max(i, 2), m.nx + 1), jc = min(max(j, 2), m.ny + 1);
+    const int b = B::at(ic, jc, x0, y0);
+    const T cdx = m.celldx_t[ic], cdy = m.celldy_t[jc];
+    const T vol = cdx * cdy;
+    const T z = T(0);
+    T d1, e1;
+    pdv_value(true, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X], V0[b + BOX_X + 1],
+              z, z, z, z, z, z, z, z, D0[b], E0[b], P[b], Q[b], d1, e1);
+    sp[l * L::NCX + p] = gm1 * d1 * e1; // eos_value's pressure
+    if (l >= 1 && p >= 1 && i == ic && j == jc) { // one of the tile's own interior cells
+      T pp, cc;
+      eos_value(d1, e1, gm1, pp, cc);
+      const int g = gidx(pitch, i, j);
+      p_out[g] = pp;
+      c_out[g] = cc;
+      d1_out[g] = D0[b]; // the predictor's revert
+      e1_out[g] = E0[b];
+      if (p_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), p_fold, i, j, pp);
+    }
+  });
+  __syncthreads();
+  // (2) accelerate (src/serial/accelerate.cpp:28-56) of the tile's nodes
+  const int i = x0 + threadIdx.x;
+  if (i >= m.nx + 3) return;
+  const bool do_fold = acc_fold && near;
+  const T halfdt = T(0.5) * dt;
+  const T cdx = m.celldx_t[i], cdxm = m.celldx_t[i - 1];
+#pragma unroll
+  for (int r = 0; r < TY / 4; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
+    if (j >= m.ny + 3) break;
+    const int b = B::at(i, j, x0, y0);
+    const int s00 = (j - y0 + 1) * L::NCX + (i - x0 + 1);
+    const T cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
+    const T vol_mm = cdxm * cdym, vol_m0 = cdxm * cdy, vol_00 = cdx * cdy, vol_0m = cdx * cdym;
+    const int c00 = b, cm0 = b - 1, c0m = b - BOX_X, cmm = b - BOX_X - 1;
+    T u, v;
+    accel_value(halfdt, vol_mm, vol_m0, vol_00, vol_0m, cdy, cdym, cdx, cdxm, D0[cmm], D0[cm0], D0[c00], D0[c0m], sp[s00], sp[s00 - 1],
+                sp[s00 - L::NCX], sp[s00 - L::NCX - 1], Q[c00], Q[cm0], Q[c0m], Q[cmm], U0[c00], V0[c00], u, v);
+    const int g = gidx(pitch, i, j);
+    u_out[g] = u;
+    v_out[g] = v;
+    if (do_fold) {
+      fold_halo(u_out, m, halo_rule(XVEL1), acc_fold, i, j, u);
+      fold_halo(v_out, m, halo_rule(YVEL1), acc_fold, i, j, v);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // flux_calc: src/serial/flux_calc.cpp:27-43, faces [2, nx+2] x [2, ny+2].
 // With a fold, the extra row of x faces and column of y faces (overwritten
 // by update_halo) take their halo values.
