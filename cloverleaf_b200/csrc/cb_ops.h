@@ -44,10 +44,10 @@ template <typename T> struct Ops {
   // fused passes of the resident loop: viscosity + calc_dt, PdV corrector + flux_calc
   static cudaError_t visc_dt(Chunk &c, const DtConsts &k, int fold);
   static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold); // ideal_gas too
-  static cudaError_t pdv_flux(Chunk &c, double dt, int fold, int flux_fold);
-  // the PdV predictor (with its ideal_gas, pressure halo and revert) and
-  // accelerate in one pass; the predicted pressure goes to p_out
-  static cudaError_t pdvp_accelerate(Chunk &c, void *p_out, int p_fold, int acc_fold);
+  // the PdV predictor, accelerate, the PdV corrector and flux_calc in one
+  // pass, every output folded (depths above zero); the predicted pressure
+  // goes to p_out
+  static cudaError_t lagrange(Chunk &c, void *p_out, int p_fold, int acc_fold, int pdv_fold, int flux_fold);
 };
 
 extern template struct Ops<double>;

@@ -282,32 +282,19 @@ template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k
   return launched(c);
 }
 
-template <typename T> cudaError_t Ops<T>::pdv_flux(Chunk &c, double dt, int fold, int flux_fold) {
-  constexpr int TY = PDV_TY;
-  using B = Box1<T, TY>;
-  const size_t smem = 4 * B::BOXS * sizeof(T);
-  cudaError_t e = allow_smem(kt_pdv_flux<T>, smem);
+template <typename T> cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, int p_fold, int acc_fold, int pdv_fold, int flux_fold) {
+  if (p_fold <= 0 || acc_fold <= 0 || pdv_fold <= 0 || flux_fold <= 0) return cudaErrorInvalidValue;
+  constexpr int TY = 8;
+  using L = LagLayout<T, TY>;
+  cudaError_t e = allow_smem(kt_lagrange<T, TY>, L::SMEM);
   if (e != cudaSuccess) return e;
-  // the faces reach one column and one row past the cells
+  // the nodes and faces reach one column and one row past the cells
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  PdvIn in{c.base(DENSITY0), c.base(ENERGY0), c.base(PRESSURE), c.base(VISCOSITY)};
-  PdvOut out{c.base(DENSITY1), c.base(ENERGY1), c.base(PRESSURE), c.base(SOUNDSPEED)};
-  Maps mp = maps_of<B::BH>(c, {XVEL0, YVEL0, XVEL1, YVEL1});
-  kt_pdv_flux<T><<<g, dim3(64, 4), smem, c.stream>>>(mp, in, out, (T *)c.base(VOL_FLUX_X), (T *)c.base(VOL_FLUX_Y), mesh<T>(c), (int)c.off,
-                                                     (T)dt, c.dt_dev, fold, flux_fold, c.d_err);
-  return launched(c);
-}
-
-template <typename T> cudaError_t Ops<T>::pdvp_accelerate(Chunk &c, void *p_out, int p_fold, int acc_fold) {
-  constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 16;
-  using L = PdvAccLayout<T, TY>;
-  cudaError_t e = allow_smem(kt_pdvp_acc<T, TY>, L::SMEM);
-  if (e != cudaSuccess) return e;
-  dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
-  kt_pdvp_acc<T, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(
-      maps_of<L::B::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, PRESSURE, VISCOSITY}), (T *)p_out, (T *)c.base(SOUNDSPEED),
-      (T *)c.base(DENSITY1), (T *)c.base(ENERGY1), (T *)c.base(XVEL1), (T *)c.base(YVEL1), mesh<T>(c), (int)c.off, T(0), c.dt_dev,
-      gm1<T>(c), p_fold, acc_fold, c.d_err);
+  const LagOut<T> out{(T *)p_out, (T *)c.base(SOUNDSPEED), (T *)c.base(XVEL1), (T *)c.base(YVEL1), (T *)c.base(DENSITY1),
+                      (T *)c.base(ENERGY1), (T *)c.base(VOL_FLUX_X), (T *)c.base(VOL_FLUX_Y)};
+  kt_lagrange<T, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, PRESSURE, VISCOSITY}), out,
+                                                            mesh<T>(c), (int)c.off, T(0), c.dt_dev, gm1<T>(c),
+                                                            LagFolds{p_fold, acc_fold, pdv_fold, flux_fold}, c.d_err);
   return launched(c);
 }
 

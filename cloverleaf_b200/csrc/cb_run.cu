@@ -159,9 +159,9 @@ template <typename T> struct Seq {
   std::vector<Pass> passes;
   cudaError_t err = cudaSuccess;
   // fused emission (only with every producer folding): ideal_gas +
-  // viscosity + calc_dt in one pass, the PdV predictor + accelerate in one
-  // pass, the PdV corrector + flux_calc in one pass, and reset_field done by
-  // the second sweeps; the freshness moves exactly as unfused
+  // viscosity + calc_dt in one pass, the PdV predictor + accelerate + the
+  // PdV corrector + flux_calc in one pass, and reset_field done by the
+  // second sweeps; the freshness moves exactly as unfused
   bool fuse = false;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
@@ -218,9 +218,11 @@ template <typename T> struct Seq {
   void lagrange() {
     const int fp = eff(1); // the predictor makes its own pressure halo
     const int fa = eff(dep(2));
+    const int fc = eff(dep(2));
+    const int ff = eff(dep(2));
     if (fuse) {
-      // fused: the predictor and accelerate in one pass
-      if (emit) run(Ops<T>::pdvp_accelerate(c, c.spare_base(4), fp, fa));
+      // fused: the whole Lagrangian step in one pass
+      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), fp, fa, fc, ff));
       swap_pressure();
     } else if (emit) {
       run(Ops<T>::pdv(c, 1, 0.0, 1, fp));
@@ -235,9 +237,7 @@ template <typename T> struct Seq {
     wrote({SS, D1, E1}, 0);
     if (emit && !fuse) run(Ops<T>::accelerate(c, 0.0, fa));
     wrote({U1, V1}, fa);
-    const int fc = eff(dep(2));
-    const int ff = eff(dep(2));
-    if (emit) run(fuse ? Ops<T>::pdv_flux(c, 0.0, fc, ff) : Ops<T>::pdv(c, 0, 0.0, 0, fc));
+    if (emit && !fuse) run(Ops<T>::pdv(c, 0, 0.0, 0, fc));
     wrote({D1, E1}, fc);
     if (emit && !fuse) run(Ops<T>::flux_calc(c, 0.0, ff));
     wrote({VFX, VFY}, ff);

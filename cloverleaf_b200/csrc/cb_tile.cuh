@@ -620,14 +620,9 @@ struct PdvOut {
 constexpr int PDV_TY = 8;
 template <typename T> constexpr size_t pdv_smem() { return 4 * Box1<T, PDV_TY>::BOXS * sizeof(T); }
 
-// FLUX: the corrector (mode 0) also does flux_calc (src/serial/flux_calc.cpp:27-43)
-// from the same staged velocities -- faces [2, nx+2] x [2, ny+2], so the grid
-// covers one more column and row than the cells -- with fold depth
-// flux_fold, as flux_calc_tile writes them.
-template <typename T, bool FLUX = false>
+template <typename T>
 __device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, const PdvIn &in, const PdvOut &out, const Mesh<T> &m, int off,
-                                         int predict, T dt, int mode, T gm1, int fold, int bx, int by, T *fx_out = nullptr,
-                                         T *fy_out = nullptr, int flux_fold = 0) {
+                                         int predict, T dt, int mode, T gm1, int fold, int bx, int by) {
   constexpr int TY = PDV_TY;
   using B = Box1<T, TY>;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
@@ -649,61 +644,40 @@ __device__ __forceinline__ bool pdv_tile(TileCtx &cx, T *sm, const MapSet &ms, c
   const int nf = predict ? 2 : 4;
   if (!stage(cx, sm, ms, nf, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
   const T *U0 = sm, *V0 = sm + B::BOXS, *U1 = sm + 2 * B::BOXS, *V1 = sm + 3 * B::BOXS;
-  if (i >= m.nx + (FLUX ? 3 : 2)) return true;
-  const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
-  const bool do_fold = fold && near;
+  if (i >= m.nx + 2) return true;
+  const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const T cdx = m.celldx_t[i];
 #pragma unroll
   for (int r = 0; r < RPT; ++r) {
     const int j = y0 + threadIdx.y + 4 * r;
-    if (j >= m.ny + (FLUX ? 3 : 2)) break;
+    if (j >= m.ny + 2) break;
     const int b = B::at(i, j, x0, y0);
     const int g = gidx(pitch, i, j);
-    if (!FLUX || (i < m.nx + 2 && j < m.ny + 2)) {
-      const T cdy = m.celldy_t[j];
-      const T vol = cdx * cdy;
-      T w00 = T(0), w01 = T(0), w10 = T(0), w11 = T(0), z00 = T(0), z10 = T(0), z01 = T(0), z11 = T(0);
-      if (!predict) {
-        w00 = U1[b], w01 = U1[b + BOX_X], w10 = U1[b + 1], w11 = U1[b + BOX_X + 1];
-        z00 = V1[b], z10 = V1[b + 1], z01 = V1[b + BOX_X], z11 = V1[b + BOX_X + 1];
-      }
-      T d1, e1;
-      pdv_value(predict != 0, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
-                V0[b + BOX_X + 1], w00, w01, w10, w11, z00, z10, z01, z11, rd[r], re[r], rp[r], rq[r], d1, e1);
-      if (mode == 0) {
-        ((T *)out.density1)[g] = d1;
-        ((T *)out.energy1)[g] = e1;
-        if (do_fold) {
-          fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, d1);
-          fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, e1);
-        }
-      } else {
-        T p, c;
-        eos_value(d1, e1, gm1, p, c);
-        ((T *)out.pressure)[g] = p;
-        ((T *)out.soundspeed)[g] = c;
-        if (do_fold) fold_halo((T *)out.pressure, m, halo_rule(PRESSURE), fold, i, j, p);
-        ((T *)out.density1)[g] = rd[r];
-        ((T *)out.energy1)[g] = re[r];
-      }
+    const T cdy = m.celldy_t[j];
+    const T vol = cdx * cdy;
+    T w00 = T(0), w01 = T(0), w10 = T(0), w11 = T(0), z00 = T(0), z10 = T(0), z01 = T(0), z11 = T(0);
+    if (!predict) {
+      w00 = U1[b], w01 = U1[b + BOX_X], w10 = U1[b + 1], w11 = U1[b + BOX_X + 1];
+      z00 = V1[b], z10 = V1[b + 1], z01 = V1[b + BOX_X], z11 = V1[b + BOX_X + 1];
     }
-    if constexpr (FLUX) {
-      // flux_calc_tile's face values and writes
-      const T fx = flux_value(dt, m.celldy_t[j], U0[b], U0[b + BOX_X], U1[b], U1[b + BOX_X]);
-      const T fy = flux_value(dt, cdx, V0[b], V0[b + 1], V1[b], V1[b + 1]);
-      if (!flux_fold) {
-        fx_out[g] = fx;
-        fy_out[g] = fy;
-        continue;
+    T d1, e1;
+    pdv_value(predict != 0, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
+              V0[b + BOX_X + 1], w00, w01, w10, w11, z00, z10, z01, z11, rd[r], re[r], rp[r], rq[r], d1, e1);
+    if (mode == 0) {
+      ((T *)out.density1)[g] = d1;
+      ((T *)out.energy1)[g] = e1;
+      if (do_fold) {
+        fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, d1);
+        fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, e1);
       }
-      if (j < m.ny + 2) {
-        fx_out[g] = fx;
-        if (near) fold_halo(fx_out, m, halo_rule(VOL_FLUX_X), flux_fold, i, j, fx);
-      }
-      if (i < m.nx + 2) {
-        fy_out[g] = fy;
-        if (near) fold_halo(fy_out, m, halo_rule(VOL_FLUX_Y), flux_fold, i, j, fy);
-      }
+    } else {
+      T p, c;
+      eos_value(d1, e1, gm1, p, c);
+      ((T *)out.pressure)[g] = p;
+      ((T *)out.soundspeed)[g] = c;
+      if (do_fold) fold_halo((T *)out.pressure, m, halo_rule(PRESSURE), fold, i, j, p);
+      ((T *)out.density1)[g] = rd[r];
+      ((T *)out.energy1)[g] = re[r];
     }
   }
   return true;
@@ -731,17 +705,6 @@ template <typename T>
 __global__ void __launch_bounds__(256, 4) kt_pdv4(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, Mesh<T> m, int off, int predict,
                                                   T dt, const double *dtp, int mode, T gm1, int fold, int *err) {
   pdv_kernel<T>(maps, in, out, m, off, predict, dt, dtp, mode, gm1, fold, err);
-}
-
-// The PdV corrector and flux_calc in one pass (the resident loop).
-template <typename T>
-__global__ void __launch_bounds__(256) kt_pdv_flux(const __grid_constant__ Maps maps, PdvIn in, PdvOut out, T *fx_out, T *fy_out, Mesh<T> m,
-                                                   int off, T dt, const double *dtp, int fold, int flux_fold, int *err) {
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  TileCtx cx = tile_ctx(&bar, err);
-  pdv_tile<T, true>(cx, reinterpret_cast<T *>(smraw), map_set(maps, 4), in, out, m, off, 0, dtp ? (T)*dtp : dt, 0, T(0), fold, blockIdx.x,
-                    blockIdx.y, fx_out, fy_out, flux_fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -833,90 +796,146 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 }
 
 // ---------------------------------------------------------------------------
-// The PdV predictor and accelerate in one pass (the resident loop).  A tile
-// of accelerate's nodes reads the predicted pressure of the cells around
-// them, a ring one cell wider than the tile's own cells on their low sides:
-// the tile evaluates the predictor there as pdv_tile mode 1 does -- a halo
-// cell through its mirror interior cell (its index clamped: the depth-1
-// reflection that the predictor's fold writes) -- keeps the pressures in
-// shared memory, writes the predictor's outputs for its own cells, then
-// accelerates its nodes.  The predicted pressure goes to p_out, a buffer
+// The Lagrangian step in one pass (the resident loop): the PdV predictor with
+// its ideal_gas and pressure halo, accelerate, the PdV corrector and
+// flux_calc (src/serial/PdV.cpp:36-133, accelerate.cpp:28-56,
+// flux_calc.cpp:27-43).  A tile of 64 x TY cells needs the level-1
+// velocities of the nodes around its cells, one node wider than the tile's
+// own nodes on their high sides, and those need the predicted pressure of a
+// ring one cell wider still on every side: the tile evaluates both rings
+// itself (a halo cell through its mirror interior cell, the depth-1
+// reflection that the predictor's fold writes), keeps them in shared memory
+// and writes the outputs of its own cells, nodes and faces.  The predictor's
+// revert is not written: the corrector overwrites density1 and energy1 in
+// every interior cell.  Every output is folded (fold depths above zero: the
+// halo faces are the fold's).  The predicted pressure goes to out.pressure, a buffer
 // other than the pressure's current one, because other tiles still read the
 // old pressure of their ring cells; the caller swaps the two.
-// Staged (Box1): 0 xvel0, 1 yvel0, 2 density0, 3 energy0, 4 pressure, 5 viscosity.
-template <typename T, int TY> struct PdvAccLayout {
-  using B = Box1<T, TY>;
-  static constexpr int NCX = TILE_X + 1, NCY = TY + 1; // ring cells along x and y
-  static constexpr size_t SMEM = (size_t)(6 * B::BOXS + NCX * NCY) * sizeof(T);
+// Staged: 0 xvel0, 1 yvel0, 2 density0, 3 energy0, 4 pressure, 5 viscosity,
+// rows y0 - 1 .. y0 + TY + 2.
+template <typename T, int TY> struct LagLayout {
+  static constexpr int BH = TY + 4;
+  static constexpr int BOXS = (BOX_X * BH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+  static constexpr int PCX = TILE_X + 2, PCY = TY + 2; // predicted pressure: cells x0 - 1 + p, y0 - 1 + l
+  static constexpr int NNX = TILE_X + 1, NNY = TY + 1; // level-1 velocities: nodes x0 + p, y0 + l
+  static constexpr size_t SMEM = (size_t)(6 * BOXS + PCX * PCY + 2 * NNX * NNY) * sizeof(T);
+  __device__ static constexpr int at(int i, int j, int x0, int y0) { return (j - y0 + 1) * BOX_X + (i - x0 + HALO); }
 };
+
+template <typename T> struct LagOut {
+  T *pressure, *soundspeed, *xvel1, *yvel1, *density1, *energy1, *vol_flux_x, *vol_flux_y;
+};
+struct LagFolds {
+  int pressure, accelerate, pdv, flux;
+};
+
 template <typename T, int TY>
-__global__ void __launch_bounds__(256) kt_pdvp_acc(const __grid_constant__ Maps maps, T *p_out, T *c_out, T *d1_out, T *e1_out, T *u_out,
-                                                   T *v_out, Mesh<T> m, int off, T dt, const double *dtp, T gm1, int p_fold, int acc_fold,
-                                                   int *err) {
-  using L = PdvAccLayout<T, TY>;
-  using B = typename L::B;
+__device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> &out, const Mesh<T> &m, int off, T dt, T gm1,
+                                              const LagFolds &fd, int *err) {
+  using L = LagLayout<T, TY>;
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
   T *sm = reinterpret_cast<T *>(smraw);
   TileCtx cx = tile_ctx(&bar, err);
-  if (dtp) dt = (T)*dtp;
   const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  if (!stage(cx, sm, map_set(maps, 6), 6, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return;
-  const T *U0 = sm, *V0 = sm + B::BOXS, *D0 = sm + 2 * B::BOXS, *E0 = sm + 3 * B::BOXS, *P = sm + 4 * B::BOXS, *Q = sm + 5 * B::BOXS;
-  T *sp = sm + 6 * B::BOXS; // predicted pressure of ring cell (x0 - 1 + p, y0 - 1 + l) at sp[l * NCX + p]
+  if (!stage(cx, sm, map_set(maps, 6), 6, L::BOXS, L::BH, off + x0 - HALO, y0 - 1)) return;
+  const T *U0 = sm, *V0 = sm + L::BOXS, *D0 = sm + 2 * L::BOXS, *E0 = sm + 3 * L::BOXS, *P = sm + 4 * L::BOXS, *Q = sm + 5 * L::BOXS;
+  T *sp = sm + 6 * L::BOXS, *su = sp + L::PCX * L::PCY, *sv = su + L::NNX * L::NNY;
   const int pitch = (int)m.pitch;
   const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
-  // (1) the predictor (src/serial/PdV.cpp:92-133) over the ring cells
-  Items<1, L::NCX, L::NCY>::each([&](int, int p, int l) {
+  // (1) the predictor over the pressure ring
+  Items<1, L::PCX, L::PCY>::each([&](int, int p, int l) {
     const int i = x0 - 1 + p, j = y0 - 1 + l;
     if (i > m.nx + 2 || j > m.ny + 2) return; // no node of the mesh reads it
     const int ic = min(max(i, 2), m.nx + 1), jc = min(max(j, 2), m.ny + 1);
-    const int b = B::at(ic, jc, x0, y0);
+    const int b = L::at(ic, jc, x0, y0);
     const T cdx = m.celldx_t[ic], cdy = m.celldy_t[jc];
     const T vol = cdx * cdy;
     const T z = T(0);
     T d1, e1;
     pdv_value(true, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X], V0[b + BOX_X + 1],
               z, z, z, z, z, z, z, z, D0[b], E0[b], P[b], Q[b], d1, e1);
-    sp[l * L::NCX + p] = gm1 * d1 * e1; // eos_value's pressure
-    if (l >= 1 && p >= 1 && i == ic && j == jc) { // one of the tile's own interior cells
+    sp[l * L::PCX + p] = gm1 * d1 * e1; // eos_value's pressure
+    if (p >= 1 && p <= TILE_X && l >= 1 && l <= TY && i == ic && j == jc) { // one of the tile's own interior cells
       T pp, cc;
       eos_value(d1, e1, gm1, pp, cc);
       const int g = gidx(pitch, i, j);
-      p_out[g] = pp;
-      c_out[g] = cc;
-      d1_out[g] = D0[b]; // the predictor's revert
-      e1_out[g] = E0[b];
-      if (p_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), p_fold, i, j, pp);
+      out.pressure[g] = pp;
+      out.soundspeed[g] = cc;
+      if (fd.pressure && near) fold_halo(out.pressure, m, halo_rule(PRESSURE), fd.pressure, i, j, pp);
     }
   });
   __syncthreads();
-  // (2) accelerate (src/serial/accelerate.cpp:28-56) of the tile's nodes
-  const int i = x0 + threadIdx.x;
-  if (i >= m.nx + 3) return;
-  const bool do_fold = acc_fold && near;
+  // (2) accelerate over the nodes [x0, x0 + 64] x [y0, y0 + TY]
   const T halfdt = T(0.5) * dt;
-  const T cdx = m.celldx_t[i], cdxm = m.celldx_t[i - 1];
-#pragma unroll
-  for (int r = 0; r < TY / 4; ++r) {
-    const int j = y0 + threadIdx.y + 4 * r;
-    if (j >= m.ny + 3) break;
-    const int b = B::at(i, j, x0, y0);
-    const int s00 = (j - y0 + 1) * L::NCX + (i - x0 + 1);
-    const T cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
+  Items<1, L::NNX, L::NNY>::each([&](int, int p, int l) {
+    const int i = x0 + p, j = y0 + l;
+    if (i > m.nx + 2 || j > m.ny + 2) return;
+    const int b = L::at(i, j, x0, y0);
+    const int s00 = (l + 1) * L::PCX + (p + 1);
+    const T cdx = m.celldx_t[i], cdxm = m.celldx_t[i - 1], cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
     const T vol_mm = cdxm * cdym, vol_m0 = cdxm * cdy, vol_00 = cdx * cdy, vol_0m = cdx * cdym;
     const int c00 = b, cm0 = b - 1, c0m = b - BOX_X, cmm = b - BOX_X - 1;
     T u, v;
     accel_value(halfdt, vol_mm, vol_m0, vol_00, vol_0m, cdy, cdym, cdx, cdxm, D0[cmm], D0[cm0], D0[c00], D0[c0m], sp[s00], sp[s00 - 1],
-                sp[s00 - L::NCX], sp[s00 - L::NCX - 1], Q[c00], Q[cm0], Q[c0m], Q[cmm], U0[c00], V0[c00], u, v);
+                sp[s00 - L::PCX], sp[s00 - L::PCX - 1], Q[c00], Q[cm0], Q[c0m], Q[cmm], U0[c00], V0[c00], u, v);
+    su[l * L::NNX + p] = u;
+    sv[l * L::NNX + p] = v;
+    if (p < TILE_X && l < TY) { // one of the tile's own nodes
+      const int g = gidx(pitch, i, j);
+      out.xvel1[g] = u;
+      out.yvel1[g] = v;
+      if (fd.accelerate && near) {
+        fold_halo(out.xvel1, m, halo_rule(XVEL1), fd.accelerate, i, j, u);
+        fold_halo(out.yvel1, m, halo_rule(YVEL1), fd.accelerate, i, j, v);
+      }
+    }
+  });
+  __syncthreads();
+  // (3) the corrector over the tile's cells and flux_calc over its faces
+  const int i = x0 + threadIdx.x;
+  if (i >= m.nx + 3) return;
+  const T cdx = m.celldx_t[i];
+#pragma unroll
+  for (int r = 0; r < TY / 4; ++r) {
+    const int j = y0 + threadIdx.y + 4 * r;
+    if (j >= m.ny + 3) break;
+    const int b = L::at(i, j, x0, y0);
+    const int n = (j - y0) * L::NNX + (i - x0);
     const int g = gidx(pitch, i, j);
-    u_out[g] = u;
-    v_out[g] = v;
-    if (do_fold) {
-      fold_halo(u_out, m, halo_rule(XVEL1), acc_fold, i, j, u);
-      fold_halo(v_out, m, halo_rule(YVEL1), acc_fold, i, j, v);
+    if (i < m.nx + 2 && j < m.ny + 2) {
+      const T cdy = m.celldy_t[j];
+      const T vol = cdx * cdy;
+      T d1, e1;
+      pdv_value(false, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
+                V0[b + BOX_X + 1], su[n], su[n + L::NNX], su[n + 1], su[n + L::NNX + 1], sv[n], sv[n + 1], sv[n + L::NNX],
+                sv[n + L::NNX + 1], D0[b], E0[b], sp[(j - y0 + 1) * L::PCX + (i - x0 + 1)], Q[b], d1, e1);
+      out.density1[g] = d1;
+      out.energy1[g] = e1;
+      if (fd.pdv && near) {
+        fold_halo(out.density1, m, halo_rule(DENSITY1), fd.pdv, i, j, d1);
+        fold_halo(out.energy1, m, halo_rule(ENERGY1), fd.pdv, i, j, e1);
+      }
+    }
+    // flux_calc_tile's face values and folded writes: x faces below row
+    // ny + 2, y faces left of column nx + 2 (the fold writes the rest)
+    if (j < m.ny + 2) {
+      const T fx = flux_value(dt, m.celldy_t[j], U0[b], U0[b + BOX_X], su[n], su[n + L::NNX]);
+      out.vol_flux_x[g] = fx;
+      if (near) fold_halo(out.vol_flux_x, m, halo_rule(VOL_FLUX_X), fd.flux, i, j, fx);
+    }
+    if (i < m.nx + 2) {
+      const T fy = flux_value(dt, cdx, V0[b], V0[b + 1], sv[n], sv[n + 1]);
+      out.vol_flux_y[g] = fy;
+      if (near) fold_halo(out.vol_flux_y, m, halo_rule(VOL_FLUX_Y), fd.flux, i, j, fy);
     }
   }
+}
+
+template <typename T, int TY>
+__global__ void __launch_bounds__(256) kt_lagrange(const __grid_constant__ Maps maps, LagOut<T> out, Mesh<T> m, int off, T dt,
+                                                   const double *dtp, T gm1, LagFolds fd, int *err) {
+  lagrange_tile<T, TY>(maps, out, m, off, dtp ? (T)*dtp : dt, gm1, fd, err);
 }
 
 // ---------------------------------------------------------------------------

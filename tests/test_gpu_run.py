@@ -9,8 +9,8 @@ the run ends on its time or on its step count, when the loop is split into
 several graphs, and when the graph takes over a run the host started.
 
 With fuse = 1 the graph runs ideal_gas and viscosity with calc_dt, the PdV
-predictor with accelerate, the PdV corrector with flux_calc and reset_field
-inside the second sweeps: FP64 stays bit-identical;
+predictor, accelerate, the PdV corrector and flux_calc as one pass and
+reset_field inside the second sweeps: FP64 stays bit-identical;
 FP32 is compared within 1e-5 (relative to each field's largest magnitude),
 because the fused kernels may contract single-precision products and sums
 differently.
@@ -201,7 +201,8 @@ def test_run_fused_falls_back(nx, ny, fold):
 
 
 def test_run_fused_launch_count():
-    """Fused, a step launches five kernels fewer (ideal_gas, viscosity, accelerate, flux_calc and reset_field run inside others)."""
+    """Fused, a step launches six kernels fewer: ideal_gas, viscosity, accelerate, the PdV corrector, flux_calc and
+    reset_field run inside others."""
     dk = deck_a(48, 48, end_step=12, freq=5)
     counts = []
     for fuse in (False, True):
@@ -211,4 +212,4 @@ def test_run_fused_launch_count():
         n0 = c.launch_count()
         r.run_steps_on_device(fuse=fuse)
         counts.append(c.launch_count() - n0)
-    assert counts[1] == counts[0] - 5 * 12
+    assert counts[1] == counts[0] - 6 * 12
