@@ -284,7 +284,7 @@ template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k
 
 template <typename T> cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, int p_fold, int acc_fold, int pdv_fold, int flux_fold) {
   if (p_fold <= 0 || acc_fold <= 0 || pdv_fold <= 0 || flux_fold <= 0) return cudaErrorInvalidValue;
-  constexpr int TY = 8;
+  constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 12;
   using L = LagLayout<T, TY>;
   cudaError_t e = allow_smem(kt_lagrange<T, TY>, L::SMEM);
   if (e != cudaSuccess) return e;

@@ -818,9 +818,22 @@ template <typename T, int TY> struct LagLayout {
   static constexpr int BOXS = (BOX_X * BH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
   static constexpr int PCX = TILE_X + 2, PCY = TY + 2; // predicted pressure: cells x0 - 1 + p, y0 - 1 + l
   static constexpr int NNX = TILE_X + 1, NNY = TY + 1; // level-1 velocities: nodes x0 + p, y0 + l
-  static constexpr size_t SMEM = (size_t)(6 * BOXS + PCX * PCY + 2 * NNX * NNY) * sizeof(T);
+  // + celldx of the box's columns and celldy of its rows (fill_widths)
+  static constexpr size_t SMEM = (size_t)(6 * BOXS + PCX * PCY + 2 * NNX * NNY + BOX_X + BH) * sizeof(T);
   __device__ static constexpr int at(int i, int j, int x0, int y0) { return (j - y0 + 1) * BOX_X + (i - x0 + HALO); }
 };
+
+// The items (p, l), p < NA, l < NB, of a ring stage, spread evenly over the
+// block's 256 threads (item t = tid + 256 k, row-major): as few rounds as
+// the item count allows.
+template <int NA, int NB, typename F> __device__ __forceinline__ void each_spread(F &&f) {
+  const int tid = threadIdx.y * 64 + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < (NA * NB + 255) / 256; ++k) {
+    const int t = tid + 256 * k;
+    if (t < NA * NB) f(t % NA, t / NA);
+  }
+}
 
 template <typename T> struct LagOut {
   T *pressure, *soundspeed, *xvel1, *yvel1, *density1, *energy1, *vol_flux_x, *vol_flux_y;
@@ -838,18 +851,20 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   T *sm = reinterpret_cast<T *>(smraw);
   TileCtx cx = tile_ctx(&bar, err);
   const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
-  if (!stage(cx, sm, map_set(maps, 6), 6, L::BOXS, L::BH, off + x0 - HALO, y0 - 1)) return;
   const T *U0 = sm, *V0 = sm + L::BOXS, *D0 = sm + 2 * L::BOXS, *E0 = sm + 3 * L::BOXS, *P = sm + 4 * L::BOXS, *Q = sm + 5 * L::BOXS;
-  T *sp = sm + 6 * L::BOXS, *su = sp + L::PCX * L::PCY, *sv = su + L::NNX * L::NNY;
+  T *sp = sm + 6 * L::BOXS, *su = sp + L::PCX * L::PCY, *sv = su + L::NNX * L::NNY, *gx = sv + L::NNX * L::NNY, *gy = gx + BOX_X;
+  stage_issue(cx, sm, map_set(maps, 6), 6, L::BOXS, L::BH, off + x0 - HALO, y0 - 1);
+  fill_widths(m, x0, y0, 1, L::BH, 1, gx, gy, nullptr, nullptr); // gx[i - x0 + HALO] = celldx[i], gy[j - y0 + 1] = celldy[j]
+  if (!stage_wait(cx)) return;
   const int pitch = (int)m.pitch;
   const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
   // (1) the predictor over the pressure ring
-  Items<1, L::PCX, L::PCY>::each([&](int, int p, int l) {
+  each_spread<L::PCX, L::PCY>([&](int p, int l) {
     const int i = x0 - 1 + p, j = y0 - 1 + l;
     if (i > m.nx + 2 || j > m.ny + 2) return; // no node of the mesh reads it
     const int ic = min(max(i, 2), m.nx + 1), jc = min(max(j, 2), m.ny + 1);
     const int b = L::at(ic, jc, x0, y0);
-    const T cdx = m.celldx_t[ic], cdy = m.celldy_t[jc];
+    const T cdx = gx[ic - x0 + HALO], cdy = gy[jc - y0 + 1];
     const T vol = cdx * cdy;
     const T z = T(0);
     T d1, e1;
@@ -868,12 +883,12 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   __syncthreads();
   // (2) accelerate over the nodes [x0, x0 + 64] x [y0, y0 + TY]
   const T halfdt = T(0.5) * dt;
-  Items<1, L::NNX, L::NNY>::each([&](int, int p, int l) {
+  each_spread<L::NNX, L::NNY>([&](int p, int l) {
     const int i = x0 + p, j = y0 + l;
     if (i > m.nx + 2 || j > m.ny + 2) return;
     const int b = L::at(i, j, x0, y0);
     const int s00 = (l + 1) * L::PCX + (p + 1);
-    const T cdx = m.celldx_t[i], cdxm = m.celldx_t[i - 1], cdy = m.celldy_t[j], cdym = m.celldy_t[j - 1];
+    const T cdx = gx[p + HALO], cdxm = gx[p + HALO - 1], cdy = gy[l + 1], cdym = gy[l];
     const T vol_mm = cdxm * cdym, vol_m0 = cdxm * cdy, vol_00 = cdx * cdy, vol_0m = cdx * cdym;
     const int c00 = b, cm0 = b - 1, c0m = b - BOX_X, cmm = b - BOX_X - 1;
     T u, v;
@@ -895,7 +910,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   // (3) the corrector over the tile's cells and flux_calc over its faces
   const int i = x0 + threadIdx.x;
   if (i >= m.nx + 3) return;
-  const T cdx = m.celldx_t[i];
+  const T cdx = gx[threadIdx.x + HALO];
 #pragma unroll
   for (int r = 0; r < TY / 4; ++r) {
     const int j = y0 + threadIdx.y + 4 * r;
@@ -903,8 +918,8 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
     const int b = L::at(i, j, x0, y0);
     const int n = (j - y0) * L::NNX + (i - x0);
     const int g = gidx(pitch, i, j);
+    const T cdy = gy[j - y0 + 1];
     if (i < m.nx + 2 && j < m.ny + 2) {
-      const T cdy = m.celldy_t[j];
       const T vol = cdx * cdy;
       T d1, e1;
       pdv_value(false, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
@@ -920,7 +935,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
     // flux_calc_tile's face values and folded writes: x faces below row
     // ny + 2, y faces left of column nx + 2 (the fold writes the rest)
     if (j < m.ny + 2) {
-      const T fx = flux_value(dt, m.celldy_t[j], U0[b], U0[b + BOX_X], su[n], su[n + L::NNX]);
+      const T fx = flux_value(dt, cdy, U0[b], U0[b + BOX_X], su[n], su[n + L::NNX]);
       out.vol_flux_x[g] = fx;
       if (near) fold_halo(out.vol_flux_x, m, halo_rule(VOL_FLUX_X), fd.flux, i, j, fx);
     }
