@@ -842,7 +842,9 @@ struct LagFolds {
   int pressure, accelerate, pdv, flux;
 };
 
-template <typename T, int TY>
+// EDGE: a tile within reach of the mesh edge (edge_tile); the others are
+// compiled without extent checks, clamps and halo folds.
+template <typename T, int TY, bool EDGE>
 __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> &out, const Mesh<T> &m, int off, T dt, T gm1,
                                               const LagFolds &fd, int *err) {
   using L = LagLayout<T, TY>;
@@ -857,12 +859,11 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   fill_widths(m, x0, y0, 1, L::BH, 1, gx, gy, nullptr, nullptr); // gx[i - x0 + HALO] = celldx[i], gy[j - y0 + 1] = celldy[j]
   if (!stage_wait(cx)) return;
   const int pitch = (int)m.pitch;
-  const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
   // (1) the predictor over the pressure ring
   each_spread<L::PCX, L::PCY>([&](int p, int l) {
     const int i = x0 - 1 + p, j = y0 - 1 + l;
-    if (i > m.nx + 2 || j > m.ny + 2) return; // no node of the mesh reads it
-    const int ic = min(max(i, 2), m.nx + 1), jc = min(max(j, 2), m.ny + 1);
+    if (EDGE && (i > m.nx + 2 || j > m.ny + 2)) return; // no node of the mesh reads it
+    const int ic = EDGE ? min(max(i, 2), m.nx + 1) : i, jc = EDGE ? min(max(j, 2), m.ny + 1) : j;
     const int b = L::at(ic, jc, x0, y0);
     const T cdx = gx[ic - x0 + HALO], cdy = gy[jc - y0 + 1];
     const T vol = cdx * cdy;
@@ -871,13 +872,13 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
     pdv_value(true, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X], V0[b + BOX_X + 1],
               z, z, z, z, z, z, z, z, D0[b], E0[b], P[b], Q[b], d1, e1);
     sp[l * L::PCX + p] = gm1 * d1 * e1; // eos_value's pressure
-    if (p >= 1 && p <= TILE_X && l >= 1 && l <= TY && i == ic && j == jc) { // one of the tile's own interior cells
+    if (p >= 1 && p <= TILE_X && l >= 1 && l <= TY && (!EDGE || (i == ic && j == jc))) { // one of the tile's own interior cells
       T pp, cc;
       eos_value(d1, e1, gm1, pp, cc);
       const int g = gidx(pitch, i, j);
       out.pressure[g] = pp;
       out.soundspeed[g] = cc;
-      if (fd.pressure && near) fold_halo(out.pressure, m, halo_rule(PRESSURE), fd.pressure, i, j, pp);
+      if (EDGE && fd.pressure) fold_halo(out.pressure, m, halo_rule(PRESSURE), fd.pressure, i, j, pp);
     }
   });
   __syncthreads();
@@ -885,7 +886,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   const T halfdt = T(0.5) * dt;
   each_spread<L::NNX, L::NNY>([&](int p, int l) {
     const int i = x0 + p, j = y0 + l;
-    if (i > m.nx + 2 || j > m.ny + 2) return;
+    if (EDGE && (i > m.nx + 2 || j > m.ny + 2)) return;
     const int b = L::at(i, j, x0, y0);
     const int s00 = (l + 1) * L::PCX + (p + 1);
     const T cdx = gx[p + HALO], cdxm = gx[p + HALO - 1], cdy = gy[l + 1], cdym = gy[l];
@@ -900,7 +901,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
       const int g = gidx(pitch, i, j);
       out.xvel1[g] = u;
       out.yvel1[g] = v;
-      if (fd.accelerate && near) {
+      if (EDGE && fd.accelerate) {
         fold_halo(out.xvel1, m, halo_rule(XVEL1), fd.accelerate, i, j, u);
         fold_halo(out.yvel1, m, halo_rule(YVEL1), fd.accelerate, i, j, v);
       }
@@ -909,17 +910,17 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   __syncthreads();
   // (3) the corrector over the tile's cells and flux_calc over its faces
   const int i = x0 + threadIdx.x;
-  if (i >= m.nx + 3) return;
+  if (EDGE && i >= m.nx + 3) return;
   const T cdx = gx[threadIdx.x + HALO];
 #pragma unroll
   for (int r = 0; r < TY / 4; ++r) {
     const int j = y0 + threadIdx.y + 4 * r;
-    if (j >= m.ny + 3) break;
+    if (EDGE && j >= m.ny + 3) break;
     const int b = L::at(i, j, x0, y0);
     const int n = (j - y0) * L::NNX + (i - x0);
     const int g = gidx(pitch, i, j);
     const T cdy = gy[j - y0 + 1];
-    if (i < m.nx + 2 && j < m.ny + 2) {
+    if (!EDGE || (i < m.nx + 2 && j < m.ny + 2)) {
       const T vol = cdx * cdy;
       T d1, e1;
       pdv_value(false, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X],
@@ -927,22 +928,22 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
                 sv[n + L::NNX + 1], D0[b], E0[b], sp[(j - y0 + 1) * L::PCX + (i - x0 + 1)], Q[b], d1, e1);
       out.density1[g] = d1;
       out.energy1[g] = e1;
-      if (fd.pdv && near) {
+      if (EDGE && fd.pdv) {
         fold_halo(out.density1, m, halo_rule(DENSITY1), fd.pdv, i, j, d1);
         fold_halo(out.energy1, m, halo_rule(ENERGY1), fd.pdv, i, j, e1);
       }
     }
     // flux_calc_tile's face values and folded writes: x faces below row
     // ny + 2, y faces left of column nx + 2 (the fold writes the rest)
-    if (j < m.ny + 2) {
+    if (!EDGE || j < m.ny + 2) {
       const T fx = flux_value(dt, cdy, U0[b], U0[b + BOX_X], su[n], su[n + L::NNX]);
       out.vol_flux_x[g] = fx;
-      if (near) fold_halo(out.vol_flux_x, m, halo_rule(VOL_FLUX_X), fd.flux, i, j, fx);
+      if (EDGE) fold_halo(out.vol_flux_x, m, halo_rule(VOL_FLUX_X), fd.flux, i, j, fx);
     }
-    if (i < m.nx + 2) {
+    if (!EDGE || i < m.nx + 2) {
       const T fy = flux_value(dt, cdx, V0[b], V0[b + 1], sv[n], sv[n + 1]);
       out.vol_flux_y[g] = fy;
-      if (near) fold_halo(out.vol_flux_y, m, halo_rule(VOL_FLUX_Y), fd.flux, i, j, fy);
+      if (EDGE) fold_halo(out.vol_flux_y, m, halo_rule(VOL_FLUX_Y), fd.flux, i, j, fy);
     }
   }
 }
@@ -950,7 +951,11 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
 template <typename T, int TY>
 __global__ void __launch_bounds__(256) kt_lagrange(const __grid_constant__ Maps maps, LagOut<T> out, Mesh<T> m, int off, T dt,
                                                    const double *dtp, T gm1, LagFolds fd, int *err) {
-  lagrange_tile<T, TY>(maps, out, m, off, dtp ? (T)*dtp : dt, gm1, fd, err);
+  const T d = dtp ? (T)*dtp : dt;
+  if (edge_tile(m.nx, m.ny, 2 + blockIdx.x * TILE_X, 2 + blockIdx.y * TY, TY))
+    lagrange_tile<T, TY, true>(maps, out, m, off, d, gm1, fd, err);
+  else
+    lagrange_tile<T, TY, false>(maps, out, m, off, d, gm1, fd, err);
 }
 
 // ---------------------------------------------------------------------------
