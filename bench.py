@@ -8,13 +8,15 @@ gamma 1.4, reflective) on a 7680x7680 mesh.  One "step" is one hydro
 timestep of the reference driver (timestep, PdV predictor, accelerate, PdV
 corrector, flux_calc, advection, reset_field, and field_summary every 10
 steps).  The headline runs the timed steps as one device-resident CUDA graph
-through the C ABI's cb_run with fuse = 1 (dt on the device, viscosity with
-calc_dt, the PdV corrector with flux_calc and reset_field inside the second
-sweeps: FP64 results identical to the bit to the phase-by-phase calls).  The
-same steps enqueued phase by phase in the driver's call order, with the
-driver's per-step dt read-back, are timed too (host_loop), with CUDA events
-at every phase boundary for the per-kernel roofline.  Every field array is
-472 MB, far above the 126 MB L2, so no flush is needed between steps.
+through the C ABI's cb_run with fuse = 1 (dt on the device; ideal_gas,
+viscosity and calc_dt in one pass; the PdV predictor, accelerate, the PdV
+corrector and flux_calc in one pass; reset_field inside the second sweeps:
+FP64 results identical to the bit to the phase-by-phase calls).  The same
+steps enqueued phase by phase in the driver's call order, with the driver's
+per-step dt read-back, are timed too (host_loop), with CUDA events at every
+phase boundary; the roofline's kernel, the fused Lagrangian pass, is timed
+the same way through cb_lagrangian.  Every field array is 472 MB, far above
+the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -28,7 +30,7 @@ end-to-end figure through the C ABI with host buffers, and the reference
 OpenMP build on the host cores (cpu_baseline).
 
 N > 1 runs under torchrun: the path does not shard (one mesh per GPU, no
-decomposition, as in the north star), so each rank advances its own replica
+decomposition), so each rank advances its own replica
 and value is the sum over ranks (weak scaling).  --impl reference times the
 reference's own OpenMP build (oracle/_ref/omp) on the host cores instead.
 """
@@ -55,6 +57,11 @@ UNIT = "cell-steps/s"
 PHASE_ARRAYS = {"ideal_gas": 4, "viscosity": 5, "calc_dt": 8, "pdv_predict": 11 + 4 + 4, "accelerate": 10,
                 "pdv_correct": 13, "flux_calc": 8, "advec_cell_s1": 8, "advec_mom_s1": 8, "advec_cell_s2": 7,
                 "advec_mom_s2": 7, "reset_field": 8, "field_summary": 10}
+# cb_lagrangian's own distinct arrays: reads xvel0, yvel0, density0, energy0,
+# pressure, viscosity; writes pressure, soundspeed, xvel1, yvel1, density1,
+# energy1, vol_flux_x, vol_flux_y (the four phases it replaces count 50)
+LAGRANGIAN_ARRAYS = 14
+LAGRANGIAN_REPLACES = ("pdv_predict", "accelerate", "pdv_correct", "flux_calc")
 STEP_ARRAYS = 105  # the step's phases, ideal_gas .. reset_field
 
 
@@ -174,15 +181,17 @@ class PhaseTimer:
         return tot, cnt
 
 
-def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1):
+def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1, lagrangian=False):
     """Sets up a chunk, runs warmup steps, then times `steps` steps; returns
-    (ms, run, chunk, phase totals, launches in the timed region)."""
+    (ms, run, chunk, phase totals, launches in the timed region).  With
+    `lagrangian` the step makes one cb_lagrangian call in place of PdV,
+    accelerate, PdV and flux_calc."""
     import torch
     from cloverleaf_b200 import Chunk, HydroRun
     dk = bench_deck(cells)
     dev = torch.cuda.current_device()
     c = Chunk(cells, cells, precision=precision, device=dev)
-    run = HydroRun(c, dk, forced_dt=forced_dt)
+    run = HydroRun(c, dk, forced_dt=forced_dt, lagrangian=lagrangian)
     run.start()
     for _ in range(warmup):
         run.hydro_step()
@@ -696,20 +705,30 @@ def main():
     e2e = {"value": replicas_value(S * S, args.steps, world, ms_e2e), "unit": UNIT,
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
 
-    # roofline of the dominant kernel (largest total time over the timed steps)
-    tot, cnt = phases
-    kern = {k: v for k, v in tot.items() if k in PHASE_ARRAYS and k != "calc_dt"}
-    dom = max(kern, key=kern.get)
-    avg_ms = tot[dom] / cnt[dom]
-    alg = PHASE_ARRAYS[dom] * 8 * S * S
+    # roofline of the headline graph's dominant kernel, kt_lagrange (the fused
+    # Lagrangian pass): the same kernel through cb_lagrangian in a host loop,
+    # a CUDA event pair around each call on the chunk's stream (the call also
+    # launches the pressure's outer-ring copy, a few microseconds)
+    lag_steps = min(args.steps, 20)
+    _, _, cf, phf, _ = run_form(FP64, S, args.warmup, lag_steps, with_phases=True, rank=rank, world=world, lagrangian=True)
+    cf.close()
+    ftot, fcnt = phf
+    dom = "lagrangian"
+    avg_ms = ftot[dom] / fcnt[dom]
+    alg = LAGRANGIAN_ARRAYS * 8 * S * S
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = traffic_per_launch(dom, S)
-    roof = {"kernel": dom, "timed_in": "host_loop (the same kernel runs in the graph)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak,
+    tot, cnt = phases
+    replaced_ms = sum(tot[k] / cnt[k] for k in LAGRANGIAN_REPLACES)
+    roof = {"kernel": "kt_lagrange<double, 8> (cb_lagrangian)", "timed_in": f"host loop with cb_lagrangian, {lag_steps} steps",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic_frac": (traffic / (avg_ms / 1e3) / 1e9 / peak) if traffic else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-            else "fallback 6.65 TB/s", "traffic": traffic, "alg_bytes_per_launch": alg,
+            else "fallback 6.65 TB/s", "traffic": traffic, "alg_bytes_per_launch": alg, "ms_per_launch": avg_ms,
+            "replaced_phases_ms": replaced_ms,
+            "replaced_phases_alg_bytes": sum(PHASE_ARRAYS[k] for k in LAGRANGIAN_REPLACES) * 8 * S * S,
             "step_frac": value / world * STEP_ARRAYS * 8 / 1e9 / peak,
+            "fused_host_loop_phase_ms_per_step": {k: ftot[k] / lag_steps for k in sorted(ftot)},
             "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)}}
 
     batch = None

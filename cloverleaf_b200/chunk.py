@@ -30,7 +30,7 @@ OPT_FOLD_HALO, OPT_RESET_BY_SWAP = 1, 2
 EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "cb_create", "cb_destroy", "cb_set_gamma", "cb_set_option", "cb_get_extent",
            "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk",
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_pdv", "cb_revert", "cb_accelerate",
-           "cb_flux_calc", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
+           "cb_flux_calc", "cb_lagrangian", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
            "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_run", "cb_field_summary_noalloc",
            "cb_batch_create", "cb_batch_destroy", "cb_batch_set_schedule", "cb_batch_get_schedule", "cb_batch_autotune",
            "cb_batch_run", "cb_batch_synchronize", "cb_batch_deck_result", "cb_batch_read_summaries", "cb_batch_read_dt",
@@ -96,7 +96,7 @@ def library() -> ctypes.CDLL:
         "cb_ideal_gas": ([P, i, i], i), "cb_viscosity": ([P, i], i),
         "cb_calc_dt": ([P, ctypes.POINTER(DtParams), dp, ip, ip, ip, ip], i),
         "cb_pdv": ([P, i, d, i, i], i), "cb_revert": ([P], i), "cb_accelerate": ([P, d, i], i),
-        "cb_flux_calc": ([P, d, i], i), "cb_advec_cell": ([P, i, i, i], i), "cb_advec_mom": ([P, i, i, i, i], i),
+        "cb_flux_calc": ([P, d, i], i), "cb_lagrangian": ([P, d, i], i), "cb_advec_cell": ([P, i, i, i], i), "cb_advec_mom": ([P, i, i, i, i], i),
         "cb_reset_field": ([P, i], i), "cb_update_halo": ([P, ip, i], i), "cb_field_summary": ([P, dp], i),
         "cb_synchronize": ([P], i), "cb_get_stream": ([P, ctypes.POINTER(P)], i),
         "cb_launch_count": ([P, ctypes.POINTER(ctypes.c_longlong)], i),
@@ -230,6 +230,10 @@ class Chunk:
     def revert(self): _check(self._L.cb_revert(self._h))
     def accelerate(self, dt: float, halo_depth: int = 0): _check(self._L.cb_accelerate(self._h, dt, halo_depth))
     def flux_calc(self, dt: float, halo_depth: int = 0): _check(self._L.cb_flux_calc(self._h, dt, halo_depth))
+
+    def lagrangian(self, dt: float, halo_depth: int = 0):
+        """pdv(True, dt, full=True, halo_depth=1), accelerate, pdv(False) and flux_calc (all at halo_depth) in one pass."""
+        _check(self._L.cb_lagrangian(self._h, dt, halo_depth))
 
     def advec_cell(self, sweep_number: int, direction: int, halo_depth: int = 0):
         _check(self._L.cb_advec_cell(self._h, sweep_number, direction, halo_depth))

@@ -617,6 +617,26 @@ int cb_flux_calc(cb_chunk *c, double dt, int halo_depth) {
   return CB_OK;
 }
 
+int cb_lagrangian(cb_chunk *c, double dt, int halo_depth) {
+  CB_CHECK_CHUNK(c);
+  if (int r = check_depth(halo_depth, true)) return r;
+  const int fold = effective_fold(c, halo_depth);
+  if (fold == 0) { // nothing folds: the four phases as their own passes
+    if (int r = cb_pdv(c, 1, dt, 1, 1)) return r;
+    if (int r = cb_accelerate(c, dt, halo_depth)) return r;
+    if (int r = cb_pdv(c, 0, dt, 0, halo_depth)) return r;
+    return cb_flux_calc(c, dt, halo_depth);
+  }
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.lagrange(*c, c->spare_base(4), dt, 1, fold, fold, fold, true); }));
+  std::swap(c->fbuf[PRESSURE], c->sbuf[4]); // the predicted pressure went to the spare
+  c->halo_fresh[PRESSURE] = 1;
+  c->halo_fresh[SOUNDSPEED] = 0;
+  c->halo_fresh[XVEL1] = c->halo_fresh[YVEL1] = fold;
+  c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = fold;
+  c->halo_fresh[VOL_FLUX_X] = c->halo_fresh[VOL_FLUX_Y] = fold;
+  return CB_OK;
+}
+
 int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth) {
   CB_CHECK_CHUNK(c);
   if (sweep_number != 1 && sweep_number != 2) return fail(CB_EINVAL, "cb_advec_cell: sweep_number must be 1 or 2");

@@ -46,8 +46,9 @@ template <typename T> struct Ops {
   static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold); // ideal_gas too
   // the PdV predictor, accelerate, the PdV corrector and flux_calc in one
   // pass, every output folded (depths above zero); the predicted pressure
-  // goes to p_out
-  static cudaError_t lagrange(Chunk &c, void *p_out, int p_fold, int acc_fold, int pdv_fold, int flux_fold);
+  // goes to p_out, with the pressure's outer halo ring (which the pass does
+  // not write) copied there first when keep_ring is set
+  static cudaError_t lagrange(Chunk &c, void *p_out, double dt, int p_fold, int acc_fold, int pdv_fold, int flux_fold, bool keep_ring);
 };
 
 extern template struct Ops<double>;

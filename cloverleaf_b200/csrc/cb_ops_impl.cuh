@@ -282,8 +282,14 @@ template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k
   return launched(c);
 }
 
-template <typename T> cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, int p_fold, int acc_fold, int pdv_fold, int flux_fold) {
+template <typename T>
+cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int acc_fold, int pdv_fold, int flux_fold, bool keep_ring) {
   if (p_fold <= 0 || acc_fold <= 0 || pdv_fold <= 0 || flux_fold <= 0) return cudaErrorInvalidValue;
+  if (keep_ring) {
+    RingPair rp{{c.base(PRESSURE), nullptr}, {p_out, nullptr}};
+    cudaError_t e = copy_ring<T>(c, rp, 1, 1, c.nx + 2, 1, c.ny + 2, c.nx + 4, c.ny + 4);
+    if (e != cudaSuccess) return e;
+  }
   constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 12;
   using L = LagLayout<T, TY>;
   cudaError_t e = allow_smem(kt_lagrange<T, TY>, L::SMEM);
@@ -293,7 +299,7 @@ template <typename T> cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, int p_
   const LagOut<T> out{(T *)p_out, (T *)c.base(SOUNDSPEED), (T *)c.base(XVEL1), (T *)c.base(YVEL1), (T *)c.base(DENSITY1),
                       (T *)c.base(ENERGY1), (T *)c.base(VOL_FLUX_X), (T *)c.base(VOL_FLUX_Y)};
   kt_lagrange<T, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, PRESSURE, VISCOSITY}), out,
-                                                            mesh<T>(c), (int)c.off, T(0), c.dt_dev, gm1<T>(c),
+                                                            mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, gm1<T>(c),
                                                             LagFolds{p_fold, acc_fold, pdv_fold, flux_fold}, c.d_err);
   return launched(c);
 }

@@ -222,7 +222,7 @@ template <typename T> struct Seq {
     const int ff = eff(dep(2));
     if (fuse) {
       // fused: the whole Lagrangian step in one pass
-      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), fp, fa, fc, ff));
+      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), 0.0, fp, fa, fc, ff, false));
       swap_pressure();
     } else if (emit) {
       run(Ops<T>::pdv(c, 1, 0.0, 1, fp));

@@ -36,10 +36,12 @@ class HydroRun:
     """State of one run: globals.step, time, dt, dtold, advect_x (driver/definitions.h:258-280)."""
 
     def __init__(self, chunk: Chunk, deck: Deck, fold: bool = True, forced_dt: Optional[List[float]] = None,
-                 probe: Optional[Callable[[str], None]] = None):
+                 probe: Optional[Callable[[str], None]] = None, lagrangian: bool = False):
         self.c = chunk
         self.deck = deck
         self.fold = fold
+        # lagrangian: the PdV / accelerate / PdV / flux_calc calls as one cb_lagrangian call
+        self.lagrangian = lagrangian
         # forced_dt replays a recorded dt sequence (calc_dt still runs); probe(name)
         # is called as each phase is about to be enqueued ("end" closes a step)
         self.forced_dt = forced_dt
@@ -119,14 +121,18 @@ class HydroRun:
         self.step += 1
         self.timestep()
         self.dt_trace.append(self.dt)
-        self._mark("pdv_predict")
-        c.pdv(True, self.dt, full=True, halo_depth=1)  # the predictor's own pressure halo
-        self._mark("accelerate")
-        c.accelerate(self.dt, self._depth(2))
-        self._mark("pdv_correct")
-        c.pdv(False, self.dt, halo_depth=self._depth(2))
-        self._mark("flux_calc")
-        c.flux_calc(self.dt, self._depth(2))
+        if self.lagrangian:
+            self._mark("lagrangian")
+            c.lagrangian(self.dt, self._depth(2))
+        else:
+            self._mark("pdv_predict")
+            c.pdv(True, self.dt, full=True, halo_depth=1)  # the predictor's own pressure halo
+            self._mark("accelerate")
+            c.accelerate(self.dt, self._depth(2))
+            self._mark("pdv_correct")
+            c.pdv(False, self.dt, halo_depth=self._depth(2))
+            self._mark("flux_calc")
+            c.flux_calc(self.dt, self._depth(2))
         self.advection()
         self._mark("reset_field")
         c.reset_field(self._depth(1))

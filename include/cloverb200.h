@@ -123,6 +123,16 @@ int cb_revert(cb_chunk *c);
 int cb_accelerate(cb_chunk *c, double dt, int halo_depth);
 /* driver/flux_calc.h:24. */
 int cb_flux_calc(cb_chunk *c, double dt, int halo_depth);
+/* The Lagrangian step of driver/hydro.cpp:69-75 in one pass: the calls
+ * cb_pdv(c, 1, dt, 1, 1), cb_accelerate(c, dt, halo_depth),
+ * cb_pdv(c, 0, dt, 0, halo_depth) and cb_flux_calc(c, dt, halo_depth) (the
+ * reference's PdV.cpp:36-133 predictor and corrector with ideal_gas,
+ * update_halo(pressure) and revert, accelerate.cpp:28-56, flux_calc.cpp:27-43),
+ * with the same results and halo state.  One kernel when the chunk folds
+ * halos (each tile recomputes the predicted pressures and level-1 velocities
+ * of a one-cell ring around it); otherwise the four phases, one pass each.
+ * No counterpart in the reference, whose model interface has the four calls. */
+int cb_lagrangian(cb_chunk *c, double dt, int halo_depth);
 /* driver/advec_cell.h:24 -- dir 1 = x, 2 = y. */
 int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth);
 /* driver/advec_mom.h:24 -- which_vel 1 (x velocity), 2 (y velocity) or 3
