@@ -823,15 +823,25 @@ template <typename T, int TY> struct LagLayout {
   __device__ static constexpr int at(int i, int j, int x0, int y0) { return (j - y0 + 1) * BOX_X + (i - x0 + HALO); }
 };
 
-// The items (p, l), p < NA, l < NB, of a ring stage, spread evenly over the
-// block's 256 threads (item t = tid + 256 k, row-major): as few rounds as
-// the item count allows.
-template <int NA, int NB, typename F> __device__ __forceinline__ void each_spread(F &&f) {
-  const int tid = threadIdx.y * 64 + threadIdx.x;
+// The items (p, l), p < NA, l < NB, of a ring stage over the block's eight
+// warps: a warp takes 32 consecutive positions of one row (G such groups per
+// row), and the R = NA mod 32 positions left at the end of every row are
+// packed into shared groups taken last.  Lanes of a full group read
+// consecutive elements of one row of shared memory (no bank conflicts), and
+// the rounds are as few as the groups allow.
+template <int NA, int NB, typename F> __device__ __forceinline__ void each_rows(F &&f) {
+  constexpr int G = NA / 32, R = NA % 32;
+  constexpr int NG = NB * G, NL = (NB * R + 31) / 32;
+  const int w = (threadIdx.y * 64 + threadIdx.x) >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-  for (int k = 0; k < (NA * NB + 255) / 256; ++k) {
-    const int t = tid + 256 * k;
-    if (t < NA * NB) f(t % NA, t / NA);
+  for (int k = 0; k < (NG + NL + 7) / 8; ++k) {
+    const int u = w + 8 * k; // warp-uniform
+    if (u < NG) {
+      f(32 * (u % G) + lane, u / G);
+    } else if (u < NG + NL) {
+      const int t = (u - NG) * 32 + lane;
+      if (t < NB * R) f(32 * G + t % R, t / R);
+    }
   }
 }
 
@@ -860,7 +870,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   if (!stage_wait(cx)) return;
   const int pitch = (int)m.pitch;
   // (1) the predictor over the pressure ring
-  each_spread<L::PCX, L::PCY>([&](int p, int l) {
+  each_rows<L::PCX, L::PCY>([&](int p, int l) {
     const int i = x0 - 1 + p, j = y0 - 1 + l;
     if (EDGE && (i > m.nx + 2 || j > m.ny + 2)) return; // no node of the mesh reads it
     const int ic = EDGE ? min(max(i, 2), m.nx + 1) : i, jc = EDGE ? min(max(j, 2), m.ny + 1) : j;
@@ -884,7 +894,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   __syncthreads();
   // (2) accelerate over the nodes [x0, x0 + 64] x [y0, y0 + TY]
   const T halfdt = T(0.5) * dt;
-  each_spread<L::NNX, L::NNY>([&](int p, int l) {
+  each_rows<L::NNX, L::NNY>([&](int p, int l) {
     const int i = x0 + p, j = y0 + l;
     if (EDGE && (i > m.nx + 2 || j > m.ny + 2)) return;
     const int b = L::at(i, j, x0, y0);
