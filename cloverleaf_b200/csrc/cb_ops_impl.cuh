@@ -269,7 +269,7 @@ template <typename T> cudaError_t Ops<T>::visc_dt(Chunk &c, const DtConsts &k, i
 template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold) {
   constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
-  const size_t smem = 4 * B::BOXS * sizeof(T);
+  const size_t smem = (4 * B::BOXS + (sizeof(T) == sizeof(double) ? REST_MEMO_ELEMS : 0)) * sizeof(T);
   cudaError_t e = allow_smem(kt_ig_visc_dt<T>, smem);
   if (e != cudaSuccess) return e;
   const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;

@@ -20,6 +20,8 @@
 #include "cb_ops.h"
 #include "cb_tma.cuh"
 
+#include <limits>
+
 namespace cb {
 
 template <int TY> struct Tile {
@@ -341,6 +343,30 @@ template <typename T> struct RestMemo {
   }
 };
 
+// RestMemo with its four values in shared memory (value k of thread t at
+// k * 256 + t): the same test, without the registers (for kernels whose
+// registers are spent elsewhere).  The values start as NaN, which no value
+// equals.
+template <typename T> struct RestMemoShared {
+  T *v;
+  __device__ __forceinline__ explicit RestMemoShared(T *base) : v(base + threadIdx.y * 64 + threadIdx.x) {
+    v[0] = v[256] = v[512] = v[768] = std::numeric_limits<T>::quiet_NaN();
+  }
+  __device__ __forceinline__ bool seen(bool rest, T s, T d, T x, T y) {
+    if (!rest) return false;
+    if (s == v[0] && d == v[256] && x == v[512] && y == v[768]) return true;
+    v[0] = s, v[256] = d, v[512] = x, v[768] = y;
+    return false;
+  }
+};
+constexpr int REST_MEMO_ELEMS = 4 * 256;
+template <typename M, typename T> __device__ __forceinline__ M make_memo(T *base) {
+  if constexpr (std::is_same<M, RestMemoShared<T>>::value)
+    return M(base);
+  else
+    return M();
+}
+
 template <typename T>
 __device__ __forceinline__ bool at_rest(T q, T u00, T u10, T u01, T u11, T v00, T v10, T v01, T v11) {
   return q == T(0) && u00 == T(0) && u10 == T(0) && u01 == T(0) && u11 == T(0) && v00 == T(0) && v10 == T(0) && v01 == T(0) &&
@@ -448,9 +474,9 @@ static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height"
 // depth ig_fold) and the neighbours' pressures viscosity reads from the
 // staged density0 / energy0 (their halos hold the mirrored values, so the
 // mirrored pressures come out as ideal_gas's fold writes them).
-template <typename T, bool IG = false>
+template <typename T, bool IG = false, typename Memo = RestMemo<T>>
 __device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, T *q_out, const Mesh<T> &m, int off,
-                                             const DtConsts &k, int fold, int bx, int by, double &vmin, RestMemo<T> &memo, T gm1 = T(0),
+                                             const DtConsts &k, int fold, int bx, int by, double &vmin, Memo &memo, T gm1 = T(0),
                                              T *p_out = nullptr, T *c_out = nullptr, int ig_fold = 0) {
   constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
@@ -550,7 +576,10 @@ __global__ void __launch_bounds__(256, 4) kt_ig_visc_dt(const __grid_constant__ 
   const MapSet ms = map_set(maps, 4);
   const DtIn in{nullptr, nullptr, nullptr};
   double vmin = g_big;
-  RestMemo<T> memo;
+  // FP64: the memo in shared memory after the four staged boxes (its registers
+  // spilled); FP32: in registers (measured faster there)
+  using Memo = std::conditional_t<sizeof(T) == sizeof(double), RestMemoShared<T>, RestMemo<T>>;
+  Memo memo = make_memo<Memo>(sm + 4 * Box1<T, VISC_TY>::BOXS);
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     if (!visc_dt_tile<T, true>(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin, memo, gm1, p_out, c_out, ig_fold))
       return;
