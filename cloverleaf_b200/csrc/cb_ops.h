@@ -41,9 +41,8 @@ template <typename T> struct Ops {
   static cudaError_t reset_field(Chunk &c, int fold);
   static cudaError_t update_halo(Chunk &c, const HaloJob &job, int depth);
   static cudaError_t field_summary(Chunk &c);
-  // fused passes of the resident loop: viscosity + calc_dt, PdV corrector + flux_calc
-  static cudaError_t visc_dt(Chunk &c, const DtConsts &k, int fold);
-  static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold); // ideal_gas too
+  // fused passes of the resident loop: ideal_gas + viscosity + calc_dt, and the Lagrangian step
+  static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold);
   // the PdV predictor, accelerate, the PdV corrector and flux_calc in one
   // pass, every output folded (depths above zero); the predicted pressure
   // goes to p_out, with the pressure's outer halo ring (which the pass does

@@ -107,7 +107,7 @@ template <typename T> cudaError_t Ops<T>::viscosity(Chunk &c, int fold) {
 template <typename T> cudaError_t Ops<T>::calc_dt(Chunk &c, const DtConsts &k) {
   constexpr int TY = 16;
   using B = Box1<T, TY>;
-  const size_t smem = 2 * B::BOXS * sizeof(T);
+  const size_t smem = (2 * B::BOXS + (sizeof(T) == sizeof(double) ? REST_MEMO_ELEMS : 0)) * sizeof(T);
   cudaError_t e = allow_smem(kt_calc_dt<T>, smem);
   if (e != cudaSuccess) return e;
   const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
@@ -248,22 +248,6 @@ template <typename T> cudaError_t Ops<T>::update_halo(Chunk &c, const HaloJob &j
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
-}
-
-template <typename T> cudaError_t Ops<T>::visc_dt(Chunk &c, const DtConsts &k, int fold) {
-  constexpr int TY = VISC_TY;
-  using B = Box1<T, TY>;
-  const size_t smem = 3 * B::BOXS * sizeof(T);
-  cudaError_t e = allow_smem(kt_visc_dt<T>, smem);
-  if (e != cudaSuccess) return e;
-  const int tx = (c.nx + TILE_X - 1) / TILE_X, ty = (c.ny + TY - 1) / TY, nt = tx * ty;
-  int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt_visc_dt<T>, 256, smem)) != cudaSuccess) return e;
-  const int grid = std::min(nt, c.sms * std::max(per_sm, 1));
-  DtIn in{c.base(SOUNDSPEED), c.base(VISCOSITY), c.base(DENSITY0)};
-  kt_visc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {PRESSURE, XVEL0, YVEL0}), in, (T *)c.base(VISCOSITY), mesh<T>(c),
-                                                       (int)c.off, k, fold, tx, nt, c.d_dt_bits, c.d_err);
-  return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold) {

@@ -382,9 +382,9 @@ struct DtIn {
 constexpr int DT_TY = 16;
 template <typename T> constexpr size_t dt_smem() { return 2 * Box1<T, DT_TY>::BOXS * sizeof(T); }
 
-template <typename T>
+template <typename T, typename Memo>
 __device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, const Mesh<T> &m, int off,
-                                             const DtConsts &k, int bx, int by, double &vmin, RestMemo<T> &memo) {
+                                             const DtConsts &k, int bx, int by, double &vmin, Memo &memo) {
   constexpr int TY = DT_TY;
   using B = Box1<T, TY>;
   const T *U = sm, *V = sm + B::BOXS;
@@ -414,8 +414,8 @@ __device__ __forceinline__ bool calc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
       const int j = y0 + threadIdx.y + 4 * r;
       if (j >= m.ny + 2) break;
       const int b = B::at(i, j, x0, y0);
-      // (FP32 only here: the FP64 kernel's registers are spent on the estimate filter)
-      if (sizeof(T) == sizeof(float) &&
+      // (FP64: only with the memo in shared memory; its registers are spent on the estimate filter)
+      if ((sizeof(T) == sizeof(float) || !std::is_same<Memo, RestMemo<T>>::value) &&
           memo.seen(at_rest(qq[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1]), ss[r],
                     dd[r], dsx, m.celldy_t[j]))
         continue;
@@ -443,7 +443,8 @@ __global__ void __launch_bounds__(256, 4) kt_calc_dt(const __grid_constant__ Map
   TileCtx cx = tile_ctx(&bar, err);
   const MapSet ms = map_set(maps, 2);
   double vmin = g_big;
-  RestMemo<T> memo;
+  using Memo = std::conditional_t<sizeof(T) == sizeof(double), RestMemoShared<T>, RestMemo<T>>;
+  Memo memo = make_memo<Memo>(sm + 2 * Box1<T, DT_TY>::BOXS);
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     if (!calc_dt_tile(cx, sm, ms, in, m, off, k, t % tiles_x, t / tiles_x, vmin, memo)) return;
   block_min_to(vmin, dt_bits);
@@ -461,45 +462,29 @@ __device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressur
 }
 
 // ---------------------------------------------------------------------------
-// viscosity and calc_dt in one pass (the resident loop): a tile's q is
-// computed and stored as viscosity_tile does, then used for the tile's dt as
-// calc_dt_tile uses the stored q -- the same values and the same minimum as
-// the two phases one after the other, with one staging of xvel0 / yvel0 and
-// one read of density0.  Staged: ms 0 pressure, 1 xvel0, 2 yvel0.
+// ideal_gas, viscosity and calc_dt in one pass (the resident loop).  A tile
+// stages density0, energy0 and the velocities; forms each cell's pressure and
+// sound speed as k_ideal_gas does (written, the pressure with its halo of
+// depth ig_fold) and the neighbours' pressures viscosity reads from the staged
+// density0 / energy0 (their halos hold the mirrored values, so the mirrored
+// pressures come out as ideal_gas's fold writes them); computes and stores q
+// as viscosity_tile does; and uses it for the cell's dt as calc_dt_tile uses
+// the stored q -- the same values and the same minimum as the three phases
+// one after the other.  Staged: ms 0 density0, 1 energy0, 2 xvel0, 3 yvel0.
 static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height");
 
-// IG: ideal_gas (the step's first phase) in the same pass as well: the tile
-// stages density0 / energy0 instead of pressure, forms each cell's pressure
-// and sound speed as k_ideal_gas does (written, the pressure with its halo of
-// depth ig_fold) and the neighbours' pressures viscosity reads from the
-// staged density0 / energy0 (their halos hold the mirrored values, so the
-// mirrored pressures come out as ideal_gas's fold writes them).
-template <typename T, bool IG = false, typename Memo = RestMemo<T>>
-__device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, const DtIn &in, T *q_out, const Mesh<T> &m, int off,
-                                             const DtConsts &k, int fold, int bx, int by, double &vmin, Memo &memo, T gm1 = T(0),
-                                             T *p_out = nullptr, T *c_out = nullptr, int ig_fold = 0) {
+template <typename T, typename Memo>
+__device__ __forceinline__ bool ig_visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, T *p_out, T *c_out, T *q_out, const Mesh<T> &m,
+                                                int off, const DtConsts &k, T gm1, int ig_fold, int fold, int bx, int by, double &vmin,
+                                                Memo &memo) {
   constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
-  const T *S = (const T *)in.soundspeed, *R = (const T *)in.density0;
   const int pitch = (int)m.pitch;
   constexpr int RPT = TY / 4;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const int i = x0 + threadIdx.x;
-  T ss[RPT], dd[RPT];
-  if constexpr (!IG) {
-#pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      const int j = y0 + threadIdx.y + 4 * r;
-      const bool in_mesh = i < m.nx + 2 && j < m.ny + 2;
-      const int g = gidx(pitch, i, j);
-      ss[r] = in_mesh ? S[g] : T(0);
-      dd[r] = in_mesh ? R[g] : T(1);
-    }
-  }
-  if (!stage(cx, sm, ms, IG ? 4 : 3, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
-  // staged: pressure, xvel0, yvel0 -- or (IG) density0, energy0, xvel0, yvel0
-  const T *P = sm, *D = sm, *E = sm + B::BOXS;
-  const T *U = sm + (IG ? 2 : 1) * B::BOXS, *V = sm + (IG ? 3 : 2) * B::BOXS;
+  if (!stage(cx, sm, ms, 4, B::BOXS, B::BH, off + x0 - HALO, y0 - 1)) return false;
+  const T *D = sm, *E = sm + B::BOXS, *U = sm + 2 * B::BOXS, *V = sm + 3 * B::BOXS;
   const double thr = sizeof(T) == sizeof(double) ? warp_min(vmin) * DT_SKIP : 0.0;
   if (i < m.nx + 2) {
     const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
@@ -512,56 +497,35 @@ __device__ __forceinline__ bool visc_dt_tile(TileCtx &cx, T *sm, const MapSet &m
       const int b = B::at(i, j, x0, y0);
       const int g = gidx(pitch, i, j);
       const T cdy = m.celldy_t[j];
-      T pl, pr, pb, pt;
-      if constexpr (IG) {
-        // src/serial/ideal_gas.cpp:28-48 for the cell; pressure alone for its neighbours
-        T p, c;
-        eos_value(D[b], E[b], gm1, p, c);
-        p_out[g] = p;
-        c_out[g] = c;
-        if (ig_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), ig_fold, i, j, p);
-        ss[r] = c;
-        dd[r] = D[b];
-        pl = gm1 * D[b - 1] * E[b - 1];
-        pr = gm1 * D[b + 1] * E[b + 1];
-        pb = gm1 * D[b - BOX_X] * E[b - BOX_X];
-        pt = gm1 * D[b + BOX_X] * E[b + BOX_X];
-      } else {
-        pl = P[b - 1], pr = P[b + 1], pb = P[b - BOX_X], pt = P[b + BOX_X];
-      }
+      // src/serial/ideal_gas.cpp:28-48 for the cell; pressure alone for its neighbours
+      T p, ss;
+      eos_value(D[b], E[b], gm1, p, ss);
+      p_out[g] = p;
+      c_out[g] = ss;
+      if (ig_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), ig_fold, i, j, p);
+      const T dd = D[b];
+      const T pl = gm1 * D[b - 1] * E[b - 1];
+      const T pr = gm1 * D[b + 1] * E[b + 1];
+      const T pb = gm1 * D[b - BOX_X] * E[b - BOX_X];
+      const T pt = gm1 * D[b + BOX_X] * E[b + BOX_X];
       const T q = viscosity_value(U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1], pl, pr, pb,
-                                  pt, dd[r], cdx, cdx1, cdy, m.celldy_t[j + 2]);
+                                  pt, dd, cdx, cdx1, cdy, m.celldy_t[j + 2]);
       q_out[g] = q;
       if (do_fold) fold_halo(q_out, m, halo_rule(VISCOSITY), fold, i, j, q);
-      if (memo.seen(at_rest(q, U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1]), ss[r], dd[r],
-                    cdx, cdy))
+      if (memo.seen(at_rest(q, U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X], V[b + BOX_X + 1]), ss, dd, cdx,
+                    cdy))
         continue;
       if constexpr (sizeof(T) == sizeof(double)) {
-        const double est = dt_estimate(ss[r], q, dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
+        const double est = dt_estimate(ss, q, dd, U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
                                        V[b + BOX_X + 1], cdx, cdy, k);
         if (est > thr) continue; // NaN estimates fall through to the exact value
       }
-      const double c = (double)dt_value(ss[r], q, dd[r], U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
+      const double c = (double)dt_value(ss, q, dd, U[b], U[b + 1], U[b + BOX_X], U[b + BOX_X + 1], V[b], V[b + 1], V[b + BOX_X],
                                         V[b + BOX_X + 1], cdx, cdy, k);
       vmin = fmin(c, vmin);
     }
   }
   return true;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256, 4) kt_visc_dt(const __grid_constant__ Maps maps, DtIn in, T *q_out, Mesh<T> m, int off, DtConsts k,
-                                                  int fold, int tiles_x, int ntiles, unsigned long long *dt_bits, int *err) {
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
-  TileCtx cx = tile_ctx(&bar, err);
-  const MapSet ms = map_set(maps, 3);
-  double vmin = g_big;
-  RestMemo<T> memo;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!visc_dt_tile(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin, memo)) return;
-  block_min_to(vmin, dt_bits);
 }
 
 // ideal_gas, viscosity and calc_dt in one pass (the resident loop).
@@ -574,15 +538,13 @@ __global__ void __launch_bounds__(256, 4) kt_ig_visc_dt(const __grid_constant__ 
   T *sm = reinterpret_cast<T *>(smraw);
   TileCtx cx = tile_ctx(&bar, err);
   const MapSet ms = map_set(maps, 4);
-  const DtIn in{nullptr, nullptr, nullptr};
   double vmin = g_big;
   // FP64: the memo in shared memory after the four staged boxes (its registers
   // spilled); FP32: in registers (measured faster there)
   using Memo = std::conditional_t<sizeof(T) == sizeof(double), RestMemoShared<T>, RestMemo<T>>;
   Memo memo = make_memo<Memo>(sm + 4 * Box1<T, VISC_TY>::BOXS);
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
-    if (!visc_dt_tile<T, true>(cx, sm, ms, in, q_out, m, off, k, fold, t % tiles_x, t / tiles_x, vmin, memo, gm1, p_out, c_out, ig_fold))
-      return;
+    if (!ig_visc_dt_tile(cx, sm, ms, p_out, c_out, q_out, m, off, k, gm1, ig_fold, fold, t % tiles_x, t / tiles_x, vmin, memo)) return;
   block_min_to(vmin, dt_bits);
 }
 
