@@ -175,10 +175,12 @@ typedef struct {
   int fold;                                          /* 1: producers write the halos the next update_halo
                                                         needs (halo_depth > 0 in the phase calls); 0: none do */
   int fuse;                                          /* 1 (with fold = 1, meshes of 8 cells and more): phases that
-                                                        share inputs run as one pass -- viscosity with calc_dt, the
-                                                        PdV corrector with flux_calc, reset_field inside the second
-                                                        sweeps; FP64 results unchanged to the bit, FP32 within its
-                                                        rounding (the fused kernels may contract differently) */
+                                                        share inputs run as one pass -- ideal_gas, viscosity and
+                                                        calc_dt; the PdV predictor, accelerate, the PdV corrector
+                                                        and flux_calc (as cb_lagrangian); reset_field inside the
+                                                        second sweeps -- six kernels a step; FP64 results unchanged
+                                                        to the bit, FP32 within its rounding (the fused kernels may
+                                                        contract differently) */
 } cb_run_params;
 
 /* The driver's loop state (driver/definitions.h:258-280). */
