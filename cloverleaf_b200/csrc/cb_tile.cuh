@@ -799,9 +799,10 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 // and writes the outputs of its own cells, nodes and faces.  The predictor's
 // revert is not written: the corrector overwrites density1 and energy1 in
 // every interior cell.  Every output is folded (fold depths above zero: the
-// halo faces are the fold's).  The predicted pressure goes to out.pressure, a buffer
-// other than the pressure's current one, because other tiles still read the
-// old pressure of their ring cells; the caller swaps the two.
+// halo faces are the fold's).  The predicted pressure goes to
+// out.pressure, a buffer other than the pressure's current one, because
+// other tiles still read the old pressure of their ring cells; the caller
+// swaps the two.
 // Staged: 0 xvel0, 1 yvel0, 2 density0, 3 energy0, 4 pressure, 5 viscosity,
 // rows y0 - 1 .. y0 + TY + 2.
 template <typename T, int TY> struct LagLayout {
