@@ -116,6 +116,48 @@ def test_lagrangian_then_device_loop(fuse):
     assert_same(c1, r1, c2, r2)
 
 
+def test_lagrangian_alternating_with_the_four_calls():
+    """Steps alternate between cb_lagrangian and the four calls: the pressure's buffer changes every other step."""
+    dk = deck_b()
+    c1, r1 = run(dk, FP64, False)
+    c2 = Chunk(dk.x_cells, dk.y_cells, gamma=dk.gamma)
+    r2 = HydroRun(c2, dk)
+    r2.start()
+    while True:
+        r2.lagrangian = r2.step % 2 == 0
+        if r2.hydro_step():
+            break
+    assert_same(c1, r1, c2, r2)
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32])
+def test_lagrangian_depth_one(precision):
+    """halo_depth 1: every output folded to depth 1, as the four calls at depth 1 leave them."""
+    dk = deck_a(48, 40, end_step=5)
+    chunks = []
+    for lag in (False, True):
+        c = Chunk(dk.x_cells, dk.y_cells, precision=precision, gamma=dk.gamma)
+        r = HydroRun(c, dk)
+        r.start()
+        for _ in range(4):
+            r.hydro_step()
+        r.timestep()
+        if lag:
+            c.lagrangian(r.dt, 1)
+        else:
+            c.pdv(True, r.dt, full=True, halo_depth=1)
+            c.accelerate(r.dt, 1)
+            c.pdv(False, r.dt, halo_depth=1)
+            c.flux_calc(r.dt, 1)
+        chunks.append(c)
+    for f in STATE_FIELDS:
+        x, y = chunks[0].read(f), chunks[1].read(f)
+        if precision == FP64:
+            assert np.array_equal(x.view(np.int64), y.view(np.int64)), f
+        else:
+            assert np.abs(x - y).max() <= 1e-5 * max(np.abs(x).max(), 1e-30), f
+
+
 def test_lagrangian_arguments_rejected():
     from cloverleaf_b200.chunk import CloverError
     c = Chunk(16, 16)
