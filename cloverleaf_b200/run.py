@@ -3,7 +3,7 @@ through the C ABI, in the reference driver's call order, and print the
 field summaries.
 
   python -m cloverleaf_b200.run --deck clover.in
-  python -m cloverleaf_b200.run --bm 4608 --steps 2 [--precision fp32] [--no-fold] [--resident [--fuse]]
+  python -m cloverleaf_b200.run --bm 4608 --steps 2 [--precision fp32] [--no-fold] [--lagrangian | --resident [--fuse]]
   python -m cloverleaf_b200.run --ensemble 512 [--precision fp32] [--runs 3]
 """
 from __future__ import annotations
@@ -27,6 +27,8 @@ def main(argv=None):
     ap.add_argument("--no-fold", action="store_true", help="run every update_halo as its own pass")
     ap.add_argument("--resident", action="store_true", help="run the steps as one device-resident CUDA graph (cb_run)")
     ap.add_argument("--fuse", action="store_true", help="with --resident: fused passes (cb_run fuse = 1)")
+    ap.add_argument("--lagrangian", action="store_true",
+                    help="host loop with one cb_lagrangian call in place of PdV, accelerate, PdV and flux_calc")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--runs", type=int, default=1, help="ensemble runs after one warm-up run")
     args = ap.parse_args(argv)
@@ -35,7 +37,7 @@ def main(argv=None):
 
     dk = read_deck(args.deck) if args.deck else nudged(benchmark_deck(args.bm, end_step=args.steps or 87))
     c = Chunk(dk.x_cells, dk.y_cells, precision=FP32 if args.precision == "fp32" else FP64, device=args.device)
-    run = HydroRun(c, dk, fold=not args.no_fold)
+    run = HydroRun(c, dk, fold=not args.no_fold, lagrangian=args.lagrangian)
     t = time.time()
     if args.resident:
         run.start()
