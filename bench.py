@@ -63,6 +63,7 @@ PHASE_ARRAYS = {"ideal_gas": 4, "viscosity": 5, "calc_dt": 8, "pdv_predict": 11 
 LAGRANGIAN_ARRAYS = 14
 LAGRANGIAN_REPLACES = ("pdv_predict", "accelerate", "pdv_correct", "flux_calc")
 STEP_ARRAYS = 105  # the step's phases, ideal_gas .. reset_field
+LARGE_STEPS = 50  # the 15360^2 deck runs 50 steps
 
 
 def max_over_ranks(ms, device):
@@ -247,6 +248,29 @@ def resident_form(precision, cells, warmup, steps, rank=0, world=1, fuse=True):
     if world > 1:
         torch.distributed.barrier()
     return t0.elapsed_time(t1), run, c, n1 - n0
+
+
+# fields the fused graph must leave bit-identical to the phase-by-phase loop
+CHECKED_FIELDS = ("density0", "energy0", "xvel0", "yvel0", "pressure", "soundspeed", "viscosity")
+
+
+def fused_identity(fused_final, fused_dt, fused_summaries, chunk, run):
+    """Compares the fused graph's final state, dt sequence and summaries
+    with the phase-by-phase loop's after the same steps of the same deck:
+    every value must agree to the bit (the fused kernels evaluate the same
+    expressions in the same order)."""
+    import numpy as np
+    bad = []
+    for n in CHECKED_FIELDS:
+        a, b = fused_final[n], chunk.read(n)
+        if not np.array_equal(a.view(np.int64), b.view(np.int64)):
+            bad.append(f"{n}: {int((a.view(np.int64) != b.view(np.int64)).sum())} values differ")
+    if fused_dt != list(run.dt_trace):
+        bad.append("dt sequence differs")
+    if [tuple(vars(x).values()) for x in fused_summaries] != [tuple(vars(x).values()) for x in run.summaries]:
+        bad.append("summaries differ")
+    return {"bit_identical": not bad, "fields": list(CHECKED_FIELDS), "steps": len(fused_dt),
+            "also": "dt of every step, every summary record", "mismatches": bad}
 
 
 def rel_errors(a64, a32):
@@ -560,11 +584,11 @@ def cpu_baseline(cells):
     (one core, a 960^2 sample) if the reference build is absent."""
     cores = cpu_cores()
     if os.path.exists(reference_exe()):
-        per_cell = run_reference_omp(cells, 3, cores)
-        v = 1.0 / statistics.mean(per_cell[1:])
+        per_cell = run_reference_omp(cells, 4, cores)  # step times of steps 1-3 (the last step prints none)
+        v = 1.0 / statistics.mean(per_cell[1:3])
         return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                 "sample": f"reference OpenMP build (oracle/_ref/omp, g++ -O3), {cells}x{cells} benchmark deck, "
-                          f"steps 2-3 of a 3-step run, OMP_NUM_THREADS={cores}"}
+                          f"steps 2-3 of a 4-step run, OMP_NUM_THREADS={cores}"}
     import oracle
     from cloverleaf_b200 import benchmark_deck, nudged
     dk = nudged(benchmark_deck(960, end_step=3))
@@ -583,10 +607,13 @@ def main_reference(args, rank, world):
     if not os.path.exists(reference_exe()):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/omp was not built (needs the reference sources)"}))
         return
-    steps = min(args.steps, 20)
-    warm = max(1, min(args.warmup, 3))
-    per_cell = run_reference_omp(args.size, warm + steps, cores)
+    steps, warm = args.steps, args.warmup
+    # the driver prints a step's time after every step but the last: a run of
+    # warm + steps + 1 steps gives the `steps` timed values after `warm`
+    per_cell = run_reference_omp(args.size, warm + steps + 1, cores, timeout=3600)
     timed = per_cell[warm:warm + steps]
+    if len(timed) != steps:
+        raise SystemExit(f"bench.py: the reference run printed {len(per_cell)} step times, expected {warm + steps}")
     v = 1.0 / statistics.mean(timed)
     ms = statistics.mean(timed) * args.size * args.size * 1e3
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": len(timed),
@@ -655,6 +682,11 @@ def main():
         return errs
 
     errs_resident = field_errors(c64r, c32r)
+    # the fused graph's final state, kept on the host for the bit-identity
+    # check against the phase-by-phase loop below (same deck, same steps)
+    fused_final = {n: c64r.read(n) for n in CHECKED_FIELDS}
+    fused_dt = list(run64r.dt_trace)
+    fused_summaries = list(run64r.summaries)
     c64r.close()
     c32r.close()
 
@@ -662,6 +694,8 @@ def main():
     ms64h, run64, c64, phases, _ = run_form(FP64, S, args.warmup, args.steps, with_phases=True, rank=rank, world=world)
     if world > 1:
         ms64h = max_over_ranks(ms64h, "cuda")
+    fused_check = fused_identity(fused_final, fused_dt, fused_summaries, c64, run64)
+    del fused_final
     # FP32 form phase by phase, replaying the FP64 run's dt sequence: errors against FP64 at the same time
     dts = list(run64.dt_trace)
     ms32, run32, c32, ph32, _ = run_form(FP32, S, args.warmup, args.steps, forced_dt=dts, with_phases=True, world=world)
@@ -690,12 +724,13 @@ def main():
     large = None
     if args.large:
         try:
-            msl, _, cl, _ = resident_form(FP64, args.large, 3, 20, world=world)
+            msl, _, cl, _ = resident_form(FP64, args.large, 3, LARGE_STEPS, world=world)
             cl.close()
             if world > 1:
                 msl = max_over_ranks(msl, "cuda")
-            large = {"cells": f"{args.large}x{args.large}", "steps": 20, "value": replicas_value(args.large ** 2, 20, world, msl),
-                     "unit": UNIT}
+            large = {"cells": f"{args.large}x{args.large}", "steps": LARGE_STEPS,
+                     "value": replicas_value(args.large ** 2, LARGE_STEPS, world, msl), "unit": UNIT,
+                     "ms_per_step": msl / LARGE_STEPS, "path": "cb_run fused, 3 warm-up steps"}
         except Exception as e:  # memory or other failure is reported, not hidden
             large = {"error": str(e)}
 
@@ -770,18 +805,29 @@ def main():
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": ms64 / args.steps,
+                # compact figures first: the fused graph's parity with the phase-by-phase loop, the FP32 form,
+                # the phase-by-phase path, the 15360^2 deck, the dominant kernel
+                "fused_bit_identical": fused_check["bit_identical"],
+                "fp32_value": value32, "fp32_speedup": value32 / value,
+                "fp32_density_l1": errs_resident["density0"]["l1_rel"],
+                "host_loop_value": host_loop["value"],
+                "large_value": large.get("value") if large else None,
+                "roofline_frac": roof["frac"],
+                "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic: the reference benchmark deck generated in-process",
                 "config": {"workload": f"clover_bm FP64 {S}x{S} hydro steps (InputDecks/clover_bm64_300.in physics)",
                            "cells": S * S, "l2": "no flush: every field array (472 MB) exceeds the 126 MB L2",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "path": "cb_run: the timed steps as one device-resident CUDA graph, fused passes",
                            "halo": "folded into producers"},
-                "roofline": roof, "host_loop": host_loop, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "resident_loop": resident, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "fused_check": fused_check, "host_loop": host_loop, "fp32": fp32, "large": large, "batch": batch, "adjoint": adjoint, "resident_loop": resident, "reference_cuda": ref_cuda, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "cpu_baseline": cpu}
         print(json.dumps(line, default=_plain))
     if world > 1:
         torch.distributed.destroy_process_group()
+    if not fused_check["bit_identical"]:
+        raise SystemExit(f"bench.py: the fused graph's results differ from the phase-by-phase loop: {fused_check['mismatches']}")
 
 
 if __name__ == "__main__":

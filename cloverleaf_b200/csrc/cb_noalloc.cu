@@ -11,12 +11,17 @@
 // this entry point needs neither.
 //
 // The reduction's block partial sums and its completion counter live in one
-// file-scope __device__ array of fixed size (NOALLOC_MAX_TILES tiles of 32 x 8
-// cells: meshes up to 4,194,304 interior cells).  Every GPU that loads the
-// library holds that array until the process exits.  Host code cannot use
-// the array's name as a device address, so the first call on each device
-// asks the runtime for the address with cudaGetSymbolAddress (with that
-// device current) and caches it.  That first call should therefore come
+// file-scope __device__ array of fixed size: NOALLOC_MAX_TILES blocks of
+// 32 x 8 cells, one block per tile.  A mesh is accepted when
+// ceil(nx / 32) * ceil(ny / 8) <= NOALLOC_MAX_TILES (16384): 4,194,304 cells
+// when nx is a multiple of 32 and ny of 8, fewer otherwise (2050 x 2040 needs
+// 16575 blocks and is rejected).  Every GPU that loads the library holds that
+// array until the process exits.  Host code cannot use the array's name as a
+// device address, so the first call on each device asks the runtime for the
+// address with cudaGetSymbolAddress (with that device current) and caches it.
+// The address belongs to the device's primary context: the entry point must
+// not be called across cudaDeviceReset or from another context created on
+// the same device (cuCtxCreate), and its first call on a device should come
 // before any stream capture.  All calls on a device share the array: the
 // counter is cleared on the stream before each launch, and calls whose work
 // overlaps on the GPU (different streams, no ordering between them) race on
@@ -65,7 +70,7 @@ extern "C" int cb_field_summary_noalloc(int nx, int ny, long long pitch, const d
   if (tiles_x * tiles_y > NOALLOC_MAX_TILES)
     return set_last_error(CB_EINVAL, "cb_field_summary_noalloc: a " + std::to_string(nx) + " x " + std::to_string(ny) + " mesh needs " +
                                          std::to_string(tiles_x * tiles_y) + " reduction blocks; the fixed scratch holds " +
-                                         std::to_string(NOALLOC_MAX_TILES) + " (at most 4194304 interior cells)");
+                                         std::to_string(NOALLOC_MAX_TILES) + " (ceil(nx/32) * ceil(ny/8) must not exceed it)");
   if (pitch * (long long)(ny + 5) >= (1ll << 31)) return set_last_error(CB_EINVAL, "cb_field_summary_noalloc: arrays above 2^31 elements");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

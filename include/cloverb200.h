@@ -330,10 +330,12 @@ int cb_adjoint_read_field(cb_adjoint *a, int field, double *host, size_t n);
  * the last reverse sweep, and the device memory the adjoint holds. */
 int cb_adjoint_stats(const cb_adjoint *a, int *checkpoint_interval, int *checkpoints, long long *recomputed_steps, size_t *device_bytes);
 
-/* Self-test of the FP64 kernels' quotient of two mesh widths (formed with a
- * precomputed reciprocal) against the device's division operator on
- * `samples` pseudo-random pairs of positive operands; *mismatches counts the
- * quotients that differ in any bit.  No counterpart in the reference. */
+/* DIAGNOSTIC, not part of the hydro interface: a self-test of the FP64
+ * kernels' quotient of two mesh widths (formed with a precomputed reciprocal)
+ * against the device's division operator on `samples` pseudo-random pairs of
+ * positive operands; *mismatches counts the quotients that differ in any bit.
+ * The test suite calls it; a solver never needs to.  No counterpart in the
+ * reference. */
 int cb_selftest_width_ratio(long long samples, unsigned long long seed, long long *mismatches);
 
 /* The field summary of cb_field_summary (ideal_gas, then the five sums) over
@@ -347,10 +349,16 @@ int cb_selftest_width_ratio(long long samples, unsigned long long seed, long lon
  * 5 doubles) receives volume, mass, internal energy, kinetic energy and
  * pressure*volume.  The work is enqueued on `stream` (a cudaStream_t; NULL for
  * the default stream) and the call returns without waiting.  The reduction
- * scratch is one fixed device array inside the library (meshes of at most
- * 4,194,304 interior cells; larger ones are rejected), shared by all calls on
- * a device: the first call on each device looks up its address, so make it
- * before any stream capture, and do not let calls overlap on the GPU. */
+ * scratch is one fixed device array inside the library, with room for 16384
+ * blocks of 32 x 8 cells: a mesh is accepted when
+ * ceil(nx / 32) * ceil(ny / 8) <= 16384 (4,194,304 cells when nx is a
+ * multiple of 32 and ny of 8; a 2050 x 2040 mesh, 4,182,000 cells, needs
+ * 16575 blocks and is rejected with CB_EINVAL).  The array is shared by all
+ * calls on a device: the first call on each device looks up its address in
+ * the device's primary context and keeps it, so make that call before any
+ * stream capture, do not call the function from another context on the same
+ * device (cuCtxCreate) or across cudaDeviceReset, and do not let calls
+ * overlap on the GPU. */
 int cb_field_summary_noalloc(int nx, int ny, long long pitch, const double *density0, const double *energy0, const double *xvel0,
                              const double *yvel0, const double *celldx, const double *celldy, double *pressure, double *soundspeed,
                              double gamma, double *sums, void *stream);

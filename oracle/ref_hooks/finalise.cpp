@@ -1,3 +1,24 @@
+/*
+ Crown Copyright 2012 AWE.
+
+ This file is part of CloverLeaf.
+
+ CloverLeaf is free software: you can redistribute it and/or modify it under
+ the terms of the GNU General Public License as published by the
+ Free Software Foundation, either version 3 of the License, or (at your option)
+ any later version.
+
+ CloverLeaf is distributed in the hope that it will be useful, but
+ WITHOUT ANY WARRANTY; without even the implied warranty of MERCHANTABILITY or
+ FITNESS FOR A PARTICULAR PURPOSE. See the GNU General Public License for more
+ details.
+
+ You should have received a copy of the GNU General Public License along with
+ CloverLeaf. If not, see http://www.gnu.org/licenses/.
+ */
+
+// Derived from the reference's model file of the same name (the notice above
+// is the reference's); modified as described below.
 // Oracle capture hook -- a model file compiled INTO the reference build under
 // oracle/_ref/ in place of src/serial/finalise.cpp (which does nothing).  When
 // CLOVER_CAPTURE_FIELDS names a file, it writes the interior of the final

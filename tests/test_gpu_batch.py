@@ -18,7 +18,7 @@ import pytest
 import oracle
 from cloverleaf_b200 import FP32, FP64, Batch, Chunk, HydroRun
 from cloverleaf_b200 import batch as B
-from cloverleaf_b200.deck import GEOM_CIRC, GEOM_RECT, Deck, State, nudged
+from cloverleaf_b200.deck import GEOM_CIRC, GEOM_POINT, GEOM_RECT, Deck, State, nudged
 
 pytestmark = pytest.mark.gpu
 
@@ -26,8 +26,30 @@ CELL_FIELDS = ("density0", "energy0", "pressure", "soundspeed", "viscosity", "de
                "mass_flux_y", "vol_flux_x", "vol_flux_y", "xvel0", "yvel0")
 
 
+def vertex(dk, i, j):
+    """The coordinates of vertex (i, j) (0-based array index, halo included)
+    as the mesh set-up forms them: a point state paints the cell whose
+    low-left vertex equals its point exactly (src/serial/generate_chunk.cpp:116-126)."""
+    o = oracle.OracleChunk(dk.x_cells, dk.y_cells)
+    o.build_field()
+    o.initialise_chunk(dk.xmin, dk.ymin, dk.xmax, dk.ymax)
+    x, y = float(o.geom("vertexx")[i]), float(o.geom("vertexy")[j])
+    o.close()
+    return x, y
+
+
+def with_point(dk, density, energy, xvel, yvel, i, j):
+    """Appends a point state at vertex (i, j); the deck is already nudged, so
+    the point is set after the nudge (the reader would move it off the vertex)."""
+    x, y = vertex(dk, i, j)
+    dk.states.append(State(density=density, energy=energy, xvel=xvel, yvel=yvel, geometry=GEOM_POINT, xmin=x, ymin=y,
+                           defined=True))
+    return dk
+
+
 def mixed_decks():
-    """Uneven meshes (8 cells up to 130), gamma, rectangles and circles, moving states."""
+    """Uneven meshes (8 cells up to 130), gamma, rectangles, circles and
+    points, moving states; three-state decks."""
     rng = np.random.default_rng(7)
     sizes = [(8, 8), (13, 9), (40, 24), (64, 64), (96, 40), (130, 70), (17, 33), (70, 130), (24, 24), (9, 57)]
     out = []
@@ -43,7 +65,10 @@ def mixed_decks():
                                    ymin=3.0 * ny / nx, radius=1.5, defined=True))
         if k == 4:
             dk.end_step, dk.end_time = 9, 10.0  # ends on its step count
-        out.append(nudged(dk))
+        dk = nudged(dk)
+        if k % 3 == 2:  # background, rectangle and a moving point: three states
+            with_point(dk, 3.0, 2.0, 0.2 * (k % 2) - 0.1, 0.15, 2 + nx // 2, 2 + (2 * ny) // 3)
+        out.append(dk)
     return out
 
 
@@ -71,6 +96,42 @@ def check_deck(b, k, c, r):
     for name in ("xvel1", "yvel1"):
         x, y = b.read(k, name), c.read(name)
         assert np.array_equal(x[2:-2, 2:-2], y[2:-2, 2:-2]), (k, name)
+
+
+def large_decks():
+    """The ensemble's largest sides, 256 and 384 cells (tiles away from the
+    mesh edge, which smaller decks do not have), one of them with four states
+    (rectangle, circle, point), plus a 192 x 320 deck."""
+    out = []
+    for k, (nx, ny) in enumerate([(256, 256), (384, 384), (192, 320)]):
+        dk = Deck(x_cells=nx, y_cells=ny, xmin=0.0, ymin=0.0, xmax=10.0, ymax=10.0 * ny / nx, end_time=0.5,
+                  dtinit=0.04, dtmax=0.04, dtrise=1.5, summary_frequency=5, gamma=1.4 + 0.1 * k)
+        dk.states = [State(density=0.2, energy=1.0, defined=True),
+                     State(density=1.2 + 0.3 * k, energy=2.0 + k, geometry=GEOM_RECT, xmin=0.0, xmax=4.0 + k,
+                           ymin=0.0, ymax=2.5, defined=True)]
+        if k != 1:
+            dk.states.append(State(density=1.5, energy=3.0, xvel=0.3, yvel=-0.2, geometry=GEOM_CIRC, xmin=6.5,
+                                   ymin=6.0 * ny / nx, radius=1.4, defined=True))
+        dk = nudged(dk)
+        if k == 0:
+            with_point(dk, 4.0, 3.5, -0.2, 0.25, 2 + 3 * nx // 4, 2 + nx // 3)
+        out.append(dk)
+    return out
+
+
+def test_batch_large_decks_match_sequential_fp64():
+    decks = large_decks()
+    seq = [sequential(dk, FP64) for dk in decks]
+    with Batch(decks, FP64) as b:
+        b.set_schedule(cells_per_cta=4096, variant=1)
+        sched, lanes, ctas = b.schedule()
+        assert ctas > lanes  # the large decks run on lanes of several CTAs
+        b.run()
+        b.synchronize()
+        for k, (c, r) in enumerate(seq):
+            check_deck(b, k, c, r)
+    for c, _ in seq:
+        c.close()
 
 
 @pytest.fixture(scope="module")

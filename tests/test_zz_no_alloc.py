@@ -39,11 +39,13 @@ def _call(lib, torch, nx, ny, pitch, arrays, out, stream):
                                         1.4, _ptr(sums), ctypes.c_void_p(stream))
 
 
-def test_noalloc_summary_matches_chunk_summary_twice():
+@pytest.mark.parametrize("nx,ny,steps", [(300, 200, 25), (2048, 2048, 6)])
+def test_noalloc_summary_matches_chunk_summary_twice(nx, ny, steps):
+    """300 x 200, and 2048 x 2048: the largest square mesh the fixed scratch
+    takes (exactly 16384 blocks of 32 x 8 cells)."""
     torch = pytest.importorskip("torch")
-    nx, ny = 300, 200
     chunk = Chunk(nx, ny)
-    HydroRun(chunk, nudged(benchmark_deck(nx, 25, ny=ny))).run()  # a state with motion in it
+    HydroRun(chunk, nudged(benchmark_deck(nx, steps, ny=ny))).run()  # a state with motion in it
     lib = library()
     pitch, rows = nx + 5, ny + 5
     arrays = [_padded(torch, chunk.read(n), rows, pitch) for n in ("density0", "energy0", "xvel0", "yvel0")]
@@ -66,10 +68,15 @@ def test_noalloc_summary_matches_chunk_summary_twice():
     assert np.array_equal(results[0][2], results[1][2])
 
 
-def test_noalloc_rejects_mesh_beyond_scratch():
+@pytest.mark.parametrize("nx,ny,blocks", [(2100, 2100, 17292), (2049, 2048, 16640), (2050, 2040, 16575)])
+def test_noalloc_rejects_mesh_beyond_scratch(nx, ny, blocks):
+    """A mesh is accepted when ceil(nx/32) * ceil(ny/8) <= 16384: one column
+    past 2048 x 2048 is rejected, and so is 2050 x 2040 although it has fewer
+    than 4,194,304 cells.  Nothing is launched, so the arrays are never read."""
     torch = pytest.importorskip("torch")
     lib = library()
     small = torch.zeros(16, dtype=torch.float64, device="cuda")
-    rc = lib.cb_field_summary_noalloc(2100, 2100, 2105, *([_ptr(small)] * 8), 1.4, _ptr(small), ctypes.c_void_p(0))
+    rc = lib.cb_field_summary_noalloc(nx, ny, nx + 5, *([_ptr(small)] * 8), 1.4, _ptr(small), ctypes.c_void_p(0))
     assert rc == CB_EINVAL
-    assert b"4194304" in lib.cb_last_error()
+    msg = lib.cb_last_error()
+    assert str(blocks).encode() in msg and b"16384" in msg and b"ceil(nx/32) * ceil(ny/8)" in msg, msg
