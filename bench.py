@@ -15,7 +15,8 @@ FP64 results identical to the bit to the phase-by-phase calls).  The same
 steps enqueued phase by phase in the driver's call order, with the driver's
 per-step dt read-back, are timed too (host_loop), with CUDA events at every
 phase boundary; the roofline's kernel, the fused Lagrangian pass, is timed
-the same way through cb_lagrangian.  Every field array is 472 MB, far above
+the same way in a host loop with the chunk's call fusion on (the graph's
+fused passes launched one by one, an event pair around each).  Every field array is 472 MB, far above
 the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
@@ -57,7 +58,7 @@ UNIT = "cell-steps/s"
 PHASE_ARRAYS = {"ideal_gas": 4, "viscosity": 5, "calc_dt": 8, "pdv_predict": 11 + 4 + 4, "accelerate": 10,
                 "pdv_correct": 13, "flux_calc": 8, "advec_cell_s1": 8, "advec_mom_s1": 8, "advec_cell_s2": 7,
                 "advec_mom_s2": 7, "reset_field": 8, "field_summary": 10}
-# cb_lagrangian's own distinct arrays: reads xvel0, yvel0, density0, energy0,
+# the Lagrangian pass's own distinct arrays: reads xvel0, yvel0, density0, energy0,
 # pressure, viscosity; writes pressure, soundspeed, xvel1, yvel1, density1,
 # energy1, vol_flux_x, vol_flux_y (the four phases it replaces count 50)
 LAGRANGIAN_ARRAYS = 14
@@ -182,17 +183,19 @@ class PhaseTimer:
         return tot, cnt
 
 
-def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1, lagrangian=False):
+def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1, fuse_calls=False):
     """Sets up a chunk, runs warmup steps, then times `steps` steps; returns
     (ms, run, chunk, phase totals, launches in the timed region).  With
-    `lagrangian` the step makes one cb_lagrangian call in place of PdV,
-    accelerate, PdV and flux_calc."""
+    `fuse_calls` the chunk runs the driver's calls as the fused passes (one
+    launch each): the calc_dt mark times the ideal_gas + viscosity + calc_dt
+    pass (and the dt read-back), flux_calc the Lagrangian pass, reset_field
+    the two second sweeps."""
     import torch
     from cloverleaf_b200 import Chunk, HydroRun
     dk = bench_deck(cells)
     dev = torch.cuda.current_device()
     c = Chunk(cells, cells, precision=precision, device=dev)
-    run = HydroRun(c, dk, forced_dt=forced_dt, lagrangian=lagrangian)
+    run = HydroRun(c, dk, forced_dt=forced_dt, fuse_calls=fuse_calls)
     run.start()
     for _ in range(warmup):
         run.hydro_step()
@@ -741,21 +744,22 @@ def main():
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
 
     # roofline of the headline graph's dominant kernel, kt_lagrange (the fused
-    # Lagrangian pass): the same kernel through cb_lagrangian in a host loop,
-    # a CUDA event pair around each call on the chunk's stream (the call also
-    # launches the pressure's outer-ring copy, a few microseconds)
+    # Lagrangian pass): the graph's fused passes in a host loop (call fusion),
+    # a CUDA event pair around each group of calls on the chunk's stream; the
+    # flux_calc group is the Lagrangian pass (with the pressure's outer-ring
+    # copy, a few microseconds)
     lag_steps = min(args.steps, 20)
-    _, _, cf, phf, _ = run_form(FP64, S, args.warmup, lag_steps, with_phases=True, rank=rank, world=world, lagrangian=True)
+    msf, _, cf, phf, _ = run_form(FP64, S, args.warmup, lag_steps, with_phases=True, rank=rank, world=world, fuse_calls=True)
     cf.close()
     ftot, fcnt = phf
-    dom = "lagrangian"
+    dom = "flux_calc"
     avg_ms = ftot[dom] / fcnt[dom]
     alg = LAGRANGIAN_ARRAYS * 8 * S * S
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = traffic_per_launch(dom, S)
     tot, cnt = phases
     replaced_ms = sum(tot[k] / cnt[k] for k in LAGRANGIAN_REPLACES)
-    roof = {"kernel": "kt_lagrange<double, 8> (cb_lagrangian)", "timed_in": f"host loop with cb_lagrangian, {lag_steps} steps",
+    roof = {"kernel": "kt_lagrange<double, 8>", "timed_in": f"host loop with call fusion, {lag_steps} steps (flux_calc group)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic_frac": (traffic / (avg_ms / 1e3) / 1e9 / peak) if traffic else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
@@ -763,7 +767,12 @@ def main():
             "replaced_phases_ms": replaced_ms,
             "replaced_phases_alg_bytes": sum(PHASE_ARRAYS[k] for k in LAGRANGIAN_REPLACES) * 8 * S * S,
             "step_frac": value / world * STEP_ARRAYS * 8 / 1e9 / peak,
-            "fused_host_loop_phase_ms_per_step": {k: ftot[k] / lag_steps for k in sorted(ftot)},
+            "fused_calls_ms_per_step": msf / lag_steps,
+            "fused_calls_phase_ms_per_step": {k: ftot[k] / lag_steps for k in sorted(ftot)},
+            "fused_calls_kernels": {"calc_dt": "kt_ig_visc_dt + 8-byte dt read-back", "flux_calc": "kt_lagrange + ring copy",
+                                    "advec_cell_s1": "kt_advec_cell", "advec_mom_s1": "kt_advec_mom",
+                                    "reset_field": "both second sweeps (with reset_field's copy)",
+                                    "field_summary": "k_field_summary + 40-byte read-back"},
             "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)}}
 
     batch = None

@@ -24,7 +24,7 @@ GEOM_NAMES = ["cellx", "celly", "celldx", "celldy", "vertexx", "vertexy", "verte
 GEOM_ID = {n: i for i, n in enumerate(GEOM_NAMES)}
 FP64, FP32 = 0, 1
 LAYOUT_XFAST, LAYOUT_YFAST = 0, 1
-OPT_FOLD_HALO, OPT_RESET_BY_SWAP = 1, 2
+OPT_FOLD_HALO, OPT_FUSE_CALLS = 1, 3
 
 # Every symbol include/cloverb200.h declares.
 EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "cb_create", "cb_destroy", "cb_set_gamma", "cb_set_option", "cb_get_extent",

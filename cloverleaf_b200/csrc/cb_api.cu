@@ -34,11 +34,21 @@ int cuda_fail(cudaError_t e, const char *where) {
   return fail(CB_ECUDA, std::string(where) + ": " + cudaGetErrorName(e) + ": " + cudaGetErrorString(e));
 }
 
-#define CB_CHECK_CHUNK(c)                                                                                                                    \
+// Every entry point on a chunk first runs the calls call fusion holds back
+// (run_pending); the phase calls that may extend a held-back group check the
+// chunk without it (CB_CHECK_CHUNK_HOLD) and decide themselves.
+#define CB_CHECK_CHUNK_HOLD(c)                                                                                                               \
   do {                                                                                                                                       \
     if (!(c)) return fail(CB_EINVAL, std::string(__func__) + ": null chunk");                                                               \
     cudaError_t _e = select_device(c);                                                                                                       \
     if (_e != cudaSuccess) return cuda_fail(_e, __func__);                                                                                   \
+  } while (0)
+
+#define CB_CHECK_CHUNK(c)                                                                                                                    \
+  do {                                                                                                                                       \
+    CB_CHECK_CHUNK_HOLD(c);                                                                                                                  \
+    cudaError_t _e2 = run_pending(c);                                                                                                        \
+    if (_e2 != cudaSuccess) return cuda_fail(_e2, __func__);                                                                                 \
   } while (0)
 
 #define CB_CUDA(expr)                                                                                                                        \
@@ -80,6 +90,58 @@ int geom_len(const cb_chunk *c, int g) {
 }
 
 bool is_state_field(int f) { return f >= 0 && f < 15; }
+
+// cb_advec_cell's launch and buffer swap; reset_fold >= 0: the sweep also does
+// reset_field's copy of what it writes (the second sweep under call fusion).
+cudaError_t launch_cell(cb_chunk *c, int sweep, int dir, int fold, int reset_fold) {
+  void *dd = c->spare_base(0), *de = c->spare_base(1);
+  cudaError_t e = dispatch(c, [&](auto ops) { return ops.advec_cell(*c, sweep, dir, fold, dd, de, reset_fold); });
+  if (e != cudaSuccess) return e;
+  std::swap(c->fbuf[DENSITY1], c->sbuf[0]);
+  std::swap(c->fbuf[ENERGY1], c->sbuf[1]);
+  return cudaSuccess;
+}
+
+// cb_advec_mom's launch and buffer swaps (the same reset_fold).
+cudaError_t launch_mom(cb_chunk *c, int which_vel, int sweep, int dir, int fold, int reset_fold) {
+  void *du = c->spare_base(2), *dv = c->spare_base(3);
+  cudaError_t e = dispatch(c, [&](auto ops) { return ops.advec_mom(*c, which_vel, sweep, dir, fold, du, dv, reset_fold); });
+  if (e != cudaSuccess) return e;
+  if (which_vel & 1) std::swap(c->fbuf[XVEL1], c->sbuf[2]);
+  if (which_vel & 2) std::swap(c->fbuf[YVEL1], c->sbuf[3]);
+  return cudaSuccess;
+}
+
+// Runs the calls call fusion held back, one by one as they were made.
+cudaError_t run_pending(cb_chunk *c) {
+  const Pending p = c->pend;
+  c->pend = Pending{};
+  cudaError_t e = cudaSuccess;
+  auto go = [&](auto &&f) {
+    if (e == cudaSuccess) e = dispatch(c, f);
+  };
+  switch (p.kind) {
+    case PEND_IG:
+    case PEND_IG_VISC:
+      go([&](auto ops) { return ops.ideal_gas(*c, 0, p.ig_fold); });
+      if (p.kind == PEND_IG_VISC) go([&](auto ops) { return ops.viscosity(*c, p.visc_fold); });
+      break;
+    case PEND_PDV1:
+    case PEND_PDV1_ACC:
+    case PEND_PDV1_ACC_PDV0:
+      go([&](auto ops) { return ops.pdv(*c, 1, p.dt, 1, p.pdv1_fold); });
+      if (p.kind != PEND_PDV1) go([&](auto ops) { return ops.accelerate(*c, p.dt, p.acc_fold); });
+      if (p.kind == PEND_PDV1_ACC_PDV0) go([&](auto ops) { return ops.pdv(*c, 0, p.dt, 0, p.pdv0_fold); });
+      break;
+    case PEND_CELL2:
+    case PEND_CELL2_MOM2:
+      e = launch_cell(c, 2, p.cell_dir, p.cell_fold, -1);
+      if (e == cudaSuccess && p.kind == PEND_CELL2_MOM2) e = launch_mom(c, p.mom_mask, 2, p.mom_dir, p.mom_fold, -1);
+      break;
+    default: break;
+  }
+  return e;
+}
 
 int effective_fold(const cb_chunk *c, int depth) { return c->can_fold() ? depth : 0; }
 
@@ -239,6 +301,7 @@ int check_device_error(cb_chunk *c, const char *where) {
 
 namespace cb {
 int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+cudaError_t run_pending_calls(cb_chunk *c) { return run_pending(c); }
 } // namespace cb
 
 extern "C" {
@@ -366,8 +429,8 @@ int cb_set_option(cb_chunk *c, int option, int value) {
   if (option == CB_OPT_FOLD_HALO) {
     c->fold_enabled = value != 0;
     std::fill(std::begin(c->halo_fresh), std::end(c->halo_fresh), 0);
-  } else if (option == CB_OPT_RESET_BY_SWAP) {
-    c->reset_by_swap = value != 0;
+  } else if (option == CB_OPT_FUSE_CALLS) {
+    c->fuse_calls = value != 0;
   } else {
     return fail(CB_EINVAL, "cb_set_option: unknown option " + std::to_string(option));
   }
@@ -531,28 +594,46 @@ int cb_ideal_gas(cb_chunk *c, int predict, int halo_depth) {
   CB_CHECK_CHUNK(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.ideal_gas(*c, predict ? 1 : 0, fold); }));
+  if (c->fuse_calls && !predict && fold > 0) { // held back for calc_dt's pass
+    c->pend.kind = PEND_IG;
+    c->pend.ig_fold = fold;
+  } else {
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.ideal_gas(*c, predict ? 1 : 0, fold); }));
+  }
   c->halo_fresh[PRESSURE] = fold;
   c->halo_fresh[SOUNDSPEED] = 0;
   return CB_OK;
 }
 
 int cb_viscosity(cb_chunk *c, int halo_depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.viscosity(*c, fold); }));
+  if (c->pend.kind == PEND_IG && fold > 0) { // held back with ideal_gas for calc_dt's pass
+    c->pend.kind = PEND_IG_VISC;
+    c->pend.visc_fold = fold;
+  } else {
+    CB_CUDA(run_pending(c));
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.viscosity(*c, fold); }));
+  }
   c->halo_fresh[VISCOSITY] = fold;
   return CB_OK;
 }
 
 int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *control, int *jldt, int *kldt, int *small) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (!p || !dt_min_val) return fail(CB_EINVAL, "cb_calc_dt: null argument");
+  const Pending held = c->pend;
+  const bool fused = held.kind == PEND_IG_VISC;
+  if (!fused) CB_CUDA(run_pending(c));
+  c->pend = Pending{};
   DtConsts k{p->dtc_safe, p->dtu_safe, p->dtv_safe, p->dtdiv_safe};
   c->h_scalars[0] = g_big;
   CB_CUDA(cudaMemcpyAsync(c->d_dt_bits, &c->h_scalars[0], sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.calc_dt(*c, k); }));
+  if (fused) // ideal_gas, viscosity and calc_dt in one pass
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.ig_visc_dt(*c, k, held.ig_fold, held.visc_fold); }));
+  else
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.calc_dt(*c, k); }));
   CB_CUDA(cudaMemcpyAsync(&c->h_scalars[1], c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CB_CUDA(cudaStreamSynchronize(c->stream));
   if (int r = check_device_error(c, "cb_calc_dt")) return r;
@@ -570,11 +651,24 @@ int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *cont
 }
 
 int cb_pdv(cb_chunk *c, int predict, double dt, int full, int halo_depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   if (full && !predict) return fail(CB_EINVAL, "cb_pdv: full = 1 is the predictor step; use predict = 1");
   const int fold = effective_fold(c, halo_depth);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.pdv(*c, predict ? 1 : 0, dt, full ? 1 : 0, fold); }));
+  if (!predict && !full && c->pend.kind == PEND_PDV1_ACC && c->pend.dt == dt && fold > 0) {
+    // the corrector, held back with the predictor and accelerate for flux_calc's pass
+    c->pend.kind = PEND_PDV1_ACC_PDV0;
+    c->pend.pdv0_fold = fold;
+  } else {
+    CB_CUDA(run_pending(c));
+    if (full && c->fuse_calls && fold > 0) { // the predictor, held back for the Lagrangian pass
+      c->pend.kind = PEND_PDV1;
+      c->pend.dt = dt;
+      c->pend.pdv1_fold = fold;
+    } else {
+      CB_CUDA(dispatch(c, [&](auto ops) { return ops.pdv(*c, predict ? 1 : 0, dt, full ? 1 : 0, fold); }));
+    }
+  }
   if (full && halo_depth > 0 && fold == 0) {
     // the predictor's own update_halo(pressure) (src/serial/PdV.cpp:118-124) on a mesh too small to fold
     HaloJob job{};
@@ -600,19 +694,36 @@ int cb_revert(cb_chunk *c) {
 }
 
 int cb_accelerate(cb_chunk *c, double dt, int halo_depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.accelerate(*c, dt, fold); }));
+  if (c->pend.kind == PEND_PDV1 && c->pend.dt == dt && fold > 0) { // held back with the predictor
+    c->pend.kind = PEND_PDV1_ACC;
+    c->pend.acc_fold = fold;
+  } else {
+    CB_CUDA(run_pending(c));
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.accelerate(*c, dt, fold); }));
+  }
   c->halo_fresh[XVEL1] = c->halo_fresh[YVEL1] = fold;
   return CB_OK;
 }
 
 int cb_flux_calc(cb_chunk *c, double dt, int halo_depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.flux_calc(*c, dt, fold); }));
+  const Pending held = c->pend;
+  if (held.kind == PEND_PDV1_ACC_PDV0 && held.dt == dt && fold > 0) {
+    // the predictor, accelerate, the corrector and flux_calc as one pass (cb_lagrangian's)
+    c->pend = Pending{};
+    CB_CUDA(dispatch(c, [&](auto ops) {
+      return ops.lagrange(*c, c->spare_base(4), dt, held.pdv1_fold, held.acc_fold, held.pdv0_fold, fold, true);
+    }));
+    std::swap(c->fbuf[PRESSURE], c->sbuf[4]); // the predicted pressure went to the spare
+  } else {
+    CB_CUDA(run_pending(c));
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.flux_calc(*c, dt, fold); }));
+  }
   c->halo_fresh[VOL_FLUX_X] = c->halo_fresh[VOL_FLUX_Y] = fold;
   return CB_OK;
 }
@@ -643,46 +754,58 @@ int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth) 
   if (direction != 1 && direction != 2) return fail(CB_EINVAL, "cb_advec_cell: direction must be 1 (x) or 2 (y)");
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  void *dd = c->spare_base(0), *de = c->spare_base(1);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.advec_cell(*c, sweep_number, direction, fold, dd, de); }));
-  std::swap(c->fbuf[DENSITY1], c->sbuf[0]);
-  std::swap(c->fbuf[ENERGY1], c->sbuf[1]);
+  if (c->fuse_calls && sweep_number == 2 && fold == 2) { // held back for reset_field (the buffers swap when it runs)
+    c->pend.kind = PEND_CELL2;
+    c->pend.cell_dir = direction;
+    c->pend.cell_fold = fold;
+  } else {
+    CB_CUDA(launch_cell(c, sweep_number, direction, fold, -1));
+  }
   c->halo_fresh[DENSITY1] = c->halo_fresh[ENERGY1] = fold;
   c->halo_fresh[direction == 1 ? MASS_FLUX_X : MASS_FLUX_Y] = fold;
   return CB_OK;
 }
 
 int cb_advec_mom(cb_chunk *c, int which_vel, int sweep_number, int direction, int halo_depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (which_vel < 1 || which_vel > 3) return fail(CB_EINVAL, "cb_advec_mom: which_vel must be 1, 2 or 3");
   if (sweep_number != 1 && sweep_number != 2) return fail(CB_EINVAL, "cb_advec_mom: sweep_number must be 1 or 2");
   if (direction != 1 && direction != 2) return fail(CB_EINVAL, "cb_advec_mom: direction must be 1 (x) or 2 (y)");
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  void *du = c->spare_base(2), *dv = c->spare_base(3);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.advec_mom(*c, which_vel, sweep_number, direction, fold, du, dv); }));
-  if (which_vel & 1) {
-    std::swap(c->fbuf[XVEL1], c->sbuf[2]);
-    c->halo_fresh[XVEL1] = fold;
+  if (c->pend.kind == PEND_CELL2 && sweep_number == 2 && which_vel == 3) { // held back with the cell sweep for reset_field
+    c->pend.kind = PEND_CELL2_MOM2;
+    c->pend.mom_dir = direction;
+    c->pend.mom_fold = fold;
+    c->pend.mom_mask = which_vel;
+  } else {
+    CB_CUDA(run_pending(c));
+    CB_CUDA(launch_mom(c, which_vel, sweep_number, direction, fold, -1));
   }
-  if (which_vel & 2) {
-    std::swap(c->fbuf[YVEL1], c->sbuf[3]);
-    c->halo_fresh[YVEL1] = fold;
-  }
+  if (which_vel & 1) c->halo_fresh[XVEL1] = fold;
+  if (which_vel & 2) c->halo_fresh[YVEL1] = fold;
   return CB_OK;
 }
 
 int cb_reset_field(cb_chunk *c, int halo_depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  CB_CUDA(dispatch(c, [&](auto ops) { return ops.reset_field(*c, fold); }));
+  const Pending held = c->pend;
+  if (held.kind == PEND_CELL2_MOM2) { // the second sweeps, each with reset_field's copy of what it writes
+    c->pend = Pending{};
+    CB_CUDA(launch_cell(c, 2, held.cell_dir, held.cell_fold, fold));
+    CB_CUDA(launch_mom(c, held.mom_mask, 2, held.mom_dir, held.mom_fold, fold));
+  } else {
+    CB_CUDA(run_pending(c));
+    CB_CUDA(dispatch(c, [&](auto ops) { return ops.reset_field(*c, fold); }));
+  }
   c->halo_fresh[DENSITY0] = c->halo_fresh[ENERGY0] = c->halo_fresh[XVEL0] = c->halo_fresh[YVEL0] = fold;
   return CB_OK;
 }
 
 int cb_update_halo(cb_chunk *c, const int fields[15], int depth) {
-  CB_CHECK_CHUNK(c);
+  CB_CHECK_CHUNK_HOLD(c); // a pass with nothing to do leaves held-back calls held back
   if (!fields) return fail(CB_EINVAL, "cb_update_halo: null field list");
   if (int r = check_depth(depth, false)) return r;
   HaloJob job{};
@@ -691,6 +814,7 @@ int cb_update_halo(cb_chunk *c, const int fields[15], int depth) {
     if (c->can_fold() && c->halo_fresh[f] >= depth) continue; // a folded producer already wrote it
     job.field[job.nfields++] = f;
   }
+  if (job.nfields) CB_CUDA(run_pending(c));
   CB_CUDA(dispatch(c, [&](auto ops) { return ops.update_halo(*c, job, depth); }));
   for (int k = 0; k < job.nfields; ++k) c->halo_fresh[job.field[k]] = std::max(c->halo_fresh[job.field[k]], depth);
   return CB_OK;

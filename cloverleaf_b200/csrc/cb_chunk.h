@@ -27,6 +27,21 @@ template <int H> constexpr int box_slot() {
   return s;
 }
 
+// Phase calls held back under call fusion (CB_OPT_FUSE_CALLS): ideal_gas
+// and viscosity wait for calc_dt (then one pass does the three), the PdV
+// predictor, accelerate and the PdV corrector wait for flux_calc (the
+// Lagrangian pass), the second advection sweeps wait for reset_field (which
+// they then do).  Any other call first runs what is held back, as called.
+enum PendKind : int { PEND_NONE = 0, PEND_IG, PEND_IG_VISC, PEND_PDV1, PEND_PDV1_ACC, PEND_PDV1_ACC_PDV0, PEND_CELL2, PEND_CELL2_MOM2 };
+struct Pending {
+  int kind = PEND_NONE;
+  int ig_fold = 0, visc_fold = 0;                  // ideal_gas, viscosity
+  double dt = 0.0;                                 // the Lagrangian calls' dt
+  int pdv1_fold = 0, acc_fold = 0, pdv0_fold = 0;  // predictor (pressure), accelerate, corrector
+  int cell_dir = 0, cell_fold = 0;                 // the second cell sweep
+  int mom_dir = 0, mom_fold = 0, mom_mask = 0;     // the second momentum sweep
+};
+
 struct Chunk {
   int nx = 0, ny = 0;
   int precision = 0; // 0 FP64, 1 FP32
@@ -65,7 +80,8 @@ struct Chunk {
 
   int halo_fresh[15] = {};     // depth to which each field's halo matches update_halo
   bool fold_enabled = true;    // fold halos into producers when the mesh allows it
-  bool reset_by_swap = false;  // reset_field swaps level buffers instead of copying
+  bool fuse_calls = false;     // call fusion (CB_OPT_FUSE_CALLS), with folding producers
+  Pending pend;                // calls held back by call fusion
 
   long long launches = 0; // kernels launched for this chunk
   // When set, the phases that take dt (PdV, accelerate, flux_calc) read it

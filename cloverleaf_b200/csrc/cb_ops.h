@@ -37,8 +37,15 @@ template <typename T> struct Ops {
   static cudaError_t flux_calc(Chunk &c, double dt, int fold);
   // reset_fold >= 0: the sweep also does reset_field's copy of what it writes (fold depth reset_fold)
   static cudaError_t advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de, int reset_fold = -1);
+  // du / dv null (with reset_fold >= 0): the velocities to level 0 only (de null in advec_cell, with
+  // reset_fold >= 0 and fold 2: the energy to level 0 only)
   static cudaError_t advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv, int reset_fold = -1);
   static cudaError_t reset_field(Chunk &c, int fold);
+  // level 1 as the phase-by-phase step leaves it, after steps whose second
+  // sweeps wrote energy and velocities to level 0 only: energy1 from level 0
+  // with its depth-2 halo, xvel1 / yvel1 from level 0 inside and from
+  // (u_ring, v_ring), the first sweep's momentum output, on their halo ring
+  static cudaError_t restore_level1(Chunk &c, const void *u_ring, const void *v_ring);
   static cudaError_t update_halo(Chunk &c, const HaloJob &job, int depth);
   static cudaError_t field_summary(Chunk &c);
   // fused passes of the resident loop: ideal_gas + viscosity + calc_dt, and the Lagrangian step

@@ -186,7 +186,10 @@ template <typename T, int DIR, int TY> cudaError_t launch_advec_cell(Chunk &c, i
 template <typename T> cudaError_t Ops<T>::advec_cell(Chunk &c, int sweep, int dir, int fold, void *dd, void *de, int reset_fold) {
   const T *sd = (const T *)c.base(DENSITY1), *se = (const T *)c.base(ENERGY1);
   cudaError_t e;
-  if (fold != 2) { // keep the halo ring exactly as the in-place reference leaves it
+  if (!dd) return cudaErrorInvalidValue;
+  if (!de) {
+    if (reset_fold < 0 || fold != 2) return cudaErrorInvalidValue; // energy to level 0 only, reset_field's copy done
+  } else if (fold != 2) { // keep the halo ring exactly as the in-place reference leaves it
     RingPair rp{{sd, se}, {dd, de}};
     if ((e = copy_ring<T>(c, rp, 2, 2, c.nx + 1, 2, c.ny + 1, c.nx + 4, c.ny + 4)) != cudaSuccess) return e;
   }
@@ -221,7 +224,9 @@ template <typename T>
 cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv, int reset_fold) {
   const T *su = (const T *)c.base(XVEL1), *sv = (const T *)c.base(YVEL1);
   cudaError_t e;
-  if (fold != 2) {
+  if (!du || !dv) {
+    if (reset_fold < 0 || du || dv) return cudaErrorInvalidValue; // level 0 only: both outputs skipped, reset_field's copy done
+  } else if (fold != 2) {
     RingPair rp{};
     int n = 0;
     if (vel_mask & 1) rp.src[n] = su, rp.dst[n++] = du;
@@ -230,6 +235,19 @@ cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fo
   }
   return dir == 1 ? launch_advec_mom<T, 1, AdvecTiles<T>::MOM_X>(c, vel_mask, sweep, fold, du, dv, reset_fold)
                   : launch_advec_mom<T, 2, AdvecTiles<T>::MOM_Y>(c, vel_mask, sweep, fold, du, dv, reset_fold);
+}
+
+template <typename T> cudaError_t Ops<T>::restore_level1(Chunk &c, const void *u_ring, const void *v_ring) {
+  dim3 b(32, 8);
+  k_level1_from_level0<T><<<dim3((c.nx + 1 + 31) / 32, (c.ny + 1 + 7) / 8), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c));
+  cudaError_t e = launched(c);
+  if (e != cudaSuccess) return e;
+  HaloJob job{};
+  job.nfields = 1;
+  job.field[0] = ENERGY1;
+  if ((e = update_halo(c, job, 2)) != cudaSuccess) return e;
+  RingPair rp{{u_ring, v_ring}, {c.base(XVEL1), c.base(YVEL1)}};
+  return copy_ring<T>(c, rp, 2, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5);
 }
 
 template <typename T> cudaError_t Ops<T>::reset_field(Chunk &c, int fold) {

@@ -310,6 +310,19 @@ __global__ void k_reset_field(Fields<T> F, Mesh<T> m, int fold) {
   reset_field_block(F, m, fold, blockIdx.x, blockIdx.y, threadIdx.x, threadIdx.y);
 }
 
+// The interior of level 1 as the step's last sweeps and reset_field leave it
+// (energy1 = energy0 on cells [2, nx+1] x [2, ny+1]; xvel1 = xvel0, yvel1 =
+// yvel0 on nodes [2, nx+2] x [2, ny+2]): the end of a resident loop whose
+// second sweeps wrote those to level 0 only.  One thread per node.
+template <typename T> __global__ void k_level1_from_level0(Fields<T> F, Mesh<T> m) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x, j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > m.nx + 2 || j > m.ny + 2) return;
+  const long long g = m.at(i, j);
+  F.f[XVEL1][g] = F.f[XVEL0][g];
+  F.f[YVEL1][g] = F.f[YVEL0][g];
+  if (i <= m.nx + 1 && j <= m.ny + 1) F.f[ENERGY1][g] = F.f[ENERGY0][g];
+}
+
 // ---------------------------------------------------------------------------
 // update_halo: src/serial/update_halo.cpp:33-684 in two launches: pass 0 does
 // bottom then top for every column, pass 1 left then right for every row, so

@@ -36,6 +36,8 @@
 
 namespace cb {
 int set_last_error(int code, const std::string &msg);
+// Defined in cb_api.cu: runs the phase calls call fusion holds back.
+cudaError_t run_pending_calls(cb_chunk *c);
 } // namespace cb
 
 using namespace cb;
@@ -244,18 +246,25 @@ template <typename T> struct Seq {
   }
   // fold depth of reset_field, which a fused second sweep does
   int reset_tail(bool last) const { return fuse && last ? eff(dep(1)) : -1; }
-  // cb_advec_cell with its buffer swap
+  // cb_advec_cell with its buffer swap.  A fused second sweep writes the new
+  // energy to energy0 only: energy1 is next read after the following step's
+  // PdV has rewritten it, and the loop restores it at its end
+  // (restore_level1); the swap still renames the buffers, so the body leaves
+  // the buffer map as it found it.
   void cell(int sweep, int dir, bool last = false) {
     const int f = eff(dep(2));
-    if (emit) run(Ops<T>::advec_cell(c, sweep, dir, f, c.spare_base(0), c.spare_base(1), reset_tail(last)));
+    if (emit) run(Ops<T>::advec_cell(c, sweep, dir, f, c.spare_base(0), fuse && last ? nullptr : c.spare_base(1), reset_tail(last)));
     std::swap(c.fbuf[DENSITY1], c.sbuf[0]);
     std::swap(c.fbuf[ENERGY1], c.sbuf[1]);
     wrote({D1, E1, dir == 1 ? MFX : MFY}, f);
   }
-  // cb_advec_mom of both velocities with its buffer swaps
+  // cb_advec_mom of both velocities with its buffer swaps; a fused second
+  // sweep writes the velocities to level 0 only (as the energy above)
   void mom(int sweep, int dir, int depth, bool last = false) {
     const int f = eff(depth);
-    if (emit) run(Ops<T>::advec_mom(c, 3, sweep, dir, f, c.spare_base(2), c.spare_base(3), reset_tail(last)));
+    const bool lvl0 = fuse && last;
+    if (emit)
+      run(Ops<T>::advec_mom(c, 3, sweep, dir, f, lvl0 ? nullptr : c.spare_base(2), lvl0 ? nullptr : c.spare_base(3), reset_tail(last)));
     std::swap(c.fbuf[XVEL1], c.sbuf[2]);
     std::swap(c.fbuf[YVEL1], c.sbuf[3]);
     wrote({U1, V1}, f);
@@ -529,10 +538,20 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
   std::memcpy(c->sbuf, sbuf0, sizeof sbuf0);
   cudaGraphExec_t x = nullptr;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
+  long long restore_launches = 0;
   if (e == cudaSuccess) {
     for (int d = 0; d < 2 && e == cudaSuccess; ++d)
       if (pro[d].nfields) e = Ops<T>::update_halo(*c, pro[d], d + 1);
     if (e == cudaSuccess) e = cudaGraphLaunch(x, c->stream);
+    if (e == cudaSuccess && q.fuse) {
+      // the fused second sweeps left energy1 / xvel1 / yvel1 stale: rebuild
+      // them as the phase-by-phase step leaves them (the last first sweep's
+      // momentum output, in the spares, gives the velocities' halo ring)
+      const long long l = c->launches;
+      e = Ops<T>::restore_level1(*c, c->spare_base(2), c->spare_base(3));
+      restore_launches = c->launches - l;
+      c->launches = l;
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   }
   if (x) cudaGraphExecDestroy(x);
@@ -558,7 +577,7 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
       return cuda_fail(e, "cb_run");
   if (nsummaries) *nsummaries = h.nsum;
   // (the passes before the loop counted themselves)
-  c->launches += 1 + (long long)steps * (n.body + RUN_KERNELS_PER_STEP + n.adv[0]) + (long long)h.sum_runs * (n.sum + 1);
+  c->launches += 1 + (long long)steps * (n.body + RUN_KERNELS_PER_STEP + n.adv[0]) + (long long)h.sum_runs * (n.sum + 1) + restore_launches;
   std::memcpy(c->halo_fresh, settled[3], sizeof c->halo_fresh);
   state->step = h.step;
   state->time = h.time;
@@ -591,6 +610,7 @@ extern "C" int cb_run(cb_chunk *c, const cb_run_params *p, cb_run_state *state, 
   if ((long long)state->step + max_steps > 0x7fffffffll) return fail(CB_EINVAL, "cb_run: the step count overflows");
   cudaError_t e = select_device(c);
   if (e != cudaSuccess) return cuda_fail(e, "cb_run");
+  if ((e = run_pending_calls(c)) != cudaSuccess) return cuda_fail(e, "cb_run");
   if (c->precision == CB_FP64) return run_impl<double>(c, p, state, max_steps, dt_trace, summaries, max_summaries, nsummaries);
   return run_impl<float>(c, p, state, max_steps, dt_trace, summaries, max_summaries, nsummaries);
 }

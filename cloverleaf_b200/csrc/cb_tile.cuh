@@ -1090,7 +1090,10 @@ __device__ __forceinline__ void cell_update_value(S d1, S e1, S pre_vol, S mf_lo
 
 // density0 / energy0 set: the sweep also does reset_field's cell copy
 // (src/serial/reset_field.cpp:33-40) of the values it writes, with its fold
-// depth rfold -- the resident loop's second sweep.
+// depth rfold -- the resident loop's second sweep, which then leaves energy1
+// null: energy1 is not read again before the next step's PdV rewrites it,
+// and the loop restores it once at its end.  (density1 stays: the momentum
+// sweep after it reads its depth-2 halo, which level 0 does not carry.)
 struct CellOut {
   void *density1, *energy1, *mass_flux;
   void *density0 = nullptr, *energy0 = nullptr;
@@ -1225,10 +1228,10 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
     }
     const int g = gidx(pitch, i, j);
     ((T *)out.density1)[g] = dnew;
-    ((T *)out.energy1)[g] = enew;
-    if (edge) {
-      fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, dnew);
-      fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, enew);
+    if (edge) fold_halo((T *)out.density1, m, halo_rule(DENSITY1), fold, i, j, dnew);
+    if (out.energy1) {
+      ((T *)out.energy1)[g] = enew;
+      if (edge) fold_halo((T *)out.energy1, m, halo_rule(ENERGY1), fold, i, j, enew);
     }
     if (out.density0) {
       ((T *)out.density0)[g] = dnew;
@@ -1345,7 +1348,9 @@ template <typename T> __device__ __forceinline__ T mom_update_value(T vel, T nm_
 
 // xvel0 / yvel0 set: the sweep also does reset_field's node copy
 // (src/serial/reset_field.cpp:42-49) of the velocities it writes, with its
-// fold depth rfold -- the resident loop's second sweep.
+// fold depth rfold -- the resident loop's second sweep, which then leaves
+// xvel1 / yvel1 null: level 1 is not read again before the next step's
+// accelerate rewrites it, and the loop restores it once at its end.
 struct MomOut {
   void *xvel1, *yvel1;
   void *xvel0 = nullptr, *yvel0 = nullptr;
@@ -1468,8 +1473,10 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
     const int g = gidx(pitch, i, j);
     if (vel_mask & 1) {
       T v = mom_update_value(U1[b], nmpre, nmpost, s_mfu[L::w(p - 1, l)], s_mfu[L::w(p, l)]);
-      ((T *)out.xvel1)[g] = v;
-      if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
+      if (out.xvel1) {
+        ((T *)out.xvel1)[g] = v;
+        if (do_fold) fold_halo((T *)out.xvel1, m, halo_rule(XVEL1), fold, i, j, v);
+      }
       if (out.xvel0) {
         ((T *)out.xvel0)[g] = v;
         if (EDGE && out.rfold) fold_halo((T *)out.xvel0, m, halo_rule(XVEL0), out.rfold, i, j, v);
@@ -1477,8 +1484,10 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
     }
     if (vel_mask & 2) {
       T v = mom_update_value(V1[b], nmpre, nmpost, s_mfv[L::w(p - 1, l)], s_mfv[L::w(p, l)]);
-      ((T *)out.yvel1)[g] = v;
-      if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
+      if (out.yvel1) {
+        ((T *)out.yvel1)[g] = v;
+        if (do_fold) fold_halo((T *)out.yvel1, m, halo_rule(YVEL1), fold, i, j, v);
+      }
       if (out.yvel0) {
         ((T *)out.yvel0)[g] = v;
         if (EDGE && out.rfold) fold_halo((T *)out.yvel0, m, halo_rule(YVEL0), out.rfold, i, j, v);

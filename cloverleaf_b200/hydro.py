@@ -15,7 +15,7 @@ from __future__ import annotations
 import dataclasses
 from typing import Callable, List, Optional
 
-from .chunk import Chunk, RunParams, RunState
+from .chunk import OPT_FUSE_CALLS, Chunk, RunParams, RunState
 from .deck import G_SMALL, G_BIG, Deck
 
 D0, D1, E0, E1, P, Q, C, U0, U1, V0, V1, VFX, VFY, MFX, MFY = range(15)
@@ -36,10 +36,14 @@ class HydroRun:
     """State of one run: globals.step, time, dt, dtold, advect_x (driver/definitions.h:258-280)."""
 
     def __init__(self, chunk: Chunk, deck: Deck, fold: bool = True, forced_dt: Optional[List[float]] = None,
-                 probe: Optional[Callable[[str], None]] = None, lagrangian: bool = False):
+                 probe: Optional[Callable[[str], None]] = None, lagrangian: bool = False, fuse_calls: bool = False):
         self.c = chunk
         self.deck = deck
         self.fold = fold
+        # fuse_calls: the same calls, with the chunk's call fusion on (the
+        # library runs ideal_gas + viscosity + calc_dt, the four Lagrangian
+        # calls, and the second sweeps + reset_field as its fused passes)
+        chunk.set_option(OPT_FUSE_CALLS, int(fuse_calls))
         # lagrangian: the PdV / accelerate / PdV / flux_calc calls as one cb_lagrangian call
         self.lagrangian = lagrangian
         # forced_dt replays a recorded dt sequence (calc_dt still runs); probe(name)

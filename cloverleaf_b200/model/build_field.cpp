@@ -11,6 +11,7 @@ void build_field(global_variables &globals) {
   const int nx = t.info.t_xmax - t.info.t_xmin + 1, ny = t.info.t_ymax - t.info.t_ymin + 1;
   clover::Runtime &rt = *globals.context.rt;
   if (!rt.chunk) clover::b200_check(cb_create(nx, ny, globals.context.precision, globals.context.device, &rt.chunk), "build_field");
+  clover::b200_check(cb_set_option(rt.chunk, CB_OPT_FUSE_CALLS, rt.fold && rt.fuse ? 1 : 0), "build_field");
   clover::b200_check(cb_build_field(rt.chunk), "build_field");
   field_type &f = t.field;
   cb_chunk *c = rt.chunk;

@@ -6,6 +6,8 @@
 // deck reader are unchanged and reject / ignore unknown options):
 //   CLOVER_B200_PRECISION = fp64 (default) | fp32  storage form
 //   CLOVER_B200_FOLD      = 1 (default) | 0        fold update_halo into producers
+//   CLOVER_B200_FUSE      = 1 (default) | 0        the driver's phase calls as fused passes
+//                                                  (with folding; results unchanged)
 #include "initialise.h"
 #include "b200_runtime.h"
 
@@ -42,6 +44,7 @@ model create_context(bool silent, const std::vector<std::string> &args) {
     }
   }
   if (const char *f = std::getenv("CLOVER_B200_FOLD")) ctx.rt->fold = std::strcmp(f, "0") != 0;
+  if (const char *f = std::getenv("CLOVER_B200_FUSE")) ctx.rt->fuse = std::strcmp(f, "0") != 0;
   return {ctx, "B200 (sm_100a CUDA, libcloverb200)", true, parsed};
 }
 
@@ -50,5 +53,6 @@ void report_context(const clover::context &ctx) {
   cb_device_name(ctx.device, name, sizeof name);
   std::cout << " - Device:    " << name << "\n"
             << " - Precision: " << (ctx.precision == CB_FP64 ? "fp64" : "fp32") << "\n"
-            << " - Halo fold: " << (ctx.rt && ctx.rt->fold ? "on" : "off") << std::endl;
+            << " - Halo fold: " << (ctx.rt && ctx.rt->fold ? "on" : "off") << "\n"
+            << " - Fused calls: " << (ctx.rt && ctx.rt->fold && ctx.rt->fuse ? "on" : "off") << std::endl;
 }

@@ -55,8 +55,21 @@ enum { CB_FP64 = 0, CB_FP32 = 1 };
 /* Host layouts for cb_read_field / cb_write_field: row-major with x fastest,
  * or the reference Buffer2D order data[j + i * sizeY] (src/serial/context.h:73). */
 enum { CB_LAYOUT_XFAST = 0, CB_LAYOUT_YFAST = 1 };
-/* Options for cb_set_option. */
-enum { CB_OPT_FOLD_HALO = 1, CB_OPT_RESET_BY_SWAP = 2 };
+/* Options for cb_set_option.
+ * CB_OPT_FOLD_HALO (default 1): producers write the halo the driver's next
+ *   update_halo asks for, which then has nothing left to do.
+ * CB_OPT_FUSE_CALLS (default 0): with folding on, the phase calls of the
+ *   reference driver's step run as the fused passes of cb_run's fuse = 1 --
+ *   cb_ideal_gas(predict 0) and cb_viscosity are held back until cb_calc_dt,
+ *   which does all three in one pass; cb_pdv(predictor), cb_accelerate and
+ *   cb_pdv(corrector) until cb_flux_calc (one Lagrangian pass, as
+ *   cb_lagrangian); the second sweeps' cb_advec_cell and cb_advec_mom until
+ *   cb_reset_field, which they then do.  Results are those of the calls made
+ *   one by one (FP64 to the bit).  A held-back call's kernels are enqueued
+ *   when its group completes or when any other call on the chunk is made
+ *   (cb_launch_count and cb_get_stream excepted): work enqueued directly on
+ *   the chunk's stream after a held-back call may run before it. */
+enum { CB_OPT_FOLD_HALO = 1, CB_OPT_FUSE_CALLS = 3 };
 /* Error codes. */
 enum { CB_OK = 0, CB_EINVAL = 1, CB_ECUDA = 2, CB_ENOMEM = 3, CB_ESTATE = 4 };
 

@@ -1,7 +1,8 @@
 """The drop-in: the reference's unchanged C++ driver linked against the b200
 model (cloverleaf_b200/bin/clover_leaf) runs the decks and passes the
 driver's own expected-solution check; its full-precision captures equal the
-reference serial build's (fields bit for bit, summaries to 1e-12)."""
+reference serial build's (fields bit for bit, summaries to 1e-12), with the
+model's call fusion on (the default) and off."""
 import os
 import subprocess
 import tempfile
@@ -39,8 +40,10 @@ def run_driver(text, env_extra=None, args=()):
 
 
 @pytest.mark.parametrize("name", SMALL_DECKS)
-def test_driver_matches_reference(name):
-    p, summ, flds = run_driver(deck_text(name))
+@pytest.mark.parametrize("fuse", ["1", "0"])
+def test_driver_matches_reference(name, fuse):
+    """With the driver's phase calls run as fused passes (the default) and one by one."""
+    p, summ, flds = run_driver(deck_text(name), {"CLOVER_B200_FUSE": fuse})
     assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
     gold = summaries(name)
     assert len(summ) == len(gold)

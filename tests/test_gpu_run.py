@@ -201,8 +201,9 @@ def test_run_fused_falls_back(nx, ny, fold):
 
 
 def test_run_fused_launch_count():
-    """Fused, a step launches six kernels fewer: ideal_gas, viscosity, accelerate, the PdV corrector, flux_calc and
-    reset_field run inside others."""
+    """Fused, a step launches seven kernels fewer: ideal_gas, viscosity, accelerate, the PdV corrector, flux_calc and
+    reset_field run inside others, and the second momentum sweep, writing level 0 only, copies no halo ring; once per
+    run, four launches restore energy1, xvel1 and yvel1 (the level-1 values the fused second sweeps skip)."""
     dk = deck_a(48, 48, end_step=12, freq=5)
     counts = []
     for fuse in (False, True):
@@ -212,4 +213,4 @@ def test_run_fused_launch_count():
         n0 = c.launch_count()
         r.run_steps_on_device(fuse=fuse)
         counts.append(c.launch_count() - n0)
-    assert counts[1] == counts[0] - 6 * 12
+    assert counts[1] == counts[0] - 7 * 12 + 4

@@ -68,7 +68,7 @@ def test_noalloc_summary_matches_chunk_summary_twice(nx, ny, steps):
     assert np.array_equal(results[0][2], results[1][2])
 
 
-@pytest.mark.parametrize("nx,ny,blocks", [(2100, 2100, 17292), (2049, 2048, 16640), (2050, 2040, 16575)])
+@pytest.mark.parametrize("nx,ny,blocks", [(2100, 2100, 17358), (2049, 2048, 16640), (2050, 2040, 16575)])
 def test_noalloc_rejects_mesh_beyond_scratch(nx, ny, blocks):
     """A mesh is accepted when ceil(nx/32) * ceil(ny/8) <= 16384: one column
     past 2048 x 2048 is rejected, and so is 2050 x 2040 although it has fewer
