@@ -25,6 +25,7 @@ GEOM_ID = {n: i for i, n in enumerate(GEOM_NAMES)}
 FP64, FP32 = 0, 1
 LAYOUT_XFAST, LAYOUT_YFAST = 0, 1
 OPT_FOLD_HALO, OPT_FUSE_CALLS = 1, 3
+FACE_LEFT, FACE_RIGHT, FACE_BOTTOM, FACE_TOP = 1, 2, 4, 8
 
 # Every symbol include/cloverb200.h declares.
 EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "cb_create", "cb_destroy", "cb_set_gamma", "cb_set_option", "cb_get_extent",
@@ -32,6 +33,7 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_lagrangian", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
            "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_run", "cb_field_summary_noalloc",
+           "cb_set_external_faces", "cb_copy_tile_halo",
            "cb_batch_create", "cb_batch_destroy", "cb_batch_set_schedule", "cb_batch_get_schedule", "cb_batch_autotune",
            "cb_batch_run", "cb_batch_synchronize", "cb_batch_deck_result", "cb_batch_read_summaries", "cb_batch_read_dt",
            "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count",
@@ -103,6 +105,7 @@ def library() -> ctypes.CDLL:
         "cb_run": ([P, ctypes.POINTER(RunParams), ctypes.POINTER(RunState), i, dp, dp, i, ip], i),
         "cb_field_summary_noalloc": ([i, i, ctypes.c_longlong] + [P] * 8 + [d, P, P], i),
         "cb_selftest_width_ratio": ([ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong)], i),
+        "cb_set_external_faces": ([P, i], i), "cb_copy_tile_halo": ([P, P, i, ip, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -110,6 +113,13 @@ def library() -> ctypes.CDLL:
         fn.restype = res
     _lib = L
     return L
+
+
+def _field_flags(fields: Iterable):
+    flags = [0] * 15
+    for f in fields:
+        flags[FIELD_ID[f] if isinstance(f, str) else int(f)] = 1
+    return (ctypes.c_int * 15)(*flags)
 
 
 def _check(rc: int):
@@ -244,11 +254,16 @@ class Chunk:
     def reset_field(self, halo_depth: int = 0): _check(self._L.cb_reset_field(self._h, halo_depth))
 
     def update_halo(self, fields: Iterable, depth: int):
-        flags = [0] * 15
-        for f in fields:
-            flags[FIELD_ID[f] if isinstance(f, str) else int(f)] = 1
-        arr = (ctypes.c_int * 15)(*flags)
-        _check(self._L.cb_update_halo(self._h, arr, depth))
+        _check(self._L.cb_update_halo(self._h, _field_flags(fields), depth))
+
+    # ---- tiles (driver/update_tile_halo.cpp)
+    def set_external_faces(self, faces: int):
+        """Faces on the physical boundary (FACE_* bits); the others border tiles."""
+        _check(self._L.cb_set_external_faces(self._h, int(faces)))
+
+    def copy_tile_halo(self, src: "Chunk", side: int, fields: Iterable, depth: int):
+        """This chunk's halo on `side` (one FACE_* value) from `src`, the tile on that side."""
+        _check(self._L.cb_copy_tile_halo(self._h, src._h, int(side), _field_flags(fields), depth))
 
     def field_summary(self) -> Tuple[float, float, float, float, float]:
         out = (ctypes.c_double * 5)()

@@ -198,6 +198,8 @@ void release(cb_chunk *c) {
   if (c->d_sums) cudaFree(c->d_sums);
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_scalars) cudaFreeHost(c->h_scalars);
+  if (c->ev_order) cudaEventDestroy(c->ev_order);
+  c->ev_order = nullptr;
   if (c->stream) cudaStreamDestroy(c->stream);
   c->d_dt_bits = nullptr;
   c->d_partials = nullptr;
@@ -369,6 +371,7 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
     return cuda_fail(err, "cb_create");
   };
   if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+  if ((e = cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
   for (int b = 0; b < NUM_BUF; ++b)
     if ((e = cudaMalloc(&c->buf[b], bytes)) != cudaSuccess) return bail(e, "fields");
   for (int f = 0; f < 15; ++f) c->fbuf[f] = f;
@@ -817,6 +820,41 @@ int cb_update_halo(cb_chunk *c, const int fields[15], int depth) {
   if (job.nfields) CB_CUDA(run_pending(c));
   CB_CUDA(dispatch(c, [&](auto ops) { return ops.update_halo(*c, job, depth); }));
   for (int k = 0; k < job.nfields; ++k) c->halo_fresh[job.field[k]] = std::max(c->halo_fresh[job.field[k]], depth);
+  return CB_OK;
+}
+
+int cb_set_external_faces(cb_chunk *c, int faces) {
+  CB_CHECK_CHUNK(c);
+  if (faces < 0 || faces > 15) return fail(CB_EINVAL, "cb_set_external_faces: faces must be a mask of CB_FACE_* bits (0..15)");
+  c->external_faces = faces;
+  std::fill(std::begin(c->halo_fresh), std::end(c->halo_fresh), 0); // what the producers folded no longer applies
+  return CB_OK;
+}
+
+int cb_copy_tile_halo(cb_chunk *dst, cb_chunk *src, int side, const int fields[15], int depth) {
+  CB_CHECK_CHUNK(dst);
+  if (!src || !fields) return fail(CB_EINVAL, "cb_copy_tile_halo: null argument");
+  if (src == dst) return fail(CB_EINVAL, "cb_copy_tile_halo: a tile is not its own neighbour");
+  if (src->device != dst->device || src->precision != dst->precision)
+    return fail(CB_EINVAL, "cb_copy_tile_halo: the tiles must share a device and a precision");
+  if (side != CB_FACE_LEFT && side != CB_FACE_RIGHT && side != CB_FACE_BOTTOM && side != CB_FACE_TOP)
+    return fail(CB_EINVAL, "cb_copy_tile_halo: side must be one CB_FACE_* value");
+  if (int r = check_depth(depth, false)) return r;
+  const bool lr = side == CB_FACE_LEFT || side == CB_FACE_RIGHT;
+  if (lr ? src->ny != dst->ny : src->nx != dst->nx)
+    return fail(CB_EINVAL, "cb_copy_tile_halo: neighbouring tiles must share their extent along the common face");
+  CB_CUDA(run_pending(src));
+  HaloJob job{};
+  for (int f = 0; f < 15; ++f)
+    if (fields[f] == 1) job.field[job.nfields++] = f;
+  if (job.nfields == 0) return CB_OK;
+  // the copy comes after src's work so far and before its later work (each chunk has its own stream)
+  CB_CUDA(cudaEventRecord(src->ev_order, src->stream));
+  CB_CUDA(cudaStreamWaitEvent(dst->stream, src->ev_order, 0));
+  CB_CUDA(dispatch(dst, [&](auto ops) { return ops.tile_halo(*dst, *src, side, job, depth); }));
+  CB_CUDA(cudaEventRecord(dst->ev_order, dst->stream));
+  CB_CUDA(cudaStreamWaitEvent(src->stream, dst->ev_order, 0));
+  for (int k = 0; k < job.nfields; ++k) dst->halo_fresh[job.field[k]] = 0;
   return CB_OK;
 }
 

@@ -79,6 +79,8 @@ struct Chunk {
   int sms = 148;
 
   int halo_fresh[15] = {};     // depth to which each field's halo matches update_halo
+  int external_faces = 15;     // faces on the physical boundary (CB_FACE_* bits): the reflective fill's faces
+  cudaEvent_t ev_order = nullptr; // orders a tile-halo copy between two chunks' streams
   bool fold_enabled = true;    // fold halos into producers when the mesh allows it
   bool fuse_calls = false;     // call fusion (CB_OPT_FUSE_CALLS), with folding producers
   Pending pend;                // calls held back by call fusion
@@ -88,7 +90,8 @@ struct Chunk {
   // from this device address instead of their argument (cb_run's graph).
   const double *dt_dev = nullptr;
 
-  bool can_fold() const { return fold_enabled && nx >= 8 && ny >= 8; }
+  // folding writes reflected halos, so it needs every face on the physical boundary
+  bool can_fold() const { return fold_enabled && nx >= 8 && ny >= 8 && external_faces == 15; }
   void *base(int f) const { return (char *)buf[fbuf[f]] + off * esize; }
   void *spare_base(int s) const { return (char *)buf[sbuf[s]] + off * esize; }
   template <int H> const CUtensorMap *map(int f) const { return &tmap[fbuf[f]][box_slot<H>()]; }

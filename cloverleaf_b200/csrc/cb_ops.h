@@ -46,7 +46,11 @@ template <typename T> struct Ops {
   // with its depth-2 halo, xvel1 / yvel1 from level 0 inside and from
   // (u_ring, v_ring), the first sweep's momentum output, on their halo ring
   static cudaError_t restore_level1(Chunk &c, const void *u_ring, const void *v_ring);
+  // the reflective fill on the chunk's external faces (c.external_faces)
   static cudaError_t update_halo(Chunk &c, const HaloJob &job, int depth);
+  // one strip of driver/update_tile_halo.cpp: dst's halo on `side` (CB_FACE_*) from the
+  // interior of src, the neighbouring tile on that side; enqueued on dst's stream
+  static cudaError_t tile_halo(Chunk &dst, const Chunk &src, int side, const HaloJob &job, int depth);
   static cudaError_t field_summary(Chunk &c);
   // fused passes of the resident loop: ideal_gas + viscosity + calc_dt, and the Lagrangian step
   static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold);

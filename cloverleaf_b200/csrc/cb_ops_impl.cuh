@@ -261,11 +261,19 @@ template <typename T> cudaError_t Ops<T>::update_halo(Chunk &c, const HaloJob &j
   const int len = std::max(c.nx, c.ny) + 5 + 2 * depth;
   dim3 g((len + 127) / 128, job.nfields);
   for (int pass = 0; pass < 2; ++pass) {
-    k_update_halo<T><<<g, 128, 0, c.stream>>>(fields<T>(c), mesh<T>(c), job, depth, pass);
+    k_update_halo<T><<<g, 128, 0, c.stream>>>(fields<T>(c), mesh<T>(c), job, depth, pass, c.external_faces);
     cudaError_t e = launched(c);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+template <typename T> cudaError_t Ops<T>::tile_halo(Chunk &dst, const Chunk &src, int side, const HaloJob &job, int depth) {
+  if (job.nfields == 0) return cudaSuccess;
+  const int n = std::max(dst.nx, dst.ny) + 2 * depth + 1;
+  dim3 g((n * depth + 127) / 128, job.nfields);
+  k_tile_halo<T><<<g, 128, 0, dst.stream>>>(fields<T>(dst), mesh<T>(dst), fields<T>(src), mesh<T>(src), job, side, depth);
+  return launched(dst);
 }
 
 template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold) {

@@ -328,31 +328,77 @@ template <typename T> __global__ void k_level1_from_level0(Fields<T> F, Mesh<T> 
 // bottom then top for every column, pass 1 left then right for every row, so
 // corner and tiny-mesh semantics are the reference's exactly.
 // Column (pass 0) or row (pass 1) t of field f's halo fill.
+// Only the faces in `faces` (bits 1 left, 2 right, 4 bottom, 8 top) are
+// filled: a tile's faces that border another tile get that tile's values
+// instead (k_tile_halo), as the reference fills only faces whose chunk and
+// tile neighbours are both external (src/serial/update_halo.cpp:41-71).
 template <typename T>
-__device__ __forceinline__ void halo_fill(const Fields<T> &F, const Mesh<T> &m, int f, int depth, int pass, int t) {
+__device__ __forceinline__ void halo_fill(const Fields<T> &F, const Mesh<T> &m, int f, int depth, int pass, int t, int faces = 15) {
   const HaloRule r = halo_rule(f);
   T *a = F.f[f];
   const int d = depth;
   if (pass == 0) {
     const int jcol = 2 - d + t;
     if (jcol >= m.nx + r.xe + d + 2) return;
-    for (int k = 0; k < d; ++k) {
-      int src = r.soundspeed_bottom_quirk ? k : r.bot_src + k;
-      a[m.at(jcol, 1 - k)] = (T)(r.sign_bt * (double)a[m.at(jcol, src)]);
-    }
-    for (int k = 0; k < d; ++k) a[m.at(jcol, m.ny + r.top_dst + k)] = (T)(r.sign_bt * (double)a[m.at(jcol, m.ny + r.top_src - k)]);
+    if (faces & 4)
+      for (int k = 0; k < d; ++k) {
+        int src = r.soundspeed_bottom_quirk ? k : r.bot_src + k;
+        a[m.at(jcol, 1 - k)] = (T)(r.sign_bt * (double)a[m.at(jcol, src)]);
+      }
+    if (faces & 8)
+      for (int k = 0; k < d; ++k) a[m.at(jcol, m.ny + r.top_dst + k)] = (T)(r.sign_bt * (double)a[m.at(jcol, m.ny + r.top_src - k)]);
   } else {
     const int krow = 2 - d + t;
     if (krow >= m.ny + r.ye + d + 2) return;
-    for (int k = 0; k < d; ++k) a[m.at(1 - k, krow)] = (T)(r.sign_lr * (double)a[m.at(r.left_src + k, krow)]);
-    for (int k = 0; k < d; ++k) a[m.at(m.nx + r.right_dst + k, krow)] = (T)(r.sign_lr * (double)a[m.at(m.nx + r.right_src - k, krow)]);
+    if (faces & 1)
+      for (int k = 0; k < d; ++k) a[m.at(1 - k, krow)] = (T)(r.sign_lr * (double)a[m.at(r.left_src + k, krow)]);
+    if (faces & 2)
+      for (int k = 0; k < d; ++k) a[m.at(m.nx + r.right_dst + k, krow)] = (T)(r.sign_lr * (double)a[m.at(m.nx + r.right_src - k, krow)]);
   }
 }
 
 template <typename T>
-__global__ void k_update_halo(Fields<T> F, Mesh<T> m, HaloJob job, int depth, int pass) {
+__global__ void k_update_halo(Fields<T> F, Mesh<T> m, HaloJob job, int depth, int pass, int faces) {
   if ((int)blockIdx.y >= job.nfields) return;
-  halo_fill(F, m, job.field[blockIdx.y], depth, pass, blockIdx.x * blockDim.x + threadIdx.x);
+  halo_fill(F, m, job.field[blockIdx.y], depth, pass, blockIdx.x * blockDim.x + threadIdx.x, faces);
+}
+
+// ---------------------------------------------------------------------------
+// Tile halo exchange: src/serial/update_tile_halo_kernel.cpp.  The halo of
+// `dst` on one side, `depth` deep, from the interior of `src`, the tile on
+// that side (they share the extent along the strip).  Along the strip the
+// copy runs over [2 - depth, n + depth + 1], one element further for the
+// arrays that extend one past the cells that way (nodes; y faces for a left /
+// right strip, x faces for a bottom / top one).  Across it, element k of the
+// halo (k = 0 nearest the interior):
+//   left   dst(1 - k, .)              <- src(src.nx + 1 - k, .)
+//   right  dst(nx + 2 + e + k, .)     <- src(2 + e + k, .)      e = 1 for nodes and x faces
+//   bottom dst(., 1 - k)              <- src(., src.ny + 1 - k)
+//   top    dst(., ny + 2 + e + k)     <- src(., 2 + e + k)      e = 1 for nodes and y faces
+// One thread per (strip position, k), blockIdx.y the field.
+template <typename T>
+__global__ void k_tile_halo(Fields<T> D, Mesh<T> md, Fields<T> S, Mesh<T> ms, HaloJob job, int side, int depth) {
+  if ((int)blockIdx.y >= job.nfields) return;
+  const int f = job.field[blockIdx.y];
+  const Kind kd = kind_of(f);
+  const bool lr = side == 1 || side == 2;
+  const int along_extra = lr ? (kd == VERTEX || kd == YFACE) : (kd == VERTEX || kd == XFACE);
+  const int across_extra = lr ? (kd == VERTEX || kd == XFACE) : (kd == VERTEX || kd == YFACE);
+  const int n_along = (lr ? md.ny : md.nx) + 2 * depth + along_extra; // positions 2 - depth .. n + depth + 1 (+1)
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_along * depth) return;
+  const int p = 2 - depth + t % n_along, k = t / n_along;
+  int di, dj, si, sj;
+  if (side == 1) {
+    di = 1 - k, si = ms.nx + 1 - k, dj = sj = p;
+  } else if (side == 2) {
+    di = md.nx + 2 + across_extra + k, si = 2 + across_extra + k, dj = sj = p;
+  } else if (side == 4) {
+    dj = 1 - k, sj = ms.ny + 1 - k, di = si = p;
+  } else {
+    dj = md.ny + 2 + across_extra + k, sj = 2 + across_extra + k, di = si = p;
+  }
+  D.f[f][md.at(di, dj)] = S.f[f][ms.at(si, sj)];
 }
 
 // ---------------------------------------------------------------------------

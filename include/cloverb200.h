@@ -70,6 +70,8 @@ enum { CB_LAYOUT_XFAST = 0, CB_LAYOUT_YFAST = 1 };
  *   (cb_launch_count and cb_get_stream excepted): work enqueued directly on
  *   the chunk's stream after a held-back call may run before it. */
 enum { CB_OPT_FOLD_HALO = 1, CB_OPT_FUSE_CALLS = 3 };
+/* Faces of a chunk (cb_set_external_faces, cb_copy_tile_halo). */
+enum { CB_FACE_LEFT = 1, CB_FACE_RIGHT = 2, CB_FACE_BOTTOM = 4, CB_FACE_TOP = 8 };
 /* Error codes. */
 enum { CB_OK = 0, CB_EINVAL = 1, CB_ECUDA = 2, CB_ENOMEM = 3, CB_ESTATE = 4 };
 
@@ -158,6 +160,22 @@ int cb_update_halo(cb_chunk *c, const int fields[15], int depth);
 /* driver/field_summary.h:25 -- ideal_gas then volume, mass, internal energy,
  * kinetic energy, pressure*volume sums, reduced on the device. */
 int cb_field_summary(cb_chunk *c, double out[5]);
+
+/* Tiles (tiles_per_chunk > 1): each tile of the reference's chunk is its own
+ * cb_chunk.  cb_set_external_faces marks which faces of a chunk lie on the
+ * physical boundary (CB_FACE_* bits, default all four): cb_update_halo's
+ * reflective fill writes those faces only, as update_halo_kernel fills the
+ * faces whose chunk and tile neighbours are both external
+ * (src/serial/update_halo.cpp:41-71); with any face internal, producers do
+ * not fold halos.  cb_copy_tile_halo fills dst's halo on `side` (one
+ * CB_FACE_* value) from src, the neighbouring tile on that side, for the
+ * listed fields (fields[f] == 1) to `depth` -- one of the four
+ * update_tile_halo_{l,r,b,t}_kernel calls of driver/update_tile_halo.cpp:27-91
+ * (driver/update_tile_halo_kernel.h:25-86; index rules of
+ * src/serial/update_tile_halo_kernel.cpp).  The copy is ordered after the
+ * work already enqueued for both chunks and before any work enqueued later. */
+int cb_set_external_faces(cb_chunk *c, int faces);
+int cb_copy_tile_halo(cb_chunk *dst, cb_chunk *src, int side, const int fields[15], int depth);
 /* Waits for everything enqueued on the chunk. */
 int cb_synchronize(cb_chunk *c);
 /* The CUDA stream (a cudaStream_t) the chunk's work is enqueued on, for

@@ -645,7 +645,12 @@ static halo_rule rule_for(int field) {
   return r;
 }
 
-void oc_update_halo(oc_chunk *c, const int fields[15], int depth) {
+void oc_update_halo(oc_chunk *c, const int fields[15], int depth) { oc_update_halo_faces(c, fields, depth, 15); }
+
+/* The same fill on the faces in `faces` only (bits 1 left, 2 right, 4 bottom,
+ * 8 top): update_halo_kernel fills a face when the chunk's and the tile's
+ * neighbours on it are both external (src/serial/update_halo.cpp:41-71). */
+void oc_update_halo_faces(oc_chunk *c, const int fields[15], int depth, int faces) {
   const int sx = c->sx;
   const int x_max = c->nx, y_max = c->ny;
   for (int f = 0; f < 15; ++f) {
@@ -653,25 +658,68 @@ void oc_update_halo(oc_chunk *c, const int fields[15], int depth) {
     halo_rule r = rule_for(f);
     double *a = c->f[f];
     /* bottom then top over j in [x_min - depth, x_max + xe + depth] (C: 2-depth .. x_max+1+xe+depth) */
-    for (int j = 2 - depth; j < x_max + r.xe + depth + 2; j++) {
+    if (faces & 4)
+      for (int j = 2 - depth; j < x_max + r.xe + depth + 2; j++) {
+        for (int k = 0; k < depth; ++k) {
+          int src = r.soundspeed_quirk ? k : r.bot_src + k;
+          AT(a, j, 1 - k) = r.sign_bt * AT(a, j, src);
+        }
+      }
+    if (faces & 8)
+      for (int j = 2 - depth; j < x_max + r.xe + depth + 2; j++) {
+        for (int k = 0; k < depth; ++k) {
+          AT(a, j, y_max + r.top_dst + k) = r.sign_bt * AT(a, j, y_max + r.top_src - k);
+        }
+      }
+    if (faces & 1)
+      for (int k = 2 - depth; k < y_max + r.ye + depth + 2; k++) {
+        for (int j = 0; j < depth; ++j) {
+          AT(a, 1 - j, k) = r.sign_lr * AT(a, r.left_src + j, k);
+        }
+      }
+    if (faces & 2)
+      for (int k = 2 - depth; k < y_max + r.ye + depth + 2; k++) {
+        for (int j = 0; j < depth; ++j) {
+          AT(a, x_max + r.right_dst + j, k) = r.sign_lr * AT(a, x_max + r.right_src - j, k);
+        }
+      }
+  }
+}
+
+/* One of update_tile_halo_{l,r,b,t}_kernel (src/serial/update_tile_halo_kernel.cpp,
+ * called from driver/update_tile_halo.cpp:27-91): dst's halo on `side` (1 left,
+ * 2 right, 4 bottom, 8 top) from src, the tile on that side, for the listed
+ * fields, `depth` deep.  Tile-local indices (x_min = y_min = 1, C index = that
+ * + 1).  Along the strip the loops run over [x_min - depth, x_max + depth]
+ * (one further for nodes, and for the faces that extend that way: y faces on
+ * a left/right strip, x faces on a bottom/top one -- the rule's ye / xe);
+ * across it, the halo element k of dst takes src's k-th interior element from
+ * the shared face, one further in for nodes and the faces normal to the strip
+ * on the right and top sides (the rule's xe / ye). */
+void oc_tile_halo(oc_chunk *dst, const oc_chunk *src, int side, const int fields[15], int depth) {
+  const size_t dsx = (size_t)dst->sx, ssx = (size_t)src->sx;
+  for (int f = 0; f < 15; ++f) {
+    if (fields[f] != 1) continue;
+    const halo_rule r = rule_for(f);
+    double *d = dst->f[f];
+    const double *s = src->f[f];
+    if (side == 1 || side == 2) {
+      for (int k = 2 - depth; k < dst->ny + r.ye + depth + 2; k++) {
+        for (int j = 0; j < depth; ++j) {
+          if (side == 1) /* left: density0(x_min - j, k) = left_density0(left_xmax + 1 - j, k) */
+            d[(size_t)k * dsx + (size_t)(1 - j)] = s[(size_t)k * ssx + (size_t)(src->nx + 1 - j)];
+          else /* right: density0(x_max + 2 + j, k) = right_density0(right_xmin - 1 + 2 + j, k); +1 for xvel / x faces */
+            d[(size_t)k * dsx + (size_t)(dst->nx + 2 + r.xe + j)] = s[(size_t)k * ssx + (size_t)(2 + r.xe + j)];
+        }
+      }
+    } else {
       for (int k = 0; k < depth; ++k) {
-        int src = r.soundspeed_quirk ? k : r.bot_src + k;
-        AT(a, j, 1 - k) = r.sign_bt * AT(a, j, src);
-      }
-    }
-    for (int j = 2 - depth; j < x_max + r.xe + depth + 2; j++) {
-      for (int k = 0; k < depth; ++k) {
-        AT(a, j, y_max + r.top_dst + k) = r.sign_bt * AT(a, j, y_max + r.top_src - k);
-      }
-    }
-    for (int k = 2 - depth; k < y_max + r.ye + depth + 2; k++) {
-      for (int j = 0; j < depth; ++j) {
-        AT(a, 1 - j, k) = r.sign_lr * AT(a, r.left_src + j, k);
-      }
-    }
-    for (int k = 2 - depth; k < y_max + r.ye + depth + 2; k++) {
-      for (int j = 0; j < depth; ++j) {
-        AT(a, x_max + r.right_dst + j, k) = r.sign_lr * AT(a, x_max + r.right_src - j, k);
+        for (int j = 2 - depth; j < dst->nx + r.xe + depth + 2; j++) {
+          if (side == 4) /* bottom: density0(j, y_min - k) = bottom_density0(j, bottom_ymax + 1 - k) */
+            d[(size_t)(1 - k) * dsx + (size_t)j] = s[(size_t)(src->ny + 1 - k) * ssx + (size_t)j];
+          else /* top: density0(j, y_max + 2 + k) = top_density0(j, top_ymin - 1 + 2 + k); +1 for yvel / y faces */
+            d[(size_t)(dst->ny + 2 + r.ye + k) * dsx + (size_t)j] = s[(size_t)(2 + r.ye + k) * ssx + (size_t)j];
+        }
       }
     }
   }

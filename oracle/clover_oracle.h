@@ -99,6 +99,8 @@ void oc_advec_cell(oc_chunk *c, int sweep_number, int dir);
 void oc_advec_mom(oc_chunk *c, int which_vel, int sweep_number, int direction);
 void oc_reset_field(oc_chunk *c);
 void oc_update_halo(oc_chunk *c, const int fields[15], int depth);
+void oc_update_halo_faces(oc_chunk *c, const int fields[15], int depth, int faces); /* :41-71, faces masked */
+void oc_tile_halo(oc_chunk *dst, const oc_chunk *src, int side, const int fields[15], int depth); /* update_tile_halo_kernel.cpp */
 void oc_field_summary(oc_chunk *c, double out[5]);
 /* The same sums in exactly rounded form (per-cell terms identical, sum with
  * a double-double accumulator): the order-free value of the five sums. */

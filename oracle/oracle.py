@@ -83,6 +83,8 @@ def lib():
             fn.restype = None
         L.oc_generate_chunk.argtypes = [P, i, ctypes.POINTER(_State)]
         L.oc_update_halo.argtypes = [P, ctypes.POINTER(ctypes.c_int), i]
+        L.oc_update_halo_faces.argtypes = [P, ctypes.POINTER(ctypes.c_int), i, i]
+        L.oc_tile_halo.argtypes = [P, P, i, ctypes.POINTER(ctypes.c_int), i]
         L.oc_field_summary.argtypes = [P, ctypes.POINTER(d)]
         L.oc_field_summary_exact.argtypes = [P, ctypes.POINTER(d)]
         ip = ctypes.POINTER(i)
@@ -150,9 +152,18 @@ class OracleChunk:
     def reset_field(self): self._L.oc_reset_field(self._c)
     def advection(self, advect_x): self._L.oc_advection(self._c, int(advect_x))
 
-    def update_halo(self, fields, depth):
+    def update_halo(self, fields, depth, faces=15):
+        """fields: 15 flags; faces: the external faces filled (1 left, 2 right, 4 bottom, 8 top)."""
         arr = (ctypes.c_int * 15)(*[1 if f else 0 for f in fields])
-        self._L.oc_update_halo(self._c, arr, depth)
+        if faces == 15:
+            self._L.oc_update_halo(self._c, arr, depth)
+        else:
+            self._L.oc_update_halo_faces(self._c, arr, depth, faces)
+
+    def tile_halo(self, src, side, fields, depth):
+        """This tile's halo on `side` from `src` (update_tile_halo_kernel.cpp); fields: 15 flags."""
+        arr = (ctypes.c_int * 15)(*[1 if f else 0 for f in fields])
+        self._L.oc_tile_halo(self._c, src._c, side, arr, depth)
 
     def calc_dt(self, dtmin=0.0000001, dtc_safe=0.7, dtu_safe=0.5, dtv_safe=0.5, dtdiv_safe=0.7):
         a, b, c_, s = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

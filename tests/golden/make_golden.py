@@ -7,11 +7,17 @@ of decks and stores, per deck:
   <name>.summary.txt   every field_summary at full precision (step time vol mass ie ke press)
   <name>.fields.bin    the final interior fields (CLVF format, small decks only)
   <name>.stdout.txt    the lines of the reference's stdout that carry the verdict
+and, for the dump deck, the reference's --dump output of driver/shared.cpp:96-189 as
+  <name>.dump.sha256   one line per dump file: its name and the sha256 of its
+                       text with the work_array blocks removed (dump_filter.py)
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref/serial-capture)
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref/serial-capture and oracle/_ref/serial)
 """
+import hashlib
 import os
+import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
@@ -55,7 +61,36 @@ def decks():
     return out
 
 
+def dump_deck():
+    """16 x 12 cells, a rectangle and a moving circle, 3 steps."""
+    c = D.benchmark_deck(16, 3, ny=12)
+    c.states.append(D.State(density=2.0, energy=3.0, xvel=0.5, yvel=-0.25, geometry=D.GEOM_CIRC, xmin=6.0, ymin=6.0,
+                            radius=2.5, defined=True))
+    return "circ16x12x3", D.format_deck(c)
+
+
+def write_dump_fixture():
+    from dump_filter import filtered
+    name, text = dump_deck()
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "clover.in"), "w") as f:
+            f.write(text)
+        p = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "serial"), "--file", "clover.in", "--dump", "dumps"], cwd=tmp,
+                           capture_output=True, text=True, timeout=600)
+        if p.returncode != 0:
+            raise SystemExit(f"{name}: reference exited {p.returncode}")
+        files = sorted(os.listdir(os.path.join(tmp, "dumps")))
+        with open(os.path.join(HERE, name + ".in"), "w") as f:
+            f.write(text)
+        with open(os.path.join(HERE, name + ".dump.sha256"), "w") as f:
+            for fn in files:
+                body = filtered(open(os.path.join(tmp, "dumps", fn)).read())
+                f.write(f"{fn} {hashlib.sha256(body.encode()).hexdigest()}\n")
+    print(name, len(files), "dump files")
+
+
 def main():
+    write_dump_fixture()
     for name, (text, keep_fields) in decks().items():
         res = oracle.run_reference(text)
         if res["returncode"] != 0:

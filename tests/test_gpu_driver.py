@@ -3,8 +3,10 @@ model (cloverleaf_b200/bin/clover_leaf) runs the decks and passes the
 driver's own expected-solution check; its full-precision captures equal the
 reference serial build's (fields bit for bit, summaries to 1e-12), with the
 model's call fusion on (the default) and off."""
+import hashlib
 import os
 import subprocess
+import sys
 import tempfile
 
 import numpy as np
@@ -12,7 +14,10 @@ import pytest
 
 import oracle
 from cloverleaf_b200 import deck as D
-from golden_util import CAPTURED, SMALL_DECKS, deck_text, fields, rel, summaries
+from golden_util import CAPTURED, GOLDEN, SMALL_DECKS, deck_text, fields, rel, summaries
+
+sys.path.insert(0, GOLDEN)
+from dump_filter import filtered, parse_arrays  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -80,3 +85,43 @@ def test_driver_config1_960_passes():
     for s, g in zip(summ, gold):
         for a, b in zip(s[2:], g[2:]):
             assert rel(a, b) <= 5e-11
+
+
+def run_driver_dump(text, env_extra):
+    assert os.path.exists(EXE), "driver binary not built (make -C cloverleaf_b200/model)"
+    with tempfile.TemporaryDirectory() as tmp:
+        open(os.path.join(tmp, "clover.in"), "w").write(text)
+        env = dict(os.environ, **env_extra)
+        p = subprocess.run([EXE, "--file", "clover.in", "--dump", "dumps"], cwd=tmp, env=env, capture_output=True, text=True,
+                           timeout=600)
+        d = os.path.join(tmp, "dumps")
+        dumps = {fn: open(os.path.join(d, fn)).read() for fn in os.listdir(d)} if os.path.isdir(d) else {}
+    return p, dumps
+
+
+def test_driver_dump_matches_reference():
+    """--dump (driver/shared.cpp:96-189: the driver's globals and every array
+    of the tile after each phase, 27 files for 3 steps).  With every
+    update_halo run as called (CLOVER_B200_FOLD=0) the dumps equal the
+    reference serial build's byte for byte once the work-array blocks are
+    dropped (phase scratch the b200 model keeps on chip; it reports zeros).
+    With folding and call fusion on (the defaults) a producer writes its halo
+    before the update_halo that would, so between phases halo elements may
+    already hold their next values; every array's interior is the same."""
+    text = deck_text("circ16x12x3")
+    gold = dict(line.split() for line in open(os.path.join(GOLDEN, "circ16x12x3.dump.sha256")))
+    p0, d0 = run_driver_dump(text, {"CLOVER_B200_FOLD": "0"})
+    assert p0.returncode == 0, p0.stdout[-2000:]
+    assert sorted(d0) == sorted(gold)
+    for fn, t in d0.items():
+        assert hashlib.sha256(filtered(t).encode()).hexdigest() == gold[fn], fn
+    p1, d1 = run_driver_dump(text, {})
+    assert p1.returncode == 0, p1.stdout[-2000:]
+    assert sorted(d1) == sorted(gold)
+    for fn in sorted(d1):
+        a0, a1 = parse_arrays(d0[fn]), parse_arrays(d1[fn])
+        assert sorted(a0) == sorted(a1), fn
+        for name in a0:
+            if name.startswith("work_array"):
+                continue
+            assert np.array_equal(a0[name][2:-2, 2:-2], a1[name][2:-2, 2:-2]), (fn, name)
