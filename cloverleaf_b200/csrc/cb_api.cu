@@ -112,6 +112,20 @@ cudaError_t launch_mom(cb_chunk *c, int which_vel, int sweep, int dir, int fold,
   return cudaSuccess;
 }
 
+bool x_fusable(const cb_chunk *c) { return c->precision == CB_FP64 ? Ops<double>::sweep_x_fusable(*c) : Ops<float>::sweep_x_fusable(*c); }
+
+// An x sweep, cell and momentum parts, as one pass (with reset_field's copy
+// when reset_fold >= 0), and the buffer swaps of both parts.
+cudaError_t launch_sweep_x(cb_chunk *c, int sweep, int cell_fold, int mom_fold, int reset_fold) {
+  cudaError_t e = dispatch(c, [&](auto ops) { return ops.advec_sweep_x(*c, sweep, cell_fold, mom_fold, reset_fold, false); });
+  if (e != cudaSuccess) return e;
+  std::swap(c->fbuf[DENSITY1], c->sbuf[0]);
+  std::swap(c->fbuf[ENERGY1], c->sbuf[1]);
+  std::swap(c->fbuf[XVEL1], c->sbuf[2]);
+  std::swap(c->fbuf[YVEL1], c->sbuf[3]);
+  return cudaSuccess;
+}
+
 // Runs the calls call fusion held back, one by one as they were made.
 cudaError_t run_pending(cb_chunk *c) {
   const Pending p = c->pend;
@@ -133,10 +147,10 @@ cudaError_t run_pending(cb_chunk *c) {
       if (p.kind != PEND_PDV1) go([&](auto ops) { return ops.accelerate(*c, p.dt, p.acc_fold); });
       if (p.kind == PEND_PDV1_ACC_PDV0) go([&](auto ops) { return ops.pdv(*c, 0, p.dt, 0, p.pdv0_fold); });
       break;
-    case PEND_CELL2:
-    case PEND_CELL2_MOM2:
-      e = launch_cell(c, 2, p.cell_dir, p.cell_fold, -1);
-      if (e == cudaSuccess && p.kind == PEND_CELL2_MOM2) e = launch_mom(c, p.mom_mask, 2, p.mom_dir, p.mom_fold, -1);
+    case PEND_CELL:
+    case PEND_CELL_MOM:
+      e = launch_cell(c, p.cell_sweep, p.cell_dir, p.cell_fold, -1);
+      if (e == cudaSuccess && p.kind == PEND_CELL_MOM) e = launch_mom(c, p.mom_mask, p.cell_sweep, p.cell_dir, p.mom_fold, -1);
       break;
     default: break;
   }
@@ -757,8 +771,10 @@ int cb_advec_cell(cb_chunk *c, int sweep_number, int direction, int halo_depth) 
   if (direction != 1 && direction != 2) return fail(CB_EINVAL, "cb_advec_cell: direction must be 1 (x) or 2 (y)");
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  if (c->fuse_calls && sweep_number == 2 && fold == 2) { // held back for reset_field (the buffers swap when it runs)
-    c->pend.kind = PEND_CELL2;
+  if (c->fuse_calls && fold == 2 && (sweep_number == 2 || (direction == 1 && x_fusable(c)))) {
+    // held back for its momentum sweep or reset_field (the buffers swap when it runs)
+    c->pend.kind = PEND_CELL;
+    c->pend.cell_sweep = sweep_number;
     c->pend.cell_dir = direction;
     c->pend.cell_fold = fold;
   } else {
@@ -776,11 +792,16 @@ int cb_advec_mom(cb_chunk *c, int which_vel, int sweep_number, int direction, in
   if (direction != 1 && direction != 2) return fail(CB_EINVAL, "cb_advec_mom: direction must be 1 (x) or 2 (y)");
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  if (c->pend.kind == PEND_CELL2 && sweep_number == 2 && which_vel == 3) { // held back with the cell sweep for reset_field
-    c->pend.kind = PEND_CELL2_MOM2;
-    c->pend.mom_dir = direction;
-    c->pend.mom_fold = fold;
-    c->pend.mom_mask = which_vel;
+  const Pending held = c->pend;
+  if (held.kind == PEND_CELL && held.cell_sweep == sweep_number && held.cell_dir == direction && which_vel == 3) {
+    if (sweep_number == 2) { // held back with the cell sweep for reset_field
+      c->pend.kind = PEND_CELL_MOM;
+      c->pend.mom_fold = fold;
+      c->pend.mom_mask = which_vel;
+    } else { // a first x sweep: cell and momentum parts as one pass
+      c->pend = Pending{};
+      CB_CUDA(launch_sweep_x(c, 1, held.cell_fold, fold, -1));
+    }
   } else {
     CB_CUDA(run_pending(c));
     CB_CUDA(launch_mom(c, which_vel, sweep_number, direction, fold, -1));
@@ -795,10 +816,14 @@ int cb_reset_field(cb_chunk *c, int halo_depth) {
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
   const Pending held = c->pend;
-  if (held.kind == PEND_CELL2_MOM2) { // the second sweeps, each with reset_field's copy of what it writes
+  if (held.kind == PEND_CELL_MOM) { // the second sweeps, each with reset_field's copy of what it writes
     c->pend = Pending{};
-    CB_CUDA(launch_cell(c, 2, held.cell_dir, held.cell_fold, fold));
-    CB_CUDA(launch_mom(c, held.mom_mask, 2, held.mom_dir, held.mom_fold, fold));
+    if (held.cell_dir == 1 && x_fusable(c)) {
+      CB_CUDA(launch_sweep_x(c, 2, held.cell_fold, held.mom_fold, fold));
+    } else {
+      CB_CUDA(launch_cell(c, 2, held.cell_dir, held.cell_fold, fold));
+      CB_CUDA(launch_mom(c, held.mom_mask, 2, held.cell_dir, held.mom_fold, fold));
+    }
   } else {
     CB_CUDA(run_pending(c));
     CB_CUDA(dispatch(c, [&](auto ops) { return ops.reset_field(*c, fold); }));

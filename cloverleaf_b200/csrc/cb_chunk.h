@@ -31,15 +31,17 @@ template <int H> constexpr int box_slot() {
 // and viscosity wait for calc_dt (then one pass does the three), the PdV
 // predictor, accelerate and the PdV corrector wait for flux_calc (the
 // Lagrangian pass), the second advection sweeps wait for reset_field (which
-// they then do).  Any other call first runs what is held back, as called.
-enum PendKind : int { PEND_NONE = 0, PEND_IG, PEND_IG_VISC, PEND_PDV1, PEND_PDV1_ACC, PEND_PDV1_ACC_PDV0, PEND_CELL2, PEND_CELL2_MOM2 };
+// they then do), and the cell part of a first x sweep waits for its
+// momentum part (the x sweep runs as one pass).  Any other call first runs
+// what is held back, as called.
+enum PendKind : int { PEND_NONE = 0, PEND_IG, PEND_IG_VISC, PEND_PDV1, PEND_PDV1_ACC, PEND_PDV1_ACC_PDV0, PEND_CELL, PEND_CELL_MOM };
 struct Pending {
   int kind = PEND_NONE;
   int ig_fold = 0, visc_fold = 0;                  // ideal_gas, viscosity
   double dt = 0.0;                                 // the Lagrangian calls' dt
   int pdv1_fold = 0, acc_fold = 0, pdv0_fold = 0;  // predictor (pressure), accelerate, corrector
-  int cell_dir = 0, cell_fold = 0;                 // the second cell sweep
-  int mom_dir = 0, mom_fold = 0, mom_mask = 0;     // the second momentum sweep
+  int cell_sweep = 0, cell_dir = 0, cell_fold = 0; // a cell sweep
+  int mom_fold = 0, mom_mask = 0;                  // its momentum sweep (the second sweep's)
 };
 
 struct Chunk {

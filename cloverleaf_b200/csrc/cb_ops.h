@@ -40,6 +40,14 @@ template <typename T> struct Ops {
   // du / dv null (with reset_fold >= 0): the velocities to level 0 only (de null in advec_cell, with
   // reset_fold >= 0 and fold 2: the energy to level 0 only)
   static cudaError_t advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fold, void *du, void *dv, int reset_fold = -1);
+  // one x sweep, advec_cell then advec_mom of both velocities, as one pass over
+  // the tiles away from the mesh edge and the one-phase kernels over the edge
+  // strip; outputs to the spares 0..3 like advec_cell / advec_mom (the caller
+  // swaps).  reset_fold >= 0: reset_field's copy too, and with level0_only the
+  // new energy and velocities go to level 0 alone.  sweep_x_fusable: whether
+  // the mesh has such tiles (otherwise the call is refused).
+  static bool sweep_x_fusable(const Chunk &c);
+  static cudaError_t advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fold, int reset_fold, bool level0_only);
   static cudaError_t reset_field(Chunk &c, int fold);
   // level 1 as the phase-by-phase step leaves it, after steps whose second
   // sweeps wrote energy and velocities to level 0 only: energy1 from level 0

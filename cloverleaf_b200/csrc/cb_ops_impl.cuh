@@ -8,6 +8,7 @@
 
 #include "cb_ops.h"
 #include "cb_phase.cuh"
+#include "cb_sweep.cuh"
 #include "cb_tile.cuh"
 
 namespace cb {
@@ -235,6 +236,74 @@ cudaError_t Ops<T>::advec_mom(Chunk &c, int vel_mask, int sweep, int dir, int fo
   }
   return dir == 1 ? launch_advec_mom<T, 1, AdvecTiles<T>::MOM_X>(c, vel_mask, sweep, fold, du, dv, reset_fold)
                   : launch_advec_mom<T, 2, AdvecTiles<T>::MOM_Y>(c, vel_mask, sweep, fold, du, dv, reset_fold);
+}
+
+// The interior tiles (edge_tile false) of the advection tile grid with TY
+// rows: x0 = 2 + 64 bx >= 12 and x0 + 64 <= nx - 8, likewise in y.
+template <int TY> EdgeSet sweep_tiles(const Chunk &c, bool nodes) {
+  EdgeSet e;
+  e.tx = (c.nx + (nodes ? 1 : 0) + TILE_X - 1) / TILE_X;
+  e.ty = (c.ny + (nodes ? 1 : 0) + TY - 1) / TY;
+  e.bx_lo = 1;
+  e.bx_hi = c.nx >= 74 ? (c.nx - 74) / TILE_X : -1;
+  e.by_lo = (10 + TY - 1) / TY;
+  e.by_hi = c.ny >= 10 + TY ? (c.ny - 10 - TY) / TY : -1;
+  return e;
+}
+
+template <typename T> bool Ops<T>::sweep_x_fusable(const Chunk &c) {
+  constexpr int TY = AdvecTiles<T>::CELL_X;
+  const EdgeSet e = sweep_tiles<TY>(c, false);
+  return c.can_fold() && e.bx_hi >= e.bx_lo && e.by_hi >= e.by_lo;
+}
+
+template <typename T>
+cudaError_t Ops<T>::advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fold, int reset_fold, bool level0_only) {
+  constexpr int TY = AdvecTiles<T>::CELL_X;
+  static_assert(AdvecTiles<T>::MOM_X == TY, "the x sweep's cell and momentum tiles of the same height");
+  if (!sweep_x_fusable(c) || cell_fold != 2 || (level0_only && reset_fold < 0)) return cudaErrorNotSupported;
+  const EdgeSet ec = sweep_tiles<TY>(c, false), en = sweep_tiles<TY>(c, true);
+  void *dd = c.spare_base(0), *de = c.spare_base(1), *du = c.spare_base(2), *dv = c.spare_base(3);
+  const int mf = MASS_FLUX_X;
+  cudaError_t e;
+  if (mom_fold != 2 && !level0_only) { // the velocities' halo ring as the in-place reference leaves it
+    RingPair rp{{c.base(XVEL1), c.base(YVEL1)}, {du, dv}};
+    if ((e = copy_ring<T>(c, rp, 2, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
+  }
+  SweepOut so;
+  so.cell = CellOut{dd, level0_only ? nullptr : de, c.base(mf)};
+  so.mom = MomOut{level0_only ? nullptr : du, level0_only ? nullptr : dv};
+  if (reset_fold >= 0) {
+    so.cell.density0 = c.base(DENSITY0);
+    so.cell.energy0 = c.base(ENERGY0);
+    so.cell.rfold = reset_fold;
+    so.mom.xvel0 = c.base(XVEL0);
+    so.mom.yvel0 = c.base(YVEL0);
+    so.mom.rfold = reset_fold;
+  }
+  // (1) the interior tiles, one pass
+  using SL = SweepXLayout<T, TY>;
+  if ((e = allow_smem(kt_advec_sweep_x<T, TY>, SL::SMEM)) != cudaSuccess) return e;
+  dim3 gi(ec.bx_hi - ec.bx_lo + 1, ec.by_hi - ec.by_lo + 1);
+  kt_advec_sweep_x<T, TY><<<gi, dim3(64, 4), SL::SMEM, c.stream>>>(
+      maps_of<SL::BH>(c, {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y, XVEL1, YVEL1}), so, mesh<T>(c), (int)c.off, sweep, ec.bx_lo, ec.by_lo,
+      c.d_err);
+  if ((e = launched(c)) != cudaSuccess) return e;
+  // (2) the edge strip's cells
+  using CL = CellLayout<T, 1, TY>;
+  if ((e = allow_smem(kt_advec_cell_edges<T, 1, TY>, CL::SMEM)) != cudaSuccess) return e;
+  kt_advec_cell_edges<T, 1, TY><<<ec.count(), dim3(64, 4), CL::SMEM, c.stream>>>(
+      maps_of<CL::BH>(c, {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y}), so.cell, mesh<T>(c), (int)c.off, sweep, cell_fold, ec, c.d_err);
+  if ((e = launched(c)) != cudaSuccess) return e;
+  // (3) the edge strip's nodes, reading the new density (spare 0) as the
+  // swapped buffer map will hold it
+  using ML = MomLayout<T, 1, TY>;
+  Maps mp = maps_of<ML::BH>(c, {XVEL1, YVEL1, DENSITY1, mf, VOL_FLUX_Y});
+  mp.m[2] = c.tmap[c.sbuf[0]][box_slot<ML::BH>()];
+  if ((e = allow_smem(kt_advec_mom_edges<T, 1, TY>, ML::SMEM)) != cudaSuccess) return e;
+  kt_advec_mom_edges<T, 1, TY><<<en.count(), dim3(64, 4), ML::SMEM, c.stream>>>(mp, so.mom, mesh<T>(c), (int)c.off, 3, sweep, mom_fold, en,
+                                                                               c.d_err);
+  return launched(c);
 }
 
 template <typename T> cudaError_t Ops<T>::restore_level1(Chunk &c, const void *u_ring, const void *v_ring) {

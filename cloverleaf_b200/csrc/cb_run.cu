@@ -269,16 +269,34 @@ template <typename T> struct Seq {
     std::swap(c.fbuf[YVEL1], c.sbuf[3]);
     wrote({U1, V1}, f);
   }
+  // One sweep: advec_cell, the halo exchange, advec_mom.  Fused, an x sweep
+  // whose exchange has nothing to do (the velocities and the y mass flux
+  // already fresh; the cell sweep makes its own outputs fresh) runs as one
+  // pass over the tiles away from the edge (Ops::advec_sweep_x).
+  void sweep_pair(int sweep, int dir, int mom_depth, bool last) {
+    const bool fused = fuse && dir == 1 && Ops<T>::sweep_x_fusable(c) && fresh[U1] >= 2 && fresh[V1] >= 2 && fresh[MFY] >= 2;
+    if (!fused) {
+      cell(sweep, dir, last);
+      halo({D1, E1, U1, V1, MFX, MFY}, 2);
+      mom(sweep, dir, mom_depth, last);
+      return;
+    }
+    const int f = eff(dep(2)), fm = eff(mom_depth);
+    if (emit) run(Ops<T>::advec_sweep_x(c, sweep, f, fm, reset_tail(last), last));
+    std::swap(c.fbuf[DENSITY1], c.sbuf[0]);
+    std::swap(c.fbuf[ENERGY1], c.sbuf[1]);
+    wrote({D1, E1, MFX}, f);
+    halo({D1, E1, U1, V1, MFX, MFY}, 2); // (no pass: every field is fresh)
+    std::swap(c.fbuf[XVEL1], c.sbuf[2]);
+    std::swap(c.fbuf[YVEL1], c.sbuf[3]);
+    wrote({U1, V1}, fm);
+  }
   // driver/advection.cpp:29-105; the two advec_mom calls of a sweep run as one pass
   void advection(bool x_first) {
     const int d1 = x_first ? 1 : 2, d2 = x_first ? 2 : 1;
     halo({E1, D1, VFX, VFY}, 2);
-    cell(1, d1);
-    halo({D1, E1, U1, V1, MFX, MFY}, 2);
-    mom(1, d1, dep(2));
-    cell(2, d2, true);
-    halo({D1, E1, U1, V1, MFX, MFY}, 2);
-    mom(2, d2, 0, true);
+    sweep_pair(1, d1, dep(2), false);
+    sweep_pair(2, d2, 0, true);
   }
   void reset() {
     const int f = eff(dep(1));

@@ -9,8 +9,9 @@ of the other run tests never reach that form.  Here:
 
 * config 1 (the reference's clover_bm_short deck: 960^2, 87 steps,
   test_problem 2) through the fused device-resident graph (cb_run, fuse = 1),
-  through the host loop with the fused Lagrangian pass (cb_lagrangian) and
-  through the unfused graph: the dt of every step equal to the oracle's, every
+  through the host loop with the fused Lagrangian pass (cb_lagrangian),
+  through the host loop with call fusion (every fused pass, the x sweeps as
+  one pass each) and through the unfused graph: the dt of every step equal to the oracle's, every
   final per-cell field bit-identical to the oracle's, every state field
   (halos included) bit-identical to the phase-by-phase host loop, the
   driver's PASS check, and the summaries within 5e-11 of the reference's
@@ -55,8 +56,8 @@ class OracleRun:
 
 def run_path(dk, path, precision=FP64):
     c = Chunk(dk.x_cells, dk.y_cells, precision=precision, gamma=dk.gamma)
-    r = HydroRun(c, dk, lagrangian=(path == "lagrangian"))
-    if path in ("host", "lagrangian"):
+    r = HydroRun(c, dk, lagrangian=(path == "lagrangian"), fuse_calls=(path == "fuse_calls"))
+    if path in ("host", "lagrangian", "fuse_calls"):
         r.run()
     else:
         r.start()
@@ -98,7 +99,7 @@ def config1():
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("path", ["fused", "lagrangian", "graph"])
+@pytest.mark.parametrize("path", ["fused", "lagrangian", "fuse_calls", "graph"])
 def test_config1_fused_paths_match_oracle(config1, path):
     dk, ref, (ch, rh) = config1
     c, r = run_path(dk, path)
@@ -158,7 +159,7 @@ def circle():
     host[0].close()
 
 
-@pytest.mark.parametrize("path", ["fused", "lagrangian"])
+@pytest.mark.parametrize("path", ["fused", "lagrangian", "fuse_calls"])
 def test_circle_200x170_fused_paths(circle, path):
     dk, ref, (ch, _) = circle
     c, r = run_path(dk, path)
