@@ -766,7 +766,7 @@ def main():
     avg_ms = ftot[dom] / fcnt[dom]
     alg = LAGRANGIAN_ARRAYS * 8 * S * S
     achieved = alg / (avg_ms / 1e3) / 1e9
-    traffic = traffic_per_launch(dom, S)
+    traffic = traffic_per_launch("lagrangian", S)  # kt_lagrange's DRAM bytes per cell (profiles/traffic.json)
     tot, cnt = phases
     replaced_ms = sum(tot[k] / cnt[k] for k in LAGRANGIAN_REPLACES)
     roof = {"kernel": "kt_lagrange<double, 8>", "timed_in": f"host loop with call fusion, {lag_steps} steps (flux_calc group)",

@@ -11,10 +11,11 @@
 // density and energy of the cells x0-4 .. x0+66.  The tile evaluates that
 // ring itself from the staged level-1 state -- the same value functions as
 // the one-phase kernels, so the values are those the separate passes would
-// store and reread -- and writes only its own cells, faces and nodes.  The
-// one-phase kernels move 14 arrays for the sweep (7 each); this pass reads
-// density1, energy1, vol_flux_x, (sweep 1: vol_flux_y), xvel1, yvel1 and
-// writes density1, energy1, mass_flux_x, xvel1, yvel1: 11 (10 in sweep 2).
+// store and reread -- and writes only its own cells, faces and nodes.  As a
+// first sweep the one-phase kernels move 14 arrays (7 each); this pass reads
+// density1, energy1, vol_flux_x, vol_flux_y, xvel1, yvel1 and writes
+// density1, energy1, mass_flux_x, xvel1, yvel1: 11.  As a second sweep
+// writing level 0 (the resident loop) it moves 11 where they move 13.
 //
 // Outputs are double-buffered like the one-phase kernels' (the caller swaps):
 // other tiles still read the old level-1 state of their rings.  With the
