@@ -10,10 +10,11 @@
 // driver/timestep.cpp:37-109, driver/advection.cpp:29-105), with every halo
 // folded into its producer (meshes of at least 8 cells per side):
 //   build_field, generate_chunk, ideal_gas, update_halo(10 fields, depth 2),
-//   field_summary; then per step ideal_gas, viscosity, calc_dt (lane-wide
-//   minimum), PdV predictor (+ ideal_gas, pressure halo, revert), accelerate,
-//   PdV corrector, flux_calc, advec_cell / advec_mom (two sweeps), reset_field,
-//   and field_summary every summary_frequency steps and at the end.
+//   field_summary; then per step ideal_gas + viscosity + calc_dt as one pass
+//   (lane-wide minimum), PdV predictor (+ ideal_gas, pressure halo, revert),
+//   accelerate, PdV corrector, flux_calc, advec_cell / advec_mom (two sweeps,
+//   the second writing reset_field's level-0 copies as it stores), and
+//   field_summary every summary_frequency steps and at the end.
 #pragma once
 
 #include "cb_batch.h"
@@ -27,6 +28,9 @@ namespace cb {
 // Rows per advection tile in both precisions: the decks are small, and more,
 // smaller tiles spread a deck's phase more evenly over its lane.
 constexpr int BATCH_ADV_TY = 8;
+// Rows per tile of the fused ideal_gas + viscosity + calc_dt pass (the at-rest
+// memo in registers, as the FP32 one-launch pass keeps it).
+constexpr int BATCH_IVD_TY = 8;
 
 template <int V> struct BatchTune;
 template <> struct BatchTune<0> {
@@ -38,9 +42,8 @@ template <> struct BatchTune<1> {
 
 template <typename T, int V> constexpr size_t batch_smem() {
   using BT = BatchTune<V>;
-  size_t s = visc_smem<T>();
   auto mx = [](size_t a, size_t b) { return a > b ? a : b; };
-  s = mx(s, dt_smem<T>());
+  size_t s = (size_t)4 * Box1<T, BATCH_IVD_TY>::BOXS * sizeof(T);
   s = mx(s, pdv_smem<T>());
   s = mx(s, acc_smem<T, BT::ACC>());
   s = mx(s, flux_smem<T, BT::FLUX>());
@@ -149,20 +152,21 @@ template <typename T> struct DeckCtx {
   }
 
 template <typename T, int DIR>
-__device__ __forceinline__ bool batch_advec_cell(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep) {
+__device__ __forceinline__ bool batch_advec_cell(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep, bool reset = false) {
   constexpr int TY = BATCH_ADV_TY;
   using L = CellLayout<T, DIR, TY>;
   const int fl[4] = {DENSITY1, ENERGY1, VOL_FLUX_X, VOL_FLUX_Y};
   if (threadIdx.x == 0 && threadIdx.y == 0) d.template set_maps<L::BH>(4, fl);
   const MapSet &ms = d.ms;
-  const CellOut out{d.base(d.bm.spare(0)), d.base(d.bm.spare(1)), d.field(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
+  CellOut out{d.base(d.bm.spare(0)), d.base(d.bm.spare(1)), d.field(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
+  if (reset) { out.density0 = d.field(DENSITY0); out.energy0 = d.field(ENERGY0); out.rfold = 1; }
   const int tx = (d.m.nx + TILE_X - 1) / TILE_X, nt = tx * ((d.m.ny + TY - 1) / TY);
   CB_LANE_TILES(d, nt, tx, (advec_cell_tile<T, DIR, TY>(cx, sm, ms, out, d.m, d.D->off, sweep, 2, bx, by)));
   return true;
 }
 
 template <typename T, int DIR>
-__device__ __forceinline__ bool batch_advec_mom(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep, int fold) {
+__device__ __forceinline__ bool batch_advec_mom(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep, int fold, bool reset = false) {
   constexpr int TY = BATCH_ADV_TY;
   using L = MomLayout<T, DIR, TY>;
   const int mom_sweep = DIR + 2 * (sweep - 1);
@@ -170,7 +174,8 @@ __device__ __forceinline__ bool batch_advec_mom(TileCtx &cx, T *sm, DeckCtx<T> &
   const int fl[5] = {XVEL1, YVEL1, DENSITY1, mf, mom_sweep == 1 ? VOL_FLUX_Y : VOL_FLUX_X};
   if (threadIdx.x == 0 && threadIdx.y == 0) d.template set_maps<L::BH>(mom_sweep <= 2 ? 5 : 4, fl);
   const MapSet &ms = d.ms;
-  const MomOut out{d.base(d.bm.spare(2)), d.base(d.bm.spare(3))};
+  MomOut out{d.base(d.bm.spare(2)), d.base(d.bm.spare(3))};
+  if (reset) { out.xvel0 = d.field(XVEL0); out.yvel0 = d.field(YVEL0); out.rfold = 1; }
   const int tx = (d.m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((d.m.ny + 1 + TY - 1) / TY);
   CB_LANE_TILES(d, nt, tx, (advec_mom_tile<T, DIR, TY>(cx, sm, ms, out, d.m, d.D->off, 3, sweep, fold, bx, by)));
   return true;
@@ -324,32 +329,18 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
   bool advect_x = true;
   while (true) {
     ++step;
-    // timestep (driver/timestep.cpp:37-109)
-    {
-      const Fields<T> &F = d.F;
-      const int gx = ((m.nx + N - 1) / N + PW_X - 1) / PW_X, gy = (m.ny + PW_Y - 1) / PW_Y;
-      for (int vb = rank; vb < gx * gy; vb += w) ideal_gas_block(F, m, 0, gm1, 1, vb % gx, vb / gx, ptx, pty);
-    }
-    CB_SYNC();
-    {
-      const int fl[3] = {PRESSURE, XVEL0, YVEL0};
-      if (tid == 0) d.template set_maps<Box1<T, VISC_TY>::BH>(3, fl);
-      const MapSet &ms = d.ms;
-      const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + VISC_TY - 1) / VISC_TY);
-      for (int t = rank; t < nt; t += w)
-        CB_PHASE(viscosity_tile(cx, sm, ms, d.field(DENSITY0), d.field(VISCOSITY), m, off, t % tx, t / tx, 1));
-    }
-    CB_SYNC();
     unsigned long long *slot = D->dt_slots + step % 3;
     {
-      const int fl[2] = {XVEL0, YVEL0};
-      if (tid == 0) d.template set_maps<Box1<T, DT_TY>::BH>(2, fl);
+      constexpr int TY = BATCH_IVD_TY;
+      const int fl[4] = {DENSITY0, ENERGY0, XVEL0, YVEL0};
+      if (tid == 0) d.template set_maps<Box1<T, TY>::BH>(4, fl);
       const MapSet &ms = d.ms;
-      const DtIn in{d.field(SOUNDSPEED), d.field(VISCOSITY), d.field(DENSITY0)};
-      const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + DT_TY - 1) / DT_TY);
+      const int tx = (m.nx + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + TY - 1) / TY);
       double vmin = g_big;
       RestMemo<T> memo;
-      for (int t = rank; t < nt; t += w) CB_PHASE(calc_dt_tile(cx, sm, ms, in, m, off, D->k, t % tx, t / tx, vmin, memo));
+      for (int t = rank; t < nt; t += w)
+        CB_PHASE((ig_visc_dt_tile<T, RestMemo<T>, TY>(cx, sm, ms, d.field(PRESSURE), d.field(SOUNDSPEED), d.field(VISCOSITY), m, off, D->k,
+                                                      gm1, 1, 1, t % tx, t / tx, vmin, memo)));
       block_min_to(vmin, slot);
     }
     CB_SYNC();
@@ -416,20 +407,15 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
     CB_SYNC();
     if (tid == 0) d.bm.mom_swapped = true, d.set_fields();
     __syncthreads();
-    CB_PHASE((dir2 == 1 ? batch_advec_cell<T, 1>(cx, sm, d, 2) : batch_advec_cell<T, 2>(cx, sm, d, 2)));
+    // the second sweep also stores reset_field's level-0 copies (src/serial/reset_field.cpp:27-70), halo folded
+    CB_PHASE((dir2 == 1 ? batch_advec_cell<T, 1>(cx, sm, d, 2, true) : batch_advec_cell<T, 2>(cx, sm, d, 2, true)));
     CB_SYNC();
     if (tid == 0) d.bm.cell_swapped = false, d.set_fields();
     __syncthreads();
-    CB_PHASE((dir2 == 1 ? batch_advec_mom<T, 1>(cx, sm, d, 2, 0) : batch_advec_mom<T, 2>(cx, sm, d, 2, 0)));
+    CB_PHASE((dir2 == 1 ? batch_advec_mom<T, 1>(cx, sm, d, 2, 0, true) : batch_advec_mom<T, 2>(cx, sm, d, 2, 0, true)));
     CB_SYNC();
     if (tid == 0) d.bm.mom_swapped = false, d.set_fields();
     __syncthreads();
-    {
-      const Fields<T> &F = d.F;
-      const int gx = ((m.nx + 1 + N - 1) / N + PW_X - 1) / PW_X, gy = (m.ny + 1 + PW_Y - 1) / PW_Y;
-      for (int vb = rank; vb < gx * gy; vb += w) reset_field_block(F, m, 1, vb % gx, vb / gx, ptx, pty);
-    }
-    CB_SYNC();
     // driver/hydro.cpp:87-111
     advect_x = !advect_x;
     time += dt;

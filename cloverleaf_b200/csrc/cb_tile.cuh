@@ -473,11 +473,10 @@ __device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressur
 // one after the other.  Staged: ms 0 density0, 1 energy0, 2 xvel0, 3 yvel0.
 static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height");
 
-template <typename T, typename Memo>
+template <typename T, typename Memo, int TY = VISC_TY>
 __device__ __forceinline__ bool ig_visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, T *p_out, T *c_out, T *q_out, const Mesh<T> &m,
                                                 int off, const DtConsts &k, T gm1, int ig_fold, int fold, int bx, int by, double &vmin,
                                                 Memo &memo) {
-  constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
   const int pitch = (int)m.pitch;
   constexpr int RPT = TY / 4;
@@ -846,20 +845,19 @@ struct LagFolds {
 
 // EDGE: a tile within reach of the mesh edge (edge_tile); the others are
 // compiled without extent checks, clamps and halo folds.
+// The tile (bx, by) with the block's staging context and shared memory
+// (L::SMEM bytes at sm); staged fields ms 0..5 as above.  Returns false when
+// the staging wait gave up.
 template <typename T, int TY, bool EDGE>
-__device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> &out, const Mesh<T> &m, int off, T dt, T gm1,
-                                              const LagFolds &fd, int *err) {
+__device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &ms, const LagOut<T> &out, const Mesh<T> &m, int off, T dt,
+                                              T gm1, const LagFolds &fd, int bx, int by) {
   using L = LagLayout<T, TY>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar;
-  T *sm = reinterpret_cast<T *>(smraw);
-  TileCtx cx = tile_ctx(&bar, err);
-  const int x0 = 2 + blockIdx.x * TILE_X, y0 = 2 + blockIdx.y * TY;
+  const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
   const T *U0 = sm, *V0 = sm + L::BOXS, *D0 = sm + 2 * L::BOXS, *E0 = sm + 3 * L::BOXS, *P = sm + 4 * L::BOXS, *Q = sm + 5 * L::BOXS;
   T *sp = sm + 6 * L::BOXS, *su = sp + L::PCX * L::PCY, *sv = su + L::NNX * L::NNY, *gx = sv + L::NNX * L::NNY, *gy = gx + BOX_X;
-  stage_issue(cx, sm, map_set(maps, 6), 6, L::BOXS, L::BH, off + x0 - HALO, y0 - 1);
+  stage_issue(cx, sm, ms, 6, L::BOXS, L::BH, off + x0 - HALO, y0 - 1);
   fill_widths(m, x0, y0, 1, L::BH, 1, gx, gy, nullptr, nullptr); // gx[i - x0 + HALO] = celldx[i], gy[j - y0 + 1] = celldy[j]
-  if (!stage_wait(cx)) return;
+  if (!stage_wait(cx)) return false;
   const int pitch = (int)m.pitch;
   // (1) the predictor over the pressure ring
   each_rows<L::PCX, L::PCY>([&](int p, int l) {
@@ -912,7 +910,7 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
   __syncthreads();
   // (3) the corrector over the tile's cells and flux_calc over its faces
   const int i = x0 + threadIdx.x;
-  if (EDGE && i >= m.nx + 3) return;
+  if (EDGE && i >= m.nx + 3) return true;
   const T cdx = gx[threadIdx.x + HALO];
 #pragma unroll
   for (int r = 0; r < TY / 4; ++r) {
@@ -948,16 +946,21 @@ __device__ __forceinline__ void lagrange_tile(const Maps &maps, const LagOut<T> 
       if (EDGE) fold_halo(out.vol_flux_y, m, halo_rule(VOL_FLUX_Y), fd.flux, i, j, fy);
     }
   }
+  return true;
 }
 
 template <typename T, int TY>
 __global__ void __launch_bounds__(256) kt_lagrange(const __grid_constant__ Maps maps, LagOut<T> out, Mesh<T> m, int off, T dt,
                                                    const double *dtp, T gm1, LagFolds fd, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  T *sm = reinterpret_cast<T *>(smraw);
+  TileCtx cx = tile_ctx(&bar, err);
   const T d = dtp ? (T)*dtp : dt;
   if (edge_tile(m.nx, m.ny, 2 + blockIdx.x * TILE_X, 2 + blockIdx.y * TY, TY))
-    lagrange_tile<T, TY, true>(maps, out, m, off, d, gm1, fd, err);
+    lagrange_tile<T, TY, true>(cx, sm, map_set(maps, 6), out, m, off, d, gm1, fd, blockIdx.x, blockIdx.y);
   else
-    lagrange_tile<T, TY, false>(maps, out, m, off, d, gm1, fd, err);
+    lagrange_tile<T, TY, false>(cx, sm, map_set(maps, 6), out, m, off, d, gm1, fd, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
