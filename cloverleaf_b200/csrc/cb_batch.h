@@ -4,12 +4,19 @@
 // A batch holds many meshes, each laid out exactly as a cb_chunk lays out
 // one (cb_chunk.h: same pitch, offset, 19 buffers and tensor maps), each
 // with its own gamma, states, dt controls and end time.  One launch of the
-// persistent kernel advances every deck from its initial state to its end:
-// the grid is split into lanes of CTAs, a lane runs its decks one after the
-// other, and the CTAs of a lane share each deck's tiles and meet at a lane
-// barrier between the phases.  Every CTA of a lane steps through the same
-// control flow (dt, time, step, summaries) with identical values, so no
-// control state has to be exchanged besides the dt minimum.
+// persistent kernel advances every deck from its initial state to its end.
+// Each deck has a width w (CTAs, a power of two) and waits in the queue of
+// its width, largest first.  The queues are worked widest first: at width W
+// the grid is cut into lanes of W consecutive CTAs; a lane takes the next
+// deck of the queue (one atomic add by its first CTA, shared at a lane
+// barrier), its CTAs share the deck's tiles and meet at a lane barrier
+// between the phases, and when the queue is empty the lane splits into the
+// lanes of the next width.  No CTA waits for a deck to gather its CTAs, and
+// a lane that finishes early goes on with narrower decks.  Every CTA of a
+// lane steps through the same control flow (dt, time, step, summaries) with
+// identical values, so no control state has to be exchanged besides the dt
+// minimum.  A deck's width is fixed by the schedule, so its results do not
+// depend on which lane ran it.
 #pragma once
 
 #include <cuda.h>
@@ -65,12 +72,12 @@ struct BatchDeck {
 
 struct BatchLaunch {
   BatchDeck *decks;
-  const int *cta_lane;   // lane of each CTA
-  const int *lane_cta0;  // first CTA of each lane
-  const int *lane_width; // CTAs of each lane
-  const int *lane_deck0; // decks of lane l: lane_decks[lane_deck0[l] .. lane_deck0[l + 1])
-  const int *lane_decks;
-  unsigned *lane_sync;   // one barrier counter per lane (zero at launch)
+  const int *queue;      // the decks, queue after queue (widest first), each largest first
+  const int *level;      // per width k: width | first queue position | decks | first lane slot (4 ints)
+  int nlevels;
+  unsigned *next;        // next queue position to hand out, per width (zero at launch)
+  unsigned *lane_sync;   // barrier counter of each lane slot (zero at launch)
+  int *lane_deck;        // the deck a lane took (written by its first CTA), per lane slot
   int *abort;            // set when a barrier wait gives up; ends every lane
   int *err;              // set when a staging wait gives up
 };

@@ -48,9 +48,10 @@ struct cb_batch {
   BatchDeck *h_desc = nullptr;      // pinned copy the graph uploads
   // launch layout
   cb_batch_schedule sched{};
-  int grid = 0, nlanes = 0;
-  int *d_plan = nullptr;            // cta_lane | lane_cta0 | lane_width | lane_deck0 | lane_decks
-  unsigned *d_sync = nullptr;
+  int grid = 0, nlanes = 0, nlevels = 0; // lanes over all widths
+  size_t sync_words = 0;
+  int *d_plan = nullptr;            // queue | level
+  unsigned *d_sync = nullptr;       // lane_sync | lane_deck | next
   int *d_flags = nullptr;           // [0] abort, [1] staging error
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -108,14 +109,24 @@ cudaError_t occupancy(const cb_batch *b, int variant, int *per_sm) {
   return b->precision == CB_FP64 ? BatchOps<double>::occupancy(variant, per_sm) : BatchOps<float>::occupancy(variant, per_sm);
 }
 
-// Lanes of the launch for schedule s: widths, deck lists, and the grid.
+// The deck queues of schedule s.  A deck of c cells gets w CTAs, w the power
+// of two >= c / cells_per_cta (at most max_lane_width, its tile count and the
+// grid, rounded down to a power of two); one queue per width, widest first,
+// each largest estimated run (cells x steps) first.  The grid is every
+// resident CTA; at width W it forms grid / W lanes, each with a lane slot
+// (barrier counter, deck taken).
 struct Plan {
-  std::vector<int> width;
-  std::vector<std::vector<int>> decks;
-  int ctas = 0;
+  std::vector<int> queue, level; // level: width | first queue position | decks | first lane slot
+  int ctas = 0, lanes = 0;
 };
 
 int tiles_of(const cb_deck &d) { return ((d.nx + 63) / 64) * ((d.ny + 15) / 16); }
+
+int pow2_floor(int v) {
+  int p = 1;
+  while (p * 2 <= v) p *= 2;
+  return p;
+}
 
 Plan make_plan(const cb_batch *b, const cb_batch_schedule &s, int grid_max) {
   const int maxw = std::max(1, std::min(s.max_lane_width > 0 ? s.max_lane_width : BATCH_MAX_LANE, BATCH_MAX_LANE));
@@ -123,80 +134,23 @@ Plan make_plan(const cb_batch *b, const cb_batch_schedule &s, int grid_max) {
   for (int d = 0; d < b->n; ++d) {
     const long long cells = (long long)b->decks[d].nx * b->decks[d].ny;
     int wd = s.cells_per_cta > 0 ? next_pow2((cells + s.cells_per_cta - 1) / s.cells_per_cta) : 1;
-    wd = std::min(wd, maxw);
+    wd = std::min(wd, pow2_floor(maxw));
     while (wd > 1 && wd > tiles_of(b->decks[d])) wd >>= 1;
-    // a deck wider than the grid gets the whole grid (not the power of two below it)
-    w[d] = std::max(std::min(wd, grid_max), 1);
+    w[d] = std::min(wd, pow2_floor(grid_max));
   }
-  // classes by width: count, work
-  std::vector<int> widths;
-  for (int d = 0; d < b->n; ++d)
-    if (std::find(widths.begin(), widths.end(), w[d]) == widths.end()) widths.push_back(w[d]);
-  std::sort(widths.begin(), widths.end());
-  const int nc = (int)widths.size();
-  std::vector<double> cw(nc, 0.0);
-  std::vector<int> cnt(nc, 0), lanes(nc, 0);
-  double total = 0.0;
-  for (int d = 0; d < b->n; ++d) {
-    const int c = (int)(std::find(widths.begin(), widths.end(), w[d]) - widths.begin());
-    cw[c] += b->work[d];
-    cnt[c] += 1;
-    total += b->work[d];
-  }
-  // lanes per class in proportion to the class's work, at least one
-  int used = 0;
-  for (int c = 0; c < nc; ++c) {
-    const double share = grid_max * cw[c] / std::max(total, 1e-300);
-    lanes[c] = std::max(1, std::min(cnt[c], (int)std::floor(share / widths[c])));
-    used += lanes[c] * widths[c];
-  }
-  while (used > grid_max) { // over budget: drop a lane from the class with the least work per CTA
-    int best = -1;
-    double bv = 1e300;
-    for (int c = 0; c < nc; ++c)
-      if (lanes[c] > 1) {
-        const double v = cw[c] / (lanes[c] * (double)widths[c]);
-        if (v < bv) bv = v, best = c;
-      }
-    if (best < 0) break;
-    lanes[best] -= 1;
-    used -= widths[best];
-  }
-  while (true) { // spare CTAs: add a lane to the class with the most work per CTA
-    int best = -1;
-    double bv = -1.0;
-    for (int c = 0; c < nc; ++c)
-      if (lanes[c] < cnt[c] && used + widths[c] <= grid_max) {
-        const double v = cw[c] / (lanes[c] * (double)widths[c]);
-        if (v > bv) bv = v, best = c;
-      }
-    if (best < 0) break;
-    lanes[best] += 1;
-    used += widths[best];
-  }
-  // decks to lanes: largest first, each to its class's least-loaded lane
+  std::vector<int> widths(w);
+  std::sort(widths.begin(), widths.end(), std::greater<int>());
+  widths.erase(std::unique(widths.begin(), widths.end()), widths.end());
   Plan p;
-  std::vector<int> order(b->n);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->work[x] > b->work[y]; });
-  std::vector<int> first(nc);
-  for (int c = 0; c < nc; ++c) {
-    first[c] = (int)p.width.size();
-    for (int l = 0; l < lanes[c]; ++l) {
-      p.width.push_back(widths[c]);
-      p.decks.emplace_back();
-    }
+  p.ctas = grid_max;
+  for (int W : widths) {
+    const int q0 = (int)p.queue.size();
+    for (int d = 0; d < b->n; ++d)
+      if (w[d] == W) p.queue.push_back(d);
+    std::stable_sort(p.queue.begin() + q0, p.queue.end(), [&](int x, int y) { return b->work[x] > b->work[y]; });
+    p.level.insert(p.level.end(), {W, q0, (int)p.queue.size() - q0, p.lanes});
+    p.lanes += grid_max / W;
   }
-  std::vector<double> load(p.width.size(), 0.0);
-  for (int d : order) {
-    const int c = (int)(std::find(widths.begin(), widths.end(), w[d]) - widths.begin());
-    int best = first[c];
-    for (int l = first[c]; l < first[c] + lanes[c]; ++l)
-      if (load[l] < load[best]) best = l;
-    load[best] += b->work[d] / widths[c];
-    p.decks[best].push_back(d);
-  }
-  p.ctas = used;
   return p;
 }
 
@@ -246,16 +200,16 @@ int check_deck(const cb_deck &d, int k) {
 cudaError_t enqueue_run(cb_batch *b) {
   cudaError_t e;
   if ((e = cudaMemcpyAsync(b->d_desc, b->h_desc, sizeof(BatchDeck) * b->n, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(b->d_sync, 0, sizeof(unsigned) * std::max(b->nlanes, 1), b->stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(b->d_sync, 0, sizeof(unsigned) * b->sync_words, b->stream)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(b->d_flags, 0, sizeof(int) * 2, b->stream)) != cudaSuccess) return e;
   BatchLaunch a{};
   a.decks = b->d_desc;
-  a.cta_lane = b->d_plan;
-  a.lane_cta0 = a.cta_lane + b->grid;
-  a.lane_width = a.lane_cta0 + b->nlanes;
-  a.lane_deck0 = a.lane_width + b->nlanes;
-  a.lane_decks = a.lane_deck0 + b->nlanes + 1;
+  a.queue = b->d_plan;
+  a.level = a.queue + b->n;
+  a.nlevels = b->nlevels;
   a.lane_sync = b->d_sync;
+  a.lane_deck = reinterpret_cast<int *>(b->d_sync + b->nlanes);
+  a.next = b->d_sync + 2 * b->nlanes;
   a.abort = b->d_flags;
   a.err = b->d_flags + 1;
   const int v = b->sched.variant;
@@ -419,31 +373,23 @@ int cb_batch_set_schedule(cb_batch *b, const cb_batch_schedule *s) {
   if (per_sm < 1) return fail(CB_ECUDA, "cb_batch_set_schedule: the ensemble kernel does not fit on an SM");
   const int use_sm = s->ctas_per_sm > 0 ? std::min(s->ctas_per_sm, per_sm) : per_sm;
   const Plan p = make_plan(b, *s, use_sm * b->sms);
-  // plan arrays: cta_lane[grid] | lane_cta0[L] | lane_width[L] | lane_deck0[L+1] | lane_decks[n]
-  const int L = (int)p.width.size();
-  std::vector<int> h;
-  h.reserve(p.ctas + 3 * L + 1 + b->n);
-  for (int l = 0; l < L; ++l)
-    for (int k = 0; k < p.width[l]; ++k) h.push_back(l);
-  int c0 = 0;
-  for (int l = 0; l < L; ++l) h.push_back(c0), c0 += p.width[l];
-  for (int l = 0; l < L; ++l) h.push_back(p.width[l]);
-  int d0 = 0;
-  for (int l = 0; l < L; ++l) h.push_back(d0), d0 += (int)p.decks[l].size();
-  h.push_back(d0);
-  for (int l = 0; l < L; ++l)
-    for (int d : p.decks[l]) h.push_back(d);
+  // plan arrays: queue[n] | level[4 K]; counters: lane_sync[lanes] | lane_deck[lanes] | next[K]
+  std::vector<int> h(p.queue);
+  h.insert(h.end(), p.level.begin(), p.level.end());
+  const int K = (int)p.level.size() / 4;
   if (b->d_plan) cudaFree(b->d_plan);
   if (b->d_sync) cudaFree(b->d_sync);
   b->d_plan = nullptr;
   b->d_sync = nullptr;
   BCUDA(cudaMalloc(&b->d_plan, sizeof(int) * h.size()));
   BCUDA(cudaMemcpy(b->d_plan, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
-  BCUDA(cudaMalloc(&b->d_sync, sizeof(unsigned) * std::max(L, 1)));
+  BCUDA(cudaMalloc(&b->d_sync, sizeof(unsigned) * (2 * (size_t)p.lanes + K)));
   b->sched = *s;
   b->sched.ctas_per_sm = use_sm;
   b->grid = p.ctas;
-  b->nlanes = L;
+  b->nlanes = p.lanes;
+  b->nlevels = K;
+  b->sync_words = 2 * (size_t)p.lanes + K;
   // capture the run in a graph; a capture the runtime refuses (the
   // cooperative launch attribute) leaves direct launches in use
   if (b->exec) cudaGraphExecDestroy(b->exec);

@@ -267,12 +267,16 @@ typedef struct {
 enum { CB_DECK_PENDING = 0, CB_DECK_DONE = 1, CB_DECK_SMALL_DT = 2, CB_DECK_STAGE_FAIL = 3, CB_DECK_SYNC_FAIL = 4 };
 
 /* How the persistent launch is laid out.  A deck of c cells runs on a lane of
- * w CTAs, w the power of two >= c / cells_per_cta (at most max_lane_width
- * and the deck's tile count); lanes of each width get a share of the grid in
- * proportion to their decks' estimated work, and decks go to the lane with
- * the least work so far, largest first.  ctas_per_sm (0 = as many as fit)
- * sets the grid; variant picks the tile shapes (0: 64 x 16 tiles for
- * accelerate and flux_calc, 1: 64 x 8 tiles and more CTAs per SM). */
+ * w CTAs, w the power of two >= c / cells_per_cta (at most max_lane_width,
+ * the deck's tile count and the grid).  The decks wait in one queue per
+ * width, largest estimated run (cells x steps) first, and the queues are
+ * worked widest first: at width W the grid forms lanes of W consecutive CTAs,
+ * each lane takes the queue's next deck until the queue is empty, then splits
+ * into the lanes of the next width.  ctas_per_sm (0 = as many as fit) sets
+ * the grid; variant picks the tile shapes (0: 64 x 16 tiles for accelerate
+ * and flux_calc, 1: 64 x 8 tiles and more CTAs per SM).  The lanes count
+ * that cb_batch_get_schedule and the trials report is the sum over the widths
+ * of grid / width. */
 typedef struct {
   int cells_per_cta;
   int max_lane_width;
