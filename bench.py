@@ -65,6 +65,17 @@ LAGRANGIAN_ARRAYS = 14
 LAGRANGIAN_REPLACES = ("pdv_predict", "accelerate", "pdv_correct", "flux_calc")
 STEP_ARRAYS = 105  # the step's phases, ideal_gas .. reset_field
 LARGE_STEPS = 50  # the 15360^2 deck runs 50 steps
+# The advection passes of the fused step and their own distinct arrays: the x
+# sweep as one pass reads density1, energy1, vol_flux_x, vol_flux_y, xvel1,
+# yvel1 and writes density1, energy1, mass_flux_x, xvel1, yvel1 (as the
+# second sweep: level 0 in place of level 1, no vol_flux_y read, density1
+# kept: 11 as well); the y sweep as the first sweep: advec_cell 4 + 3,
+# advec_mom 5 + 2; as the second sweep with reset_field's copy: advec_cell
+# density1, energy1, vol_flux_y read, density1, density0, energy0,
+# mass_flux_y written, advec_mom xvel1, yvel1, density1, mass_flux_y read,
+# xvel0, yvel0 written
+SWEEP_ARRAYS = {"x_sweep": 11, "y_sweep_first": 14, "y_sweep_second": 13}
+SWEEP_MARKS = ("advec_cell_s1", "advec_mom_s1", "advec_cell_s2", "advec_mom_s2", "reset_field")
 
 
 def max_over_ranks(ms, device):
@@ -160,17 +171,22 @@ def bench_deck(cells, gamma=1.4):
 
 
 class PhaseTimer:
-    """CUDA events on the chunk's own stream at every phase boundary."""
+    """CUDA events on the chunk's own stream at every phase boundary.  With
+    `run`, the advection marks carry the step's first direction ("@x" when
+    the x sweep goes first, "@y" otherwise)."""
 
-    def __init__(self, chunk):
+    def __init__(self, chunk, run=None):
         import torch
         self.torch = torch
         self.stream = torch.cuda.ExternalStream(chunk.stream())
         self.marks = []
+        self.run = run
 
     def __call__(self, name):
         e = self.torch.cuda.Event(enable_timing=True)
         e.record(self.stream)
+        if self.run is not None and name in SWEEP_MARKS:
+            name += "@x" if self.run.advect_x else "@y"
         self.marks.append((name, e))
 
     def totals(self):
@@ -183,7 +199,8 @@ class PhaseTimer:
         return tot, cnt
 
 
-def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1, fuse_calls=False):
+def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False, rank=0, world=1, fuse_calls=False,
+             tag_sweeps=False):
     """Sets up a chunk, runs warmup steps, then times `steps` steps; returns
     (ms, run, chunk, phase totals, launches in the timed region).  With
     `fuse_calls` the chunk runs the driver's calls as the fused passes (one
@@ -200,7 +217,7 @@ def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False,
     for _ in range(warmup):
         run.hydro_step()
     ext = torch.cuda.ExternalStream(c.stream())
-    timer = PhaseTimer(c) if with_phases else None
+    timer = PhaseTimer(c, run if tag_sweeps else None) if with_phases else None
     run.probe = timer
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     c.synchronize()
@@ -358,6 +375,28 @@ def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
         row["speedup"] = row["host_loop"]["ms_per_step"] / row["device_graph"]["ms_per_step"]
         row["speedup_fused"] = row["host_loop"]["ms_per_step"] / row["device_graph_fused"]["ms_per_step"]
         out.append(row)
+    return out
+
+
+def sweep_rooflines(ftag, ctag, cells, peak):
+    """The fused step's advection passes from the call-fused host loop's
+    direction-tagged groups: the x sweep as one pass with its edge strip
+    (advec_mom_s1 when x goes first, reset_field when y goes first), the y
+    sweep as the first sweep (advec_cell_s1 + advec_mom_s1 when y goes first)
+    and as the second (reset_field when x goes first); ms per launch and the
+    fraction of the peak its own arrays reach."""
+    def per(keys, n_key):
+        n = ctag.get(n_key, 0)
+        return sum(ftag.get(k, 0.0) for k in keys) / n if n else None
+    xs = [v for v in (per(["advec_mom_s1@x"], "advec_mom_s1@x"), per(["reset_field@y"], "reset_field@y")) if v]
+    ms = {"x_sweep": sum(xs) / len(xs) if xs else None,
+          "y_sweep_first": per(["advec_cell_s1@y", "advec_mom_s1@y"], "advec_mom_s1@y"),
+          "y_sweep_second": per(["reset_field@x"], "reset_field@x")}
+    out = {}
+    for k, t in ms.items():
+        if t:
+            gbs = SWEEP_ARRAYS[k] * 8 * cells * cells / (t / 1e3) / 1e9
+            out[k] = {"ms_per_launch": t, "arrays": SWEEP_ARRAYS[k], "achieved": gbs, "frac": gbs / peak}
     return out
 
 
@@ -759,9 +798,15 @@ def main():
     # flux_calc group is the Lagrangian pass (with the pressure's outer-ring
     # copy, a few microseconds)
     lag_steps = min(args.steps, 20)
-    msf, _, cf, phf, _ = run_form(FP64, S, args.warmup, lag_steps, with_phases=True, rank=rank, world=world, fuse_calls=True)
+    msf, _, cf, phf, _ = run_form(FP64, S, args.warmup, lag_steps, with_phases=True, rank=rank, world=world, fuse_calls=True,
+                                  tag_sweeps=True)
     cf.close()
-    ftot, fcnt = phf
+    ftag, ctag = phf
+    ftot, fcnt = {}, {}
+    for k in ftag:  # the groups over both step directions
+        g = k.split("@")[0]
+        ftot[g] = ftot.get(g, 0.0) + ftag[k]
+        fcnt[g] = fcnt.get(g, 0) + ctag[k]
     dom = "flux_calc"
     avg_ms = ftot[dom] / fcnt[dom]
     alg = LAGRANGIAN_ARRAYS * 8 * S * S
@@ -780,10 +825,12 @@ def main():
             "fused_calls_ms_per_step": msf / lag_steps,
             "fused_calls_phase_ms_per_step": {k: ftot[k] / lag_steps for k in sorted(ftot)},
             "fused_calls_kernels": {"calc_dt": "kt_ig_visc_dt + 8-byte dt read-back", "flux_calc": "kt_lagrange + ring copy",
-                                    "advec_cell_s1": "kt_advec_cell", "advec_mom_s1": "kt_advec_mom",
+                                    "advec_cell_s1": "kt_advec_cell (y first; held back when x goes first)",
+                                    "advec_mom_s1": "kt_advec_sweep_x + edge strip (x first) / kt_advec_mom (y first)",
                                     "reset_field": "both second sweeps (with reset_field's copy)",
                                     "field_summary": "k_field_summary + 40-byte read-back"},
-            "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)}}
+            "phase_ms_per_step": {k: tot[k] / args.steps for k in sorted(tot)},
+            "sweeps": sweep_rooflines(ftag, ctag, S, peak)}
 
     batch = None
     if args.batch:
