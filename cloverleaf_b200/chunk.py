@@ -39,7 +39,7 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count",
            "cb_adjoint_create", "cb_adjoint_destroy", "cb_adjoint_set_initial", "cb_adjoint_set_checkpoint_interval",
            "cb_adjoint_forward", "cb_adjoint_dt", "cb_adjoint_gradient", "cb_adjoint_tangent", "cb_adjoint_read_tangent",
-           "cb_adjoint_read_field", "cb_adjoint_stats", "cb_selftest_width_ratio"]
+           "cb_adjoint_read_field", "cb_adjoint_stats", "cb_selftest_width_ratio", "cb_selftest_wait_limits"]
 
 
 class CloverError(RuntimeError):
@@ -105,6 +105,7 @@ def library() -> ctypes.CDLL:
         "cb_run": ([P, ctypes.POINTER(RunParams), ctypes.POINTER(RunState), i, dp, dp, i, ip], i),
         "cb_field_summary_noalloc": ([i, i, ctypes.c_longlong] + [P] * 8 + [d, P, P], i),
         "cb_selftest_width_ratio": ([ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong)], i),
+        "cb_selftest_wait_limits": ([d, ip, ip, dp, ip, ip, dp], i),
         "cb_set_external_faces": ([P, i], i), "cb_copy_tile_halo": ([P, P, i, ip, i], i),
     }
     for name, (args, res) in sig.items():

@@ -19,6 +19,7 @@
 
 #include "cb_batch.h"
 #include "cb_ops_impl.cuh"
+#include "cb_sync.cuh"
 
 namespace cb {
 
@@ -52,54 +53,6 @@ template <typename T, int V> constexpr size_t batch_smem() {
   s = mx(s, MomLayout<T, 2, BATCH_ADV_TY>::SMEM);
   s = mx(s, (size_t)5 * 256 * sizeof(double)); // the summary's block reduction
   return s;
-}
-
-constexpr unsigned long long LANE_SYNC_LIMIT_NS = 2000000000ull; // a lane barrier gives up after 2 s
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Barrier over the w CTAs of a lane, with release/acquire at GPU scope so
-// that each CTA's writes of the phase are visible to the lane's next phase,
-// and proxy fences so that bulk tensor copies (the async proxy) of the next
-// phase see them too.  Bounded: gives up after LANE_SYNC_LIMIT_NS or when
-// another lane has given up, and then returns false in every thread.
-__device__ __forceinline__ bool lane_sync(unsigned *ctr, int w, int *abort) {
-  __shared__ int s_ok;
-  asm volatile("fence.proxy.async.global;" ::: "memory");
-  __syncthreads();
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    int ok = 1;
-    if (w > 1) {
-      __threadfence();
-      const unsigned old = atomicAdd(ctr, 1u);
-      const unsigned target = (old / (unsigned)w + 1u) * (unsigned)w;
-      const unsigned long long t0 = global_ns();
-      while (true) {
-        unsigned v;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
-        if ((int)(v - target) >= 0) break;
-        if (*(volatile int *)abort) {
-          ok = 0;
-          break;
-        }
-        if (global_ns() - t0 > LANE_SYNC_LIMIT_NS) {
-          atomicExch(abort, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-      __threadfence();
-      asm volatile("fence.proxy.async.global;" ::: "memory");
-    }
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
 }
 
 // Buffers of the double-buffered pairs during a step: advec_cell writes the

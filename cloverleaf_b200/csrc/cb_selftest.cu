@@ -1,12 +1,18 @@
-// cb_selftest.cu -- cb_selftest_width_ratio: checks width_ratio (cb_mesh.cuh),
-// the FP64 kernels' quotient of two mesh widths with a precomputed
-// reciprocal, against the division operator on the device, bit for bit.
+// cb_selftest.cu -- diagnostics the test suite calls:
+// cb_selftest_width_ratio checks width_ratio (cb_mesh.cuh), the FP64
+// kernels' quotient of two mesh widths with a precomputed reciprocal, against
+// the division operator on the device, bit for bit; cb_selftest_wait_limits
+// runs the kernels' two bounded waits (a tile's staging wait, cb_tma.cuh,
+// and the ensemble's lane barrier, cb_sync.cuh) to their limit on purpose,
+// on a barrier nothing completes, and reports that each gave up and set its
+// error flag.
 #include <cuda_runtime.h>
 
 #include <string>
 
 #include "../../include/cloverb200.h"
 #include "cb_mesh.cuh"
+#include "cb_sync.cuh"
 
 namespace cb {
 int set_last_error(int code, const std::string &msg);
@@ -49,7 +55,69 @@ __global__ void k_width_ratio(unsigned long long n, unsigned long long seed, uns
   if (local) atomicAdd(bad, local);
 }
 
+// A staging wait on a barrier that needs two arrivals and gets one: no copy
+// is in flight, nothing will complete the phase, and mbar_wait gives up
+// after limit_ns with the error flag set.
+__global__ void k_stage_wait_limit(unsigned long long limit_ns, int *err, unsigned long long *elapsed, int *returned) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  cb::mbar_init(&bar, 2);
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(cb::smem_addr(&bar)) : "memory");
+  const unsigned long long t0 = cb::global_ns();
+  const bool ok = cb::mbar_wait(&bar, 0, err, limit_ns);
+  elapsed[0] = cb::global_ns() - t0;
+  returned[0] = ok ? 1 : 0;
+}
+
+// A lane of two CTAs whose second CTA exits without arriving: the first
+// gives up after limit_ns, sets the abort flag and returns false.
+__global__ void k_lane_wait_limit(unsigned *ctr, int *abort, unsigned long long limit_ns, unsigned long long *elapsed, int *returned) {
+  if (blockIdx.x == 1) return;
+  const unsigned long long t0 = cb::global_ns();
+  const bool ok = cb::lane_sync(ctr, 2, abort, limit_ns);
+  if (threadIdx.x == 0) {
+    elapsed[1] = cb::global_ns() - t0;
+    returned[1] = ok ? 1 : 0;
+  }
+}
+
 } // namespace
+
+extern "C" int cb_selftest_wait_limits(double limit_ms, int *stage_flag, int *stage_returned, double *stage_ms, int *lane_abort,
+                                       int *lane_returned, double *lane_ms) {
+  if (!(limit_ms > 0.0 && limit_ms <= 1000.0) || !stage_flag || !stage_returned || !stage_ms || !lane_abort || !lane_returned || !lane_ms)
+    return cb::set_last_error(CB_EINVAL, "cb_selftest_wait_limits: bad argument (limit_ms in (0, 1000])");
+  const unsigned long long limit_ns = (unsigned long long)(limit_ms * 1e6);
+  // words: [0] staging error flag, [1] lane counter, [2] abort flag, [3..4] returned flags; then two elapsed times
+  int *d_w = nullptr;
+  unsigned long long *d_t = nullptr;
+  cudaError_t e = cudaMalloc(&d_w, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_t, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(d_w, 0, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(d_t, 0, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) {
+    k_stage_wait_limit<<<1, 32>>>(limit_ns, d_w, d_t, d_w + 3);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_lane_wait_limit<<<2, 64>>>(reinterpret_cast<unsigned *>(d_w + 1), d_w + 2, limit_ns, d_t, d_w + 3);
+    e = cudaGetLastError();
+  }
+  int w[8] = {0};
+  unsigned long long t[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(w, d_w, sizeof(w), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(t, d_t, sizeof(t), cudaMemcpyDeviceToHost);
+  cudaFree(d_w);
+  cudaFree(d_t);
+  if (e != cudaSuccess) return cb::set_last_error(CB_ECUDA, std::string("cb_selftest_wait_limits: ") + cudaGetErrorString(e));
+  *stage_flag = w[0];
+  *stage_returned = w[3];
+  *stage_ms = (double)t[0] / 1e6;
+  *lane_abort = w[2];
+  *lane_returned = w[4];
+  *lane_ms = (double)t[1] / 1e6;
+  return CB_OK;
+}
 
 extern "C" int cb_selftest_width_ratio(long long samples, unsigned long long seed, long long *mismatches) {
   if (samples < 0 || !mismatches) return cb::set_last_error(CB_EINVAL, "cb_selftest_width_ratio: bad argument");

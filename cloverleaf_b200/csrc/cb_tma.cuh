@@ -22,7 +22,7 @@ namespace cb {
 constexpr int TILE_X = 64;  // output columns per block
 constexpr int HALO = 4;     // staged halo on every side
 constexpr int BOX_X = TILE_X + 2 * HALO;
-constexpr unsigned TMA_SPIN_LIMIT = 1u << 24; // bounded mbarrier wait
+constexpr unsigned long long TMA_WAIT_LIMIT_NS = 1000000000ull; // a staging wait gives up after 1 s
 
 // Up to eight tensor maps passed by value as one __grid_constant__ parameter.
 struct Maps {
@@ -30,6 +30,12 @@ struct Maps {
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
@@ -57,11 +63,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
   return ok != 0;
 }
 
-// Waits for the barrier's phase with a bounded number of polls; on give-up
-// it records an error for the host and reports failure.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase, int *err) {
-  for (unsigned it = 0; it < TMA_SPIN_LIMIT; ++it)
-    if (mbar_try_wait(bar, phase)) return true;
+// Waits for the barrier's phase for at most limit_ns (the clock read every
+// 64 polls); on give-up it records an error for the host and reports
+// failure.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase, int *err, unsigned long long limit_ns = TMA_WAIT_LIMIT_NS) {
+  if (mbar_try_wait(bar, phase)) return true;
+  const unsigned long long t0 = global_ns();
+  do {
+    for (int it = 0; it < 64; ++it)
+      if (mbar_try_wait(bar, phase)) return true;
+  } while (global_ns() - t0 <= limit_ns);
   if (err) atomicExch(err, 1);
   return false;
 }

@@ -34,6 +34,8 @@ def main(argv=None):
                     help="host loop with the chunk's call fusion on (the fused passes, one launch each)")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--runs", type=int, default=1, help="ensemble runs after one warm-up run")
+    ap.add_argument("--cells-per-cta", type=int, default=0, help="ensemble schedule: cells per CTA (0: the default schedule)")
+    ap.add_argument("--variant", type=int, default=0, help="ensemble schedule: tile variant (with --cells-per-cta)")
     args = ap.parse_args(argv)
     if args.ensemble:
         return ensemble(args)
@@ -65,6 +67,8 @@ def ensemble(args):
     from .batch import Batch, ensemble_decks
     decks = ensemble_decks(args.ensemble)
     b = Batch(decks, precision=FP32 if args.precision == "fp32" else FP64, device=args.device)
+    if args.cells_per_cta > 0:
+        b.set_schedule(cells_per_cta=args.cells_per_cta, variant=args.variant)
     sched, lanes, ctas = b.schedule()
     for k in range(args.runs + 1):
         b.run()

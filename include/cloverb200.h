@@ -373,6 +373,18 @@ int cb_adjoint_stats(const cb_adjoint *a, int *checkpoint_interval, int *checkpo
  * reference. */
 int cb_selftest_width_ratio(long long samples, unsigned long long seed, long long *mismatches);
 
+/* DIAGNOSTIC, not part of the hydro interface: runs the kernels' two bounded
+ * waits to their limit on purpose, with limit_ms (0 < limit_ms <= 1000) in
+ * place of the kernels' own limits (1 s for a tile's staging wait, 2 s for
+ * the ensemble's lane barrier): a staging wait on an mbarrier that nothing
+ * completes (no copy in flight) and a lane barrier whose second CTA never
+ * arrives.  Reports each wait's error flag (*stage_flag, *lane_abort: 1 when
+ * it gave up), what it returned (0: gave up) and how long it waited.  The
+ * device stays usable afterwards.  The test suite calls it; a solver never
+ * needs to.  No counterpart in the reference. */
+int cb_selftest_wait_limits(double limit_ms, int *stage_flag, int *stage_returned, double *stage_ms, int *lane_abort, int *lane_returned,
+                            double *lane_ms);
+
 /* The field summary of cb_field_summary (ideal_gas, then the five sums) over
  * FP64 device arrays the caller owns, allocating no memory: for callers that
  * must not allocate device memory where they need the summary (their device
