@@ -460,7 +460,7 @@ int cb_batch_autotune(cb_batch *b, int repeats, cb_batch_trial *trials, int max_
   if (!b) return fail(CB_EINVAL, "cb_batch_autotune: null batch");
   if (repeats < 1) repeats = 1;
   std::vector<cb_batch_schedule> cand;
-  const int cpc[] = {1024, 2048, 4096, 16384, 65536};
+  const int cpc[] = {1024, 2048, 4096, 8192, 16384, 32768, 65536};
   for (int v = 0; v < BATCH_VARIANTS; ++v)
     for (int c : cpc) cand.push_back(cb_batch_schedule{c, BATCH_MAX_LANE, 0, v});
   float best_ms = 1e30f;

@@ -106,6 +106,14 @@ template <typename T> struct DeckCtx {
 // The advection phases and the summary are called, not inlined: each gets
 // its own register allocation instead of sharing the whole kernel's, which
 // spills less (measured 2 % faster on the 512-deck ensemble).
+//
+// Code size: the kernel holds every phase, and its code outgrew the
+// instruction caches (ncu: "no instruction" the second stall).  So the
+// advection tiles are compiled in their edge form only (ALL_EDGE; 512-deck
+// ensemble 279 -> 241 ms FP64, 193 -> 168 ms FP32), their item loops and the
+// row loops of ideal_gas + viscosity + calc_dt, accelerate and flux_calc are
+// kept as loops instead of unrolled (then 187 ms / 129 ms with the autotuner's
+// wider choice of cells per CTA).
 template <typename T, int DIR>
 __device__ __noinline__ bool batch_advec_cell(TileCtx &cx, T *sm, DeckCtx<T> &d, int sweep, bool reset = false) {
   constexpr int TY = BATCH_ADV_TY;
@@ -116,7 +124,7 @@ __device__ __noinline__ bool batch_advec_cell(TileCtx &cx, T *sm, DeckCtx<T> &d,
   CellOut out{d.base(d.bm.spare(0)), d.base(d.bm.spare(1)), d.field(DIR == 1 ? MASS_FLUX_X : MASS_FLUX_Y)};
   if (reset) { out.density0 = d.field(DENSITY0); out.energy0 = d.field(ENERGY0); out.rfold = 1; }
   const int tx = (d.m.nx + TILE_X - 1) / TILE_X, nt = tx * ((d.m.ny + TY - 1) / TY);
-  CB_LANE_TILES(d, nt, tx, (advec_cell_tile<T, DIR, TY>(cx, sm, ms, out, d.m, d.D->off, sweep, 2, bx, by)));
+  CB_LANE_TILES(d, nt, tx, (advec_cell_tile<T, DIR, TY, true>(cx, sm, ms, out, d.m, d.D->off, sweep, 2, bx, by)));
   return true;
 }
 
@@ -132,7 +140,7 @@ __device__ __noinline__ bool batch_advec_mom(TileCtx &cx, T *sm, DeckCtx<T> &d, 
   MomOut out{d.base(d.bm.spare(2)), d.base(d.bm.spare(3))};
   if (reset) { out.xvel0 = d.field(XVEL0); out.yvel0 = d.field(YVEL0); out.rfold = 1; }
   const int tx = (d.m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((d.m.ny + 1 + TY - 1) / TY);
-  CB_LANE_TILES(d, nt, tx, (advec_mom_tile<T, DIR, TY>(cx, sm, ms, out, d.m, d.D->off, 3, sweep, fold, bx, by)));
+  CB_LANE_TILES(d, nt, tx, (advec_mom_tile<T, DIR, TY, true>(cx, sm, ms, out, d.m, d.D->off, 3, sweep, fold, bx, by)));
   return true;
 }
 
@@ -296,7 +304,7 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
       using Memo = std::conditional_t<sizeof(T) == sizeof(double), RestMemoShared<T>, RestMemo<T>>;
       Memo memo = make_memo<Memo>(sm + 4 * Box1<T, TY>::BOXS);
       for (int t = rank; t < nt; t += w)
-        CB_PHASE((ig_visc_dt_tile<T, Memo, TY>(cx, sm, ms, d.field(PRESSURE), d.field(SOUNDSPEED), d.field(VISCOSITY), m, off, D->k,
+        CB_PHASE((ig_visc_dt_tile<T, Memo, TY, true>(cx, sm, ms, d.field(PRESSURE), d.field(SOUNDSPEED), d.field(VISCOSITY), m, off, D->k,
                                                       gm1, 1, 1, t % tx, t / tx, vmin, memo)));
       block_min_to(vmin, slot);
     }
@@ -331,7 +339,7 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
       const MapSet &ms = d.ms;
       const int tx = (m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + 1 + BT::ACC - 1) / BT::ACC);
       for (int t = rank; t < nt; t += w)
-        CB_PHASE((accelerate_tile<T, BT::ACC>(cx, sm, ms, d.field(XVEL1), d.field(YVEL1), m, off, (T)dt, 2, t % tx, t / tx)));
+        CB_PHASE((accelerate_tile<T, BT::ACC, true>(cx, sm, ms, d.field(XVEL1), d.field(YVEL1), m, off, (T)dt, 2, t % tx, t / tx)));
     }
     CB_SYNC();
     {
@@ -350,7 +358,7 @@ __device__ __forceinline__ bool batch_run_deck(TileCtx &cx, T *sm, BatchDeck *D,
       const MapSet &ms = d.ms;
       const int tx = (m.nx + 1 + TILE_X - 1) / TILE_X, nt = tx * ((m.ny + 1 + BT::FLUX - 1) / BT::FLUX);
       for (int t = rank; t < nt; t += w)
-        CB_PHASE((flux_calc_tile<T, BT::FLUX>(cx, sm, ms, d.field(VOL_FLUX_X), d.field(VOL_FLUX_Y), m, off, (T)dt, 2, t % tx, t / tx)));
+        CB_PHASE((flux_calc_tile<T, BT::FLUX, true>(cx, sm, ms, d.field(VOL_FLUX_X), d.field(VOL_FLUX_Y), m, off, (T)dt, 2, t % tx, t / tx)));
     }
     CB_SYNC();
     // advection (driver/advection.cpp:29-105): the two advec_mom calls of a sweep in one pass

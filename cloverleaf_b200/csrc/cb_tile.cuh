@@ -54,10 +54,13 @@ template <int DIR, int NP, int NL> struct Items {
   static constexpr int TAIL = NA > 64 ? (NA - 64) * NB : 0;
   static constexpr int KT = (TAIL + 255) / 256;
   static constexpr int K = KB + KT;
-  template <typename F> __device__ __forceinline__ static void each(F &&f) {
+  // UNROLL = false keeps the loops as loops: one copy of f's body (for a
+  // caller that holds many phases in one kernel and must stay small)
+  template <bool UNROLL = true, typename F> __device__ __forceinline__ static void each(F &&f) {
+    constexpr int UB = UNROLL ? KB : 1, UT = UNROLL ? KT : 1;
     const int tx = threadIdx.x, ty = threadIdx.y;
     if (NA >= 64 || tx < NA) {
-#pragma unroll
+#pragma unroll UB
       for (int kb = 0; kb < KB; ++kb) {
         const int b = ty + 4 * kb;
         if (NB % 4 == 0 || b < NB) {
@@ -70,7 +73,7 @@ template <int DIR, int NP, int NL> struct Items {
     }
     if constexpr (TAIL > 0) {
       const int tid = ty * 64 + tx;
-#pragma unroll
+#pragma unroll UT
       for (int kt = 0; kt < KT; ++kt) {
         const int t = tid + 256 * kt;
         if (t < TAIL) {
@@ -473,7 +476,7 @@ __device__ __forceinline__ void eos_value(T density, T energy, T gm1, T &pressur
 // one after the other.  Staged: ms 0 density0, 1 energy0, 2 xvel0, 3 yvel0.
 static_assert(VISC_TY == DT_TY, "viscosity and calc_dt tiles of the same height");
 
-template <typename T, typename Memo, int TY = VISC_TY>
+template <typename T, typename Memo, int TY = VISC_TY, bool ROLL = false>
 __device__ __forceinline__ bool ig_visc_dt_tile(TileCtx &cx, T *sm, const MapSet &ms, T *p_out, T *c_out, T *q_out, const Mesh<T> &m,
                                                 int off, const DtConsts &k, T gm1, int ig_fold, int fold, int bx, int by, double &vmin,
                                                 Memo &memo) {
@@ -489,7 +492,7 @@ __device__ __forceinline__ bool ig_visc_dt_tile(TileCtx &cx, T *sm, const MapSet
     const bool near = edge_tile(m.nx, m.ny, x0, y0, TY);
     const bool do_fold = fold && near;
     const T cdx = m.celldx_t[i], cdx1 = m.celldx_t[i + 1];
-#pragma unroll
+#pragma unroll(ROLL ? 1 : RPT)
     for (int r = 0; r < RPT; ++r) {
       const int j = y0 + threadIdx.y + 4 * r;
       if (j >= m.ny + 2) break;
@@ -739,7 +742,7 @@ constexpr int ACC_TY = 16;
 // Staged boxes start one row above the tile (the nodes' lower cells): Box1.
 template <typename T, int TY> constexpr size_t acc_smem() { return 5 * Box1<T, TY>::BOXS * sizeof(T); }
 
-template <typename T, int TY>
+template <typename T, int TY, bool ROLL = false>
 __device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet &ms, T *u_out, T *v_out, const Mesh<T> &m, int off, T dt,
                                                 int fold, int bx, int by) {
   using B = Box1<T, TY>;
@@ -753,7 +756,7 @@ __device__ __forceinline__ bool accelerate_tile(TileCtx &cx, T *sm, const MapSet
   const int pitch = (int)m.pitch;
   const T halfdt = T(0.5) * dt;
   const T cdx = m.celldx_t[i], cdxm = m.celldx_t[i - 1];
-#pragma unroll
+#pragma unroll(ROLL ? 1 : RPT)
   for (int r = 0; r < RPT; ++r) {
     const int j = y0 + threadIdx.y + 4 * r, ly = 1 + threadIdx.y + 4 * r;
     if (j >= m.ny + 3) break;
@@ -973,7 +976,7 @@ constexpr int FLUX_TY = 16;
 // Staged boxes start one row above the tile: Box1 (the faces need rows j and j + 1).
 template <typename T, int TY> constexpr size_t flux_smem() { return 4 * Box1<T, TY>::BOXS * sizeof(T); }
 
-template <typename T, int TY>
+template <typename T, int TY, bool ROLL = false>
 __device__ __forceinline__ bool flux_calc_tile(TileCtx &cx, T *sm, const MapSet &ms, T *fx_out, T *fy_out, const Mesh<T> &m, int off, T dt,
                                                int fold, int bx, int by) {
   using B = Box1<T, TY>;
@@ -986,7 +989,7 @@ __device__ __forceinline__ bool flux_calc_tile(TileCtx &cx, T *sm, const MapSet 
   const bool do_fold = fold && edge_tile(m.nx, m.ny, x0, y0, TY);
   const int pitch = (int)m.pitch;
   const T cdx = m.celldx_t[i];
-#pragma unroll
+#pragma unroll(ROLL ? 1 : RPT)
   for (int r = 0; r < RPT; ++r) {
     const int j = y0 + threadIdx.y + 4 * r, ly = 1 + threadIdx.y + 4 * r;
     if (j >= m.ny + 3) break;
@@ -1133,7 +1136,7 @@ template <typename T, int DIR, int TY> struct CellLayout {
 // The tile's work once its boxes are staged at `sm` (density1, energy1,
 // vol_flux_x, vol_flux_y, L::BOXS elements apart); `scratch` holds the face
 // fluxes and pre_vol (L::SCRATCH_BYTES).
-template <typename T, int DIR, int TY, bool EDGE>
+template <typename T, int DIR, int TY, bool EDGE, bool COMPACT = false>
 __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, const CellOut &out, const Mesh<T> &m, int sweep, int fold,
                                                    int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
@@ -1163,7 +1166,7 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   };
   // (2) face fluxes (:63-113 / :155-205), faces a0 .. a0+LA
   const bool edge = EDGE && fold;
-  Items<DIR, L::NF, LL>::each([&](int, int p, int l) {
+  Items<DIR, L::NF, LL>::template each<!COMPACT>([&](int, int p, int l) {
     const int f = a0 + p, line = l0 + l; // position of the face along the sweep
     const int i = DIR == 1 ? f : line, j = DIR == 1 ? line : f;
     if (EDGE && (i > (DIR == 1 ? m.nx + 3 : m.nx + 1) || j > (DIR == 1 ? m.ny + 1 : m.ny + 3))) return;
@@ -1198,7 +1201,7 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
   });
   __syncthreads();
   // (3) the update (:117-129 / :209-221), mass/energy accumulation in FP64
-  Items<DIR, LA, LL>::each([&](int, int p, int l) {
+  Items<DIR, LA, LL>::template each<!COMPACT>([&](int, int p, int l) {
     const int a = a0 + p, line = l0 + l;
     const int i = DIR == 1 ? a : line, j = DIR == 1 ? line : a;
     if (EDGE && (i >= m.nx + 2 || j >= m.ny + 2)) return;
@@ -1251,7 +1254,9 @@ __device__ __forceinline__ void advec_cell_compute(const T *sm, void *scratch, c
 template <int DIR> __device__ __forceinline__ int cell_staged(int sweep) { return (sweep == 1) ? 4 : (DIR == 1 ? 3 : 4); }
 
 // One tile: staging, then the work (an edge tile keeps the extent checks).
-template <typename T, int DIR, int TY>
+// ALL_EDGE compiles the edge form only, used for every tile (the same
+// values; less code for a caller that holds many phases in one kernel).
+template <typename T, int DIR, int TY, bool ALL_EDGE = false>
 __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet &ms, const CellOut &out, const Mesh<T> &m, int off,
                                                 int sweep, int fold, int bx, int by) {
   using L = CellLayout<T, DIR, TY>;
@@ -1264,8 +1269,8 @@ __device__ __forceinline__ bool advec_cell_tile(TileCtx &cx, T *sm, const MapSet
     fill_widths(m, x0, y0, L::YH, L::BH, DIR, gx, gx + BOX_X, gv, grv);
   }
   if (!stage_wait(cx)) return false;
-  if (edge_tile(m.nx, m.ny, x0, y0, TY))
-    advec_cell_compute<T, DIR, TY, true>(sm, sm + 4 * L::BOXS, out, m, sweep, fold, bx, by);
+  if (ALL_EDGE || edge_tile(m.nx, m.ny, x0, y0, TY))
+    advec_cell_compute<T, DIR, TY, true, ALL_EDGE>(sm, sm + 4 * L::BOXS, out, m, sweep, fold, bx, by);
   else
     advec_cell_compute<T, DIR, TY, false>(sm, sm + 4 * L::BOXS, out, m, sweep, fold, bx, by);
   return true;
@@ -1383,7 +1388,7 @@ template <typename T, int DIR, int TY> struct MomLayout {
 // (no edge_tile), so the extent checks and the halo fold drop out.
 // The tile's work once its boxes are staged at `sm` (L::SMEM bytes: the
 // boxes, then the work arrays over the boxes the first stage consumes).
-template <typename T, int DIR, int TY, bool EDGE>
+template <typename T, int DIR, int TY, bool EDGE, bool COMPACT = false>
 __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, const Mesh<T> &m, int vel_mask, int sweep, int fold, int bx,
                                                   int by) {
   using L = MomLayout<T, DIR, TY>;
@@ -1443,7 +1448,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
   // (3) mom_flux (:108-133 / :180-205) over positions 1 .. LA+1
   // the sweep direction's cell widths: position a at celld[a]
   const T *celld = DIR == 1 ? sm + L::GEO + HALO - x0 : sm + L::GEO + BOX_X + YH - y0;
-  Items<DIR, LA + 1, LL>::each([&](int, int p, int l) {
+  Items<DIR, LA + 1, LL>::template each<!COMPACT>([&](int, int p, int l) {
     p += 1;
     const int a = a0 - 2 + p, line = l0 + l;
     if (EDGE && (line >= nlmax + 3 || a < 1 || a > na + 2)) return;
@@ -1466,7 +1471,7 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
 
   // (4) velocity update (:139-144 / :211-216) over positions 2 .. LA+1
   const bool do_fold = EDGE && fold;
-  Items<DIR, LA, LL>::each([&](int, int p, int l) {
+  Items<DIR, LA, LL>::template each<!COMPACT>([&](int, int p, int l) {
     p += 2;
     const int a = a0 - 2 + p, line = l0 + l;
     if (EDGE && (line > nlmax + 2 || a > na + 2)) return;
@@ -1502,8 +1507,9 @@ __device__ __forceinline__ void advec_mom_compute(T *sm, const MomOut &out, cons
 // Fields the momentum sweep stages: the other direction's volume flux only for mom_sweep 1 and 2.
 template <int DIR> __device__ __forceinline__ int mom_staged(int sweep) { return DIR + 2 * (sweep - 1) <= 2 ? 5 : 4; }
 
-// One tile: staging, then the work (an edge tile keeps the extent checks).
-template <typename T, int DIR, int TY>
+// One tile: staging, then the work (an edge tile keeps the extent checks;
+// ALL_EDGE as for advec_cell_tile).
+template <typename T, int DIR, int TY, bool ALL_EDGE = false>
 __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet &ms, const MomOut &out, const Mesh<T> &m, int off,
                                                int vel_mask, int sweep, int fold, int bx, int by) {
   using L = MomLayout<T, DIR, TY>;
@@ -1511,8 +1517,8 @@ __device__ __forceinline__ bool advec_mom_tile(TileCtx &cx, T *sm, const MapSet 
   stage_issue(cx, sm, ms, mom_staged<DIR>(sweep), L::BOXS, L::BH, off + x0 - HALO, y0 - L::YH);
   fill_widths<T>(m, x0, y0, L::YH, L::BH, DIR, sm + L::GEO, sm + L::GEO + BOX_X, nullptr, nullptr);
   if (!stage_wait(cx)) return false;
-  if (edge_tile(m.nx, m.ny, x0, y0, TY))
-    advec_mom_compute<T, DIR, TY, true>(sm, out, m, vel_mask, sweep, fold, bx, by);
+  if (ALL_EDGE || edge_tile(m.nx, m.ny, x0, y0, TY))
+    advec_mom_compute<T, DIR, TY, true, ALL_EDGE>(sm, out, m, vel_mask, sweep, fold, bx, by);
   else
     advec_mom_compute<T, DIR, TY, false>(sm, out, m, vel_mask, sweep, fold, bx, by);
   return true;
