@@ -343,17 +343,19 @@ def e2e_run(cells, warmup, steps):
 def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
     """The whole hydro loop as one device-resident CUDA graph (cb_run, without
     and with fused passes) against the host-driven loop (dt read back every
-    step), FP64, same deck, same steps; ms per step from CUDA events on the
-    chunk's stream around the whole loop (the graph's capture and
-    instantiation included)."""
+    step: the reference driver's path) -- phase by phase, with call fusion,
+    and with call fusion and the Lagrangian pass run ahead from calc_dt --
+    FP64, same deck, same steps; ms per step from CUDA events on the chunk's
+    stream around the whole loop (the graph's capture and instantiation
+    included)."""
     import torch
     from cloverleaf_b200 import Chunk, HydroRun
     out = []
     for cells, steps in sizes:
         row = {"cells": f"{cells}x{cells}", "steps": steps}
-        for mode in ("host_loop", "device_graph", "device_graph_fused"):
+        for mode in ("host_loop", "host_loop_fused_calls", "host_loop_fused_ahead", "device_graph", "device_graph_fused"):
             c = Chunk(cells, cells, device=torch.cuda.current_device())
-            r = HydroRun(c, bench_deck(cells))
+            r = HydroRun(c, bench_deck(cells), fuse_calls=mode.startswith("host_loop_fused"), dt_ahead=mode == "host_loop_fused_ahead")
             r.start()
             for _ in range(warmup):
                 r.hydro_step()
@@ -362,7 +364,7 @@ def resident_leg(sizes=((960, 87), (7680, 100)), warmup=3):
             c.synchronize()
             torch.cuda.synchronize()
             t0.record(ext)
-            if mode != "host_loop":
+            if mode.startswith("device_graph"):
                 r.run_steps_on_device(max_steps=r.step + steps, fuse=mode == "device_graph_fused")
             else:
                 for _ in range(steps):

@@ -30,7 +30,7 @@ FACE_LEFT, FACE_RIGHT, FACE_BOTTOM, FACE_TOP = 1, 2, 4, 8
 # Every symbol include/cloverb200.h declares.
 EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "cb_create", "cb_destroy", "cb_set_gamma", "cb_set_option", "cb_get_extent",
            "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk",
-           "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_pdv", "cb_revert", "cb_accelerate",
+           "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_set_dt_ahead", "cb_dt_ahead_stats", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_lagrangian", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
            "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_run", "cb_field_summary_noalloc",
            "cb_set_external_faces", "cb_copy_tile_halo",
@@ -97,6 +97,8 @@ def library() -> ctypes.CDLL:
         "cb_generate_chunk": ([P, i, ctypes.POINTER(State)], i),
         "cb_ideal_gas": ([P, i, i], i), "cb_viscosity": ([P, i], i),
         "cb_calc_dt": ([P, ctypes.POINTER(DtParams), dp, ip, ip, ip, ip], i),
+        "cb_set_dt_ahead": ([P, d, d, d], i),
+        "cb_dt_ahead_stats": ([P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)], i),
         "cb_pdv": ([P, i, d, i, i], i), "cb_revert": ([P], i), "cb_accelerate": ([P, d, i], i),
         "cb_flux_calc": ([P, d, i], i), "cb_lagrangian": ([P, d, i], i), "cb_advec_cell": ([P, i, i, i], i), "cb_advec_mom": ([P, i, i, i, i], i),
         "cb_reset_field": ([P, i], i), "cb_update_halo": ([P, ip, i], i), "cb_field_summary": ([P, dp], i),
@@ -234,6 +236,17 @@ class Chunk:
         _check(self._L.cb_calc_dt(self._h, ctypes.byref(p), ctypes.byref(dt), ctypes.byref(ctl), ctypes.byref(jl),
                                   ctypes.byref(kl), ctypes.byref(sm)))
         return dt.value, ctl.value, jl.value, kl.value, sm.value
+
+    def set_dt_ahead(self, dtold: float, dtrise: float, dtmax: float):
+        """Arms the next calc_dt to run the Lagrangian pass ahead with the
+        driver's clamp of its minimum (with call fusion; cb_set_dt_ahead)."""
+        _check(self._L.cb_set_dt_ahead(self._h, dtold, dtrise, dtmax))
+
+    def dt_ahead_stats(self):
+        """(passes run ahead, passes the four Lagrangian calls consumed)."""
+        a, u = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self._L.cb_dt_ahead_stats(self._h, ctypes.byref(a), ctypes.byref(u)))
+        return a.value, u.value
 
     def pdv(self, predict: bool, dt: float, full: bool = False, halo_depth: int = 0):
         _check(self._L.cb_pdv(self._h, int(predict), dt, int(full), halo_depth))

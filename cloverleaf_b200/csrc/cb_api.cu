@@ -36,12 +36,22 @@ int cuda_fail(cudaError_t e, const char *where) {
 
 // Every entry point on a chunk first runs the calls call fusion holds back
 // (run_pending); the phase calls that may extend a held-back group check the
-// chunk without it (CB_CHECK_CHUNK_HOLD) and decide themselves.
-#define CB_CHECK_CHUNK_HOLD(c)                                                                                                               \
+// chunk without it (CB_CHECK_CHUNK_HOLD) and decide themselves.  A Lagrangian
+// pass run ahead (cb_set_dt_ahead) is settled by every entry point but the
+// four calls it stands for (CB_CHECK_CHUNK_AHEAD), which match themselves
+// against it.
+#define CB_CHECK_CHUNK_AHEAD(c)                                                                                                              \
   do {                                                                                                                                       \
     if (!(c)) return fail(CB_EINVAL, std::string(__func__) + ": null chunk");                                                               \
     cudaError_t _e = select_device(c);                                                                                                       \
     if (_e != cudaSuccess) return cuda_fail(_e, __func__);                                                                                   \
+  } while (0)
+
+#define CB_CHECK_CHUNK_HOLD(c)                                                                                                               \
+  do {                                                                                                                                       \
+    CB_CHECK_CHUNK_AHEAD(c);                                                                                                                 \
+    cudaError_t _e1 = settle_ahead(c);                                                                                                       \
+    if (_e1 != cudaSuccess) return cuda_fail(_e1, __func__);                                                                                 \
   } while (0)
 
 #define CB_CHECK_CHUNK(c)                                                                                                                    \
@@ -126,8 +136,25 @@ cudaError_t launch_sweep_x(cb_chunk *c, int sweep, int cell_fold, int mom_fold, 
   return cudaSuccess;
 }
 
+// A Lagrangian pass run ahead that its calls did not all consume: the calls
+// that matched it so far (their work was skipped) run now, as they were made;
+// the pass's outputs are overwritten by them and by the calls still to come.
+cudaError_t settle_ahead(cb_chunk *c) {
+  DtAhead &a = c->ahead;
+  if (!a.launched) return cudaSuccess;
+  a.launched = false;
+  cudaError_t e = cudaSuccess;
+  const double dt = a.dt;
+  if (a.stage >= 1) e = dispatch(c, [&](auto ops) { return ops.pdv(*c, 1, dt, 1, a.folds[0]); });
+  if (e == cudaSuccess && a.stage >= 2) e = dispatch(c, [&](auto ops) { return ops.accelerate(*c, dt, a.folds[1]); });
+  if (e == cudaSuccess && a.stage >= 3) e = dispatch(c, [&](auto ops) { return ops.pdv(*c, 0, dt, 0, a.folds[2]); });
+  a.stage = 0;
+  return e;
+}
+
 // Runs the calls call fusion held back, one by one as they were made.
 cudaError_t run_pending(cb_chunk *c) {
+  if (cudaError_t e0 = settle_ahead(c)) return e0;
   const Pending p = c->pend;
   c->pend = Pending{};
   cudaError_t e = cudaSuccess;
@@ -214,6 +241,10 @@ void release(cb_chunk *c) {
   if (c->h_scalars) cudaFreeHost(c->h_scalars);
   if (c->ev_order) cudaEventDestroy(c->ev_order);
   c->ev_order = nullptr;
+  if (c->ev_dt) cudaEventDestroy(c->ev_dt);
+  c->ev_dt = nullptr;
+  if (c->d_dt_ahead) cudaFree(c->d_dt_ahead);
+  c->d_dt_ahead = nullptr;
   if (c->stream) cudaStreamDestroy(c->stream);
   c->d_dt_bits = nullptr;
   c->d_partials = nullptr;
@@ -320,6 +351,33 @@ int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 cudaError_t run_pending_calls(cb_chunk *c) { return run_pending(c); }
 } // namespace cb
 
+namespace {
+
+// The driver's dt from calc_dt's minimum (driver/timestep.cpp:93):
+// min(min(dtlp, dtold * dtrise), dtmax), in the same order on the host and on
+// the device (std::min(a, b) is b < a ? b : a).
+__host__ __device__ inline double driver_dt_clamp(double dtlp, double dtold, double dtrise, double dtmax) {
+  const double r = dtold * dtrise;
+  const double m = r < dtlp ? r : dtlp;
+  return dtmax < m ? dtmax : m;
+}
+
+__global__ void k_dt_ahead(const unsigned long long *dt_bits, double dtold, double dtrise, double dtmax, double *dt_out) {
+  *dt_out = driver_dt_clamp(__longlong_as_double((long long)*dt_bits), dtold, dtrise, dtmax);
+}
+
+// Whether a call is the next of the four the pass run ahead stands for
+// (stage: the calls matched before it), with the pass's dt and halo depth;
+// if so it counts as matched.  A call that does not match settles the pass.
+bool ahead_match(cb_chunk *c, int stage, double dt, int fold) {
+  DtAhead &a = c->ahead;
+  if (!a.launched || a.stage != stage || a.dt != dt || a.folds[stage] != fold) return false;
+  a.stage = stage + 1;
+  return true;
+}
+
+} // namespace
+
 extern "C" {
 
 int cb_version(void) { return 1; }
@@ -386,6 +444,7 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
   };
   if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
   if ((e = cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+  if ((e = cudaEventCreateWithFlags(&c->ev_dt, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
   for (int b = 0; b < NUM_BUF; ++b)
     if ((e = cudaMalloc(&c->buf[b], bytes)) != cudaSuccess) return bail(e, "fields");
   for (int f = 0; f < 15; ++f) c->fbuf[f] = f;
@@ -410,6 +469,7 @@ int cb_create(int nx, int ny, int precision, int device, cb_chunk **out) {
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   c->summary_grid = c->sms * 8;
   if ((e = cudaMalloc(&c->d_dt_bits, sizeof(unsigned long long))) != cudaSuccess) return bail(e, "scratch");
+  if ((e = cudaMalloc(&c->d_dt_ahead, sizeof(double))) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&c->d_partials, sizeof(double) * 5 * (size_t)c->summary_grid)) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&c->d_counter, sizeof(unsigned int))) != cudaSuccess) return bail(e, "scratch");
   if ((e = cudaMalloc(&c->d_sums, sizeof(double) * 5)) != cudaSuccess) return bail(e, "scratch");
@@ -637,6 +697,24 @@ int cb_viscosity(cb_chunk *c, int halo_depth) {
   return CB_OK;
 }
 
+int cb_set_dt_ahead(cb_chunk *c, double dtold, double dtrise, double dtmax) {
+  CB_CHECK_CHUNK_AHEAD(c);
+  if (!(dtold > 0.0) || !(dtrise > 0.0) || !(dtmax > 0.0))
+    return fail(CB_EINVAL, "cb_set_dt_ahead: dtold, dtrise and dtmax must be positive");
+  c->ahead.armed = true;
+  c->ahead.dtold = dtold;
+  c->ahead.dtrise = dtrise;
+  c->ahead.dtmax = dtmax;
+  return CB_OK;
+}
+
+int cb_dt_ahead_stats(const cb_chunk *c, long long *launched, long long *used) {
+  if (!c) return fail(CB_EINVAL, "cb_dt_ahead_stats: null chunk");
+  if (launched) *launched = c->ahead.launched_count;
+  if (used) *used = c->ahead.used_count;
+  return CB_OK;
+}
+
 int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *control, int *jldt, int *kldt, int *small) {
   CB_CHECK_CHUNK_HOLD(c);
   if (!p || !dt_min_val) return fail(CB_EINVAL, "cb_calc_dt: null argument");
@@ -644,6 +722,10 @@ int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *cont
   const bool fused = held.kind == PEND_IG_VISC;
   if (!fused) CB_CUDA(run_pending(c));
   c->pend = Pending{};
+  DtAhead &ah = c->ahead;
+  // the Lagrangian pass goes ahead when armed, with the fused pass, on a folding chunk outside cb_run
+  const bool ahead = ah.armed && fused && c->fuse_calls && c->can_fold() && !c->dt_dev;
+  ah.armed = false;
   DtConsts k{p->dtc_safe, p->dtu_safe, p->dtv_safe, p->dtdiv_safe};
   c->h_scalars[0] = g_big;
   CB_CUDA(cudaMemcpyAsync(c->d_dt_bits, &c->h_scalars[0], sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -652,8 +734,32 @@ int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *cont
   else
     CB_CUDA(dispatch(c, [&](auto ops) { return ops.calc_dt(*c, k); }));
   CB_CUDA(cudaMemcpyAsync(&c->h_scalars[1], c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CB_CUDA(cudaStreamSynchronize(c->stream));
-  if (int r = check_device_error(c, "cb_calc_dt")) return r;
+  if (ahead) {
+    // the staging-error flag comes back with the minimum; then the pass is
+    // enqueued behind the read-back, with the clamped dt read on the device
+    int *h_err = reinterpret_cast<int *>(&c->h_scalars[7]);
+    CB_CUDA(cudaMemcpyAsync(h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CB_CUDA(cudaEventRecord(c->ev_dt, c->stream));
+    k_dt_ahead<<<1, 1, 0, c->stream>>>(c->d_dt_bits, ah.dtold, ah.dtrise, ah.dtmax, c->d_dt_ahead);
+    c->launches += 1;
+    CB_CUDA(cudaGetLastError());
+    const int f1 = effective_fold(c, 1), f2 = effective_fold(c, 2);
+    c->dt_dev = c->d_dt_ahead;
+    const cudaError_t le = dispatch(c, [&](auto ops) { return ops.lagrange(*c, c->spare_base(4), 0.0, f1, f2, f2, f2, true); });
+    c->dt_dev = nullptr;
+    CB_CUDA(le);
+    CB_CUDA(cudaEventSynchronize(c->ev_dt));
+    if (*h_err) return fail(CB_ECUDA, "cb_calc_dt: a kernel's tile staging did not complete (TMA wait limit reached)");
+    ah.launched = true;
+    ah.stage = 0;
+    ah.dt = driver_dt_clamp(c->h_scalars[1], ah.dtold, ah.dtrise, ah.dtmax);
+    ah.folds[0] = f1;
+    ah.folds[1] = ah.folds[2] = ah.folds[3] = f2;
+    ah.launched_count += 1;
+  } else {
+    CB_CUDA(cudaStreamSynchronize(c->stream));
+    if (int r = check_device_error(c, "cb_calc_dt")) return r;
+  }
   const double dt = c->h_scalars[1];
   *dt_min_val = dt;
   // src/serial/calc_dt.cpp:73-79: control is always "sound" (jk_control = 1.1)
@@ -668,11 +774,13 @@ int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *cont
 }
 
 int cb_pdv(cb_chunk *c, int predict, double dt, int full, int halo_depth) {
-  CB_CHECK_CHUNK_HOLD(c);
+  CB_CHECK_CHUNK_AHEAD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   if (full && !predict) return fail(CB_EINVAL, "cb_pdv: full = 1 is the predictor step; use predict = 1");
   const int fold = effective_fold(c, halo_depth);
-  if (!predict && !full && c->pend.kind == PEND_PDV1_ACC && c->pend.dt == dt && fold > 0) {
+  if ((full && ahead_match(c, 0, dt, fold)) || (!predict && !full && ahead_match(c, 2, dt, fold))) {
+    // done by the pass run ahead
+  } else if (!predict && !full && c->pend.kind == PEND_PDV1_ACC && c->pend.dt == dt && fold > 0) {
     // the corrector, held back with the predictor and accelerate for flux_calc's pass
     c->pend.kind = PEND_PDV1_ACC_PDV0;
     c->pend.pdv0_fold = fold;
@@ -711,10 +819,12 @@ int cb_revert(cb_chunk *c) {
 }
 
 int cb_accelerate(cb_chunk *c, double dt, int halo_depth) {
-  CB_CHECK_CHUNK_HOLD(c);
+  CB_CHECK_CHUNK_AHEAD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
-  if (c->pend.kind == PEND_PDV1 && c->pend.dt == dt && fold > 0) { // held back with the predictor
+  if (ahead_match(c, 1, dt, fold)) {
+    // done by the pass run ahead
+  } else if (c->pend.kind == PEND_PDV1 && c->pend.dt == dt && fold > 0) { // held back with the predictor
     c->pend.kind = PEND_PDV1_ACC;
     c->pend.acc_fold = fold;
   } else {
@@ -726,11 +836,16 @@ int cb_accelerate(cb_chunk *c, double dt, int halo_depth) {
 }
 
 int cb_flux_calc(cb_chunk *c, double dt, int halo_depth) {
-  CB_CHECK_CHUNK_HOLD(c);
+  CB_CHECK_CHUNK_AHEAD(c);
   if (int r = check_depth(halo_depth, true)) return r;
   const int fold = effective_fold(c, halo_depth);
   const Pending held = c->pend;
-  if (held.kind == PEND_PDV1_ACC_PDV0 && held.dt == dt && fold > 0) {
+  if (ahead_match(c, 3, dt, fold)) { // the pass run ahead is complete: its predicted pressure went to the spare
+    c->ahead.launched = false;
+    c->ahead.stage = 0;
+    c->ahead.used_count += 1;
+    std::swap(c->fbuf[PRESSURE], c->sbuf[4]);
+  } else if (held.kind == PEND_PDV1_ACC_PDV0 && held.dt == dt && fold > 0) {
     // the predictor, accelerate, the corrector and flux_calc as one pass (cb_lagrangian's)
     c->pend = Pending{};
     CB_CUDA(dispatch(c, [&](auto ops) {

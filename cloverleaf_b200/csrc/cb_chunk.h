@@ -44,6 +44,22 @@ struct Pending {
   int mom_fold = 0, mom_mask = 0;                  // its momentum sweep (the second sweep's)
 };
 
+// The Lagrangian pass run ahead (cb_set_dt_ahead): cb_calc_dt, with the
+// driver's dt clamp in hand, also enqueues the pass with the clamped dt on
+// the device, so the GPU keeps working while the host reads the minimum
+// back; the four calls that follow are checked against it (dt and halo
+// depths) and find their work done.  A call out of that sequence first
+// enqueues the calls it already stood for.
+struct DtAhead {
+  bool armed = false;             // set for the next cb_calc_dt
+  double dtold = 0.0, dtrise = 0.0, dtmax = 0.0;
+  bool launched = false;          // the pass is enqueued
+  double dt = 0.0;                // its dt: the host's clamp of the read-back minimum
+  int folds[4] = {};              // predictor (pressure), accelerate, corrector, flux_calc
+  int stage = 0;                  // calls matched: 1 predictor, 2 accelerate, 3 corrector
+  long long launched_count = 0, used_count = 0; // passes run ahead / consumed
+};
+
 struct Chunk {
   int nx = 0, ny = 0;
   int precision = 0; // 0 FP64, 1 FP32
@@ -86,6 +102,9 @@ struct Chunk {
   bool fold_enabled = true;    // fold halos into producers when the mesh allows it
   bool fuse_calls = false;     // call fusion (CB_OPT_FUSE_CALLS), with folding producers
   Pending pend;                // calls held back by call fusion
+  DtAhead ahead;               // the Lagrangian pass run ahead of its calls
+  double *d_dt_ahead = nullptr; // its dt on the device
+  cudaEvent_t ev_dt = nullptr;  // the dt read-back's completion
 
   long long launches = 0; // kernels launched for this chunk
   // When set, the phases that take dt (PdV, accelerate, flux_calc) read it

@@ -36,7 +36,8 @@ class HydroRun:
     """State of one run: globals.step, time, dt, dtold, advect_x (driver/definitions.h:258-280)."""
 
     def __init__(self, chunk: Chunk, deck: Deck, fold: bool = True, forced_dt: Optional[List[float]] = None,
-                 probe: Optional[Callable[[str], None]] = None, lagrangian: bool = False, fuse_calls: bool = False):
+                 probe: Optional[Callable[[str], None]] = None, lagrangian: bool = False, fuse_calls: bool = False,
+                 dt_ahead: bool = False):
         self.c = chunk
         self.deck = deck
         self.fold = fold
@@ -46,6 +47,10 @@ class HydroRun:
         chunk.set_option(OPT_FUSE_CALLS, int(fuse_calls))
         # lagrangian: the PdV / accelerate / PdV / flux_calc calls as one cb_lagrangian call
         self.lagrangian = lagrangian
+        # dt_ahead: each calc_dt also runs the Lagrangian pass ahead with this
+        # loop's dt clamp (cb_set_dt_ahead; with fuse_calls), and the four
+        # Lagrangian calls find it done
+        self.dt_ahead = dt_ahead
         # forced_dt replays a recorded dt sequence (calc_dt still runs); probe(name)
         # is called as each phase is about to be enqueued ("end" closes a step)
         self.forced_dt = forced_dt
@@ -90,6 +95,8 @@ class HydroRun:
         c.viscosity(self._depth(1))
         c.update_halo([Q], 1)
         self._mark("calc_dt")
+        if self.dt_ahead and self.forced_dt is None:
+            c.set_dt_ahead(self.dtold, d.dtrise, d.dtmax)
         dtlp, control, jldt, kldt, small = c.calc_dt(d.dtmin, d.dtc_safe, d.dtu_safe, d.dtv_safe, d.dtdiv_safe)
         if self.forced_dt is not None:
             dtlp = self.forced_dt[self.step - 1]

@@ -14,6 +14,7 @@ struct Runtime {
   cb_chunk *chunk = nullptr; // the one tile's chunk (tiles_per_chunk 1)
   bool fold = true;          // fold update_halo into the producing kernels
   bool fuse = true;          // run the driver's phase calls as the library's fused passes (CB_OPT_FUSE_CALLS)
+  bool ahead = true;         // with fuse: calc_dt also runs the Lagrangian pass ahead (cb_set_dt_ahead)
   // advec_mom pairing (driver/advection.cpp:56-57, :85-86): the which_vel 1
   // call advances both velocity components; the matching which_vel 2 call
   // of the same sweep is then a no-op.

@@ -1,7 +1,11 @@
 // calc_dt.cpp -- driver/calc_dt.h:26-27.  The minimum over the mesh is taken
 // on the device; the host receives dt_min_val and forms control / jldt /
 // kldt as src/serial/calc_dt.cpp:73-79 does.  The small-timestep diagnostic
-// of :85-110 is printed from device data when it triggers.
+// of :85-110 is printed from device data when it triggers.  With fused calls
+// the library is first given the driver's dt clamp (driver/timestep.cpp:93:
+// dtold, dtrise, dtmax), so the Lagrangian pass runs on the GPU while the
+// host reads the minimum back and prints the step line (not with --dump,
+// whose files between the phases would show the pass's outputs early).
 #include "calc_dt.h"
 #include "b200_runtime.h"
 
@@ -23,6 +27,9 @@ void calc_dt(global_variables &globals, int tile, double &local_dt, std::string 
   const global_config &cfg = globals.config;
   cb_dt_params p{cfg.dtmin, cfg.dtc_safe, cfg.dtu_safe, cfg.dtv_safe, cfg.dtdiv_safe};
   int l_control = 0, small = 0;
+  const clover::Runtime *rt = globals.context.rt.get();
+  if (rt && rt->fold && rt->fuse && rt->ahead && cfg.dumpDir.empty())
+    clover::b200_check(cb_set_dt_ahead(c, globals.dtold, cfg.dtrise, cfg.dtmax), "calc_dt");
   clover::b200_check(cb_calc_dt(c, &p, &local_dt, &l_control, &jldt, &kldt, &small), "calc_dt");
   if (small != 0) {
     const int nx = globals.chunk.tiles[tile].info.t_xmax - globals.chunk.tiles[tile].info.t_xmin + 1;

@@ -8,6 +8,8 @@
 //   CLOVER_B200_FOLD      = 1 (default) | 0        fold update_halo into producers
 //   CLOVER_B200_FUSE      = 1 (default) | 0        the driver's phase calls as fused passes
 //                                                  (with folding; results unchanged)
+//   CLOVER_B200_AHEAD     = 1 (default) | 0        with fused calls: calc_dt runs the
+//                                                  Lagrangian pass ahead (not with --dump)
 #include "initialise.h"
 #include "b200_runtime.h"
 
@@ -45,6 +47,7 @@ model create_context(bool silent, const std::vector<std::string> &args) {
   }
   if (const char *f = std::getenv("CLOVER_B200_FOLD")) ctx.rt->fold = std::strcmp(f, "0") != 0;
   if (const char *f = std::getenv("CLOVER_B200_FUSE")) ctx.rt->fuse = std::strcmp(f, "0") != 0;
+  if (const char *f = std::getenv("CLOVER_B200_AHEAD")) ctx.rt->ahead = std::strcmp(f, "0") != 0;
   return {ctx, "B200 (sm_100a CUDA, libcloverb200)", true, parsed};
 }
 
@@ -54,5 +57,7 @@ void report_context(const clover::context &ctx) {
   std::cout << " - Device:    " << name << "\n"
             << " - Precision: " << (ctx.precision == CB_FP64 ? "fp64" : "fp32") << "\n"
             << " - Halo fold: " << (ctx.rt && ctx.rt->fold ? "on" : "off") << "\n"
-            << " - Fused calls: " << (ctx.rt && ctx.rt->fold && ctx.rt->fuse ? "on" : "off") << std::endl;
+            << " - Fused calls: " << (ctx.rt && ctx.rt->fold && ctx.rt->fuse ? "on" : "off")
+            << ", Lagrangian pass ahead of its calls: " << (ctx.rt && ctx.rt->fold && ctx.rt->fuse && ctx.rt->ahead ? "on" : "off")
+            << std::endl;
 }

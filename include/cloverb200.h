@@ -128,6 +128,23 @@ int cb_viscosity(cb_chunk *c, int halo_depth);
 /* driver/calc_dt.h:26-27 -- the minimum over cells, on the device; returns the
  * kernel's dt_min_val and control/jldt/kldt/small as src/serial/calc_dt.cpp:73-79 forms them. */
 int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *control, int *jldt, int *kldt, int *small);
+/* The Lagrangian pass run ahead (no counterpart in the reference; for the
+ * driver's step under CB_OPT_FUSE_CALLS).  Arms the next cb_calc_dt -- when it
+ * is the fused ideal_gas + viscosity + calc_dt pass on a folding chunk -- to
+ * enqueue, behind the minimum's read-back, the Lagrangian pass with the dt
+ * the driver will take, min(min(minimum, dtold * dtrise), dtmax)
+ * (driver/timestep.cpp:93), formed on the device: the GPU keeps working while
+ * the host reads the minimum back.  The four calls that follow --
+ * cb_pdv(predictor, full), cb_accelerate, cb_pdv(corrector), cb_flux_calc
+ * with halo depths 1, 2, 2, 2 -- find their work done when their dt is that
+ * clamp's (host arithmetic, the same order); any other call, or a different
+ * dt or depth, first enqueues the calls matched so far, and the results are
+ * those of the calls made one by one (FP64 to the bit).  Until the four
+ * calls are made, level-1 fields, soundspeed and the volume fluxes hold the
+ * pass's outputs.  One-shot: arm before each cb_calc_dt. */
+int cb_set_dt_ahead(cb_chunk *c, double dtold, double dtrise, double dtmax);
+/* Passes run ahead, and those the four calls consumed, since cb_create. */
+int cb_dt_ahead_stats(const cb_chunk *c, long long *launched, long long *used);
 /* driver/PdV.h:24.  full = 0: the PdV kernel alone (src/serial/PdV.cpp:36-87);
  * full = 1 with predict = 1: the model's whole predictor step (:92-133:
  * kernel, ideal_gas on level 1, depth-1 pressure halo, revert) in one pass. */

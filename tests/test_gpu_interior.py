@@ -11,7 +11,9 @@ of the other run tests never reach that form.  Here:
   test_problem 2) through the fused device-resident graph (cb_run, fuse = 1),
   through the host loop with the fused Lagrangian pass (cb_lagrangian),
   through the host loop with call fusion (every fused pass, the x sweeps as
-  one pass each) and through the unfused graph: the dt of every step equal to the oracle's, every
+  one pass each), the same with the Lagrangian pass run ahead from calc_dt
+  (cb_set_dt_ahead: every pass consumed by its four calls) and through the
+  unfused graph: the dt of every step equal to the oracle's, every
   final per-cell field bit-identical to the oracle's, every state field
   (halos included) bit-identical to the phase-by-phase host loop, the
   driver's PASS check, and the summaries within 5e-11 of the reference's
@@ -56,9 +58,11 @@ class OracleRun:
 
 def run_path(dk, path, precision=FP64):
     c = Chunk(dk.x_cells, dk.y_cells, precision=precision, gamma=dk.gamma)
-    r = HydroRun(c, dk, lagrangian=(path == "lagrangian"), fuse_calls=(path == "fuse_calls"))
-    if path in ("host", "lagrangian", "fuse_calls"):
+    r = HydroRun(c, dk, lagrangian=(path == "lagrangian"), fuse_calls=(path in ("fuse_calls", "ahead")), dt_ahead=(path == "ahead"))
+    if path in ("host", "lagrangian", "fuse_calls", "ahead"):
         r.run()
+        if path == "ahead":  # every step's Lagrangian pass ran ahead and was consumed
+            assert c.dt_ahead_stats() == (r.step, r.step)
     else:
         r.start()
         assert r.run_steps_on_device(fuse=(path == "fused"))
@@ -99,7 +103,7 @@ def config1():
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("path", ["fused", "lagrangian", "fuse_calls", "graph"])
+@pytest.mark.parametrize("path", ["fused", "lagrangian", "fuse_calls", "ahead", "graph"])
 def test_config1_fused_paths_match_oracle(config1, path):
     dk, ref, (ch, rh) = config1
     c, r = run_path(dk, path)
@@ -159,7 +163,7 @@ def circle():
     host[0].close()
 
 
-@pytest.mark.parametrize("path", ["fused", "lagrangian", "fuse_calls"])
+@pytest.mark.parametrize("path", ["fused", "lagrangian", "fuse_calls", "ahead"])
 def test_circle_200x170_fused_paths(circle, path):
     dk, ref, (ch, _) = circle
     c, r = run_path(dk, path)
