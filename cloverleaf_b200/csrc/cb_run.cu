@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <initializer_list>
 #include <string>
@@ -56,6 +57,7 @@ int cuda_fail(cudaError_t e, const char *where) {
 struct RunState {
   double dt, dtold, time;
   int step, nsum, sum_runs, small, advect_x, records_due;
+  int last; // the step under way is the run's last (k_run_end will stop the loop)
 };
 
 struct RunConsts {
@@ -94,6 +96,8 @@ __global__ void k_run_dt(RunState *s, const unsigned long long *dt_bits, RunCons
   m = m < dt ? m : dt;
   dt = k.dtmax < m ? k.dtmax : m;
   if (dt < k.dtmin) s->small = 1;
+  // k_run_end's stop test, with the same time sum
+  s->last = s->time + dt + g_small > k.end_time || s->step >= k.end_step || s->step >= k.last_step || s->small;
   s->dt = dt;
   s->dtold = dt;
   *dt_dev = dt;
@@ -165,6 +169,10 @@ template <typename T> struct Seq {
   // PdV corrector + flux_calc in one pass, and reset_field done by the
   // second sweeps; the freshness moves exactly as unfused
   bool fuse = false;
+  // fused: the run's last-step flag on the device; the Lagrangian pass
+  // stores the predicted pressure and soundspeed in that step only, and the
+  // fused ideal_gas pass no soundspeed (both rewritten unread otherwise)
+  const int *last_flag = nullptr;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
 
@@ -209,7 +217,7 @@ template <typename T> struct Seq {
     // passes between them are none: density0 / energy0 and q are fresh),
     // the pressure written to its second buffer (see lagrange)
     if (fuse) swap_pressure();
-    if (emit) run(fuse ? Ops<T>::ig_visc_dt(c, dk, fi, fv) : Ops<T>::calc_dt(c, dk));
+    if (emit) run(fuse ? Ops<T>::ig_visc_dt(c, dk, fi, fv, last_flag == nullptr) : Ops<T>::calc_dt(c, dk));
     ++pos;
   }
   // Fused, the predicted pressure goes to the other of two buffers: the pass
@@ -224,7 +232,7 @@ template <typename T> struct Seq {
     const int ff = eff(dep(2));
     if (fuse) {
       // fused: the whole Lagrangian step in one pass
-      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), 0.0, fp, fa, fc, ff, false));
+      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), 0.0, fp, fa, fc, ff, false, last_flag));
       swap_pressure();
     } else if (emit) {
       run(Ops<T>::pdv(c, 1, 0.0, 1, fp));
@@ -541,6 +549,7 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
   }
   Seq<T> q(*c, true, fold, dk);
   q.fuse = p->fuse != 0 && fold && c->can_fold();
+  if (q.fuse) q.last_flag = reinterpret_cast<const int *>(reinterpret_cast<const char *>(rb.st) + offsetof(RunState, last));
   std::memcpy(q.fresh, settled[3], sizeof q.fresh);
   const cudaStream_t user = c->stream;
   const long long launches0 = c->launches;

@@ -503,7 +503,7 @@ __device__ __forceinline__ bool ig_visc_dt_tile(TileCtx &cx, T *sm, const MapSet
       T p, ss;
       eos_value(D[b], E[b], gm1, p, ss);
       p_out[g] = p;
-      c_out[g] = ss;
+      if (c_out) c_out[g] = ss; // null in the resident loop: the step's Lagrangian pass rewrites it unread
       if (ig_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), ig_fold, i, j, p);
       const T dd = D[b];
       const T pl = gm1 * D[b - 1] * E[b - 1];
@@ -841,8 +841,12 @@ template <int NA, int NB, typename F> __device__ __forceinline__ void each_rows(
   }
 }
 
+// store_ps: when set, the predicted pressure and soundspeed are stored only
+// if *store_ps is nonzero (the resident loop's last step: in the others the
+// next step's pass rewrites both before anything reads them).
 template <typename T> struct LagOut {
   T *pressure, *soundspeed, *xvel1, *yvel1, *density1, *energy1, *vol_flux_x, *vol_flux_y;
+  const int *store_ps = nullptr;
 };
 struct LagFolds {
   int pressure, accelerate, pdv, flux;
@@ -864,6 +868,7 @@ __device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &
   fill_widths(m, x0, y0, 1, L::BH, 1, gx, gy, nullptr, nullptr); // gx[i - x0 + HALO] = celldx[i], gy[j - y0 + 1] = celldy[j]
   if (!stage_wait(cx)) return false;
   const int pitch = (int)m.pitch;
+  const bool store_ps = !out.store_ps || *out.store_ps != 0;
   // (1) the predictor over the pressure ring
   each_rows<L::PCX, L::PCY>([&](int p, int l) {
     const int i = x0 - 1 + p, j = y0 - 1 + l;
@@ -877,7 +882,7 @@ __device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &
     pdv_value(true, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X], V0[b + BOX_X + 1],
               z, z, z, z, z, z, z, z, D0[b], E0[b], P[b], Q[b], d1, e1);
     sp[l * L::PCX + p] = gm1 * d1 * e1; // eos_value's pressure
-    if (p >= 1 && p <= TILE_X && l >= 1 && l <= TY && (!EDGE || (i == ic && j == jc))) { // one of the tile's own interior cells
+    if (store_ps && p >= 1 && p <= TILE_X && l >= 1 && l <= TY && (!EDGE || (i == ic && j == jc))) { // one of the tile's own interior cells
       T pp, cc;
       eos_value(d1, e1, gm1, pp, cc);
       const int g = gidx(pitch, i, j);
