@@ -47,7 +47,8 @@ template <typename T> struct Ops {
   // new energy and velocities go to level 0 alone.  sweep_x_fusable: whether
   // the mesh has such tiles (otherwise the call is refused).
   static bool sweep_x_fusable(const Chunk &c);
-  static cudaError_t advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fold, int reset_fold, bool level0_only);
+  static cudaError_t advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fold, int reset_fold, bool level0_only,
+                                   const int *store_mf = nullptr);
   static cudaError_t reset_field(Chunk &c, int fold);
   // level 1 as the phase-by-phase step leaves it, after steps whose second
   // sweeps wrote energy and velocities to level 0 only: energy1 from level 0

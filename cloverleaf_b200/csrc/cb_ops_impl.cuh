@@ -262,7 +262,8 @@ template <typename T> bool Ops<T>::sweep_x_fusable(const Chunk &c) {
 }
 
 template <typename T>
-cudaError_t Ops<T>::advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fold, int reset_fold, bool level0_only) {
+cudaError_t Ops<T>::advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fold, int reset_fold, bool level0_only,
+                                  const int *store_mf) {
   constexpr int TY = AdvecTiles<T>::CELL_X;
   static_assert(AdvecTiles<T>::MOM_X == TY, "the x sweep's cell and momentum tiles of the same height");
   if (!sweep_x_fusable(c) || cell_fold != 2 || (level0_only && reset_fold < 0)) return cudaErrorNotSupported;
@@ -275,6 +276,7 @@ cudaError_t Ops<T>::advec_sweep_x(Chunk &c, int sweep, int cell_fold, int mom_fo
     if ((e = copy_ring<T>(c, rp, 2, 2, c.nx + 2, 2, c.ny + 2, c.nx + 5, c.ny + 5)) != cudaSuccess) return e;
   }
   SweepOut so;
+  so.store_mf = store_mf;
   so.cell = CellOut{dd, level0_only ? nullptr : de, c.base(mf)};
   so.mom = MomOut{level0_only ? nullptr : du, level0_only ? nullptr : dv};
   if (reset_fold >= 0) {

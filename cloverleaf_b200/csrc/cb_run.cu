@@ -170,8 +170,10 @@ template <typename T> struct Seq {
   // second sweeps; the freshness moves exactly as unfused
   bool fuse = false;
   // fused: the run's last-step flag on the device; the Lagrangian pass
-  // stores the predicted pressure and soundspeed in that step only, and the
-  // fused ideal_gas pass no soundspeed (both rewritten unread otherwise)
+  // stores the predicted pressure and soundspeed in that step only, the
+  // fused x sweep the mass flux of the tiles the edge strip does not read,
+  // and the fused ideal_gas pass no soundspeed (all rewritten unread
+  // otherwise)
   const int *last_flag = nullptr;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
@@ -290,7 +292,7 @@ template <typename T> struct Seq {
       return;
     }
     const int f = eff(dep(2)), fm = eff(mom_depth);
-    if (emit) run(Ops<T>::advec_sweep_x(c, sweep, f, fm, reset_tail(last), last));
+    if (emit) run(Ops<T>::advec_sweep_x(c, sweep, f, fm, reset_tail(last), last, last_flag));
     std::swap(c.fbuf[DENSITY1], c.sbuf[0]);
     std::swap(c.fbuf[ENERGY1], c.sbuf[1]);
     wrote({D1, E1, MFX}, f);

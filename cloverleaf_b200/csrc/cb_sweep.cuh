@@ -50,6 +50,12 @@ template <typename T, int TY> struct SweepXLayout {
 struct SweepOut {
   CellOut cell; // density1 / energy1 (spares), mass_flux_x, level 0 when set
   MomOut mom;   // xvel1 / yvel1 (spares, or null for level 0 only), level 0 when set
+  // when set: the mass flux is stored by the tiles on the border of the
+  // interior rectangle (the edge strip's momentum tiles read it), and by the
+  // others only if *store_mf is nonzero (the resident loop's last step: the
+  // pass's own momentum update takes it from shared memory, and the next
+  // sweep in x rewrites it unread)
+  const int *store_mf = nullptr;
 };
 
 // The interior tile (bx, by) of the x sweep; staged: ms 0 density1,
@@ -91,6 +97,8 @@ __device__ __forceinline__ void sweep_x_tile(TileCtx &cx, T *sm, const Maps &map
     const T vol = g_x[i - x0 + HALO] * g_y[j - y0 + 1];
     return sweep == 1 ? cell_pre_vol1(vol, VFX[b], VFX[b + 1], VFY[b], VFY[b + BOX_X]) : cell_pre_vol2(vol, VFX[b], VFX[b + 1]);
   };
+  const bool border = blockIdx.x == 0 || blockIdx.x == gridDim.x - 1 || blockIdx.y == 0 || blockIdx.y == gridDim.y - 1;
+  const bool store_mf = border || !out.store_mf || *out.store_mf != 0;
   // (A) face fluxes (advec_cell.cpp:63-113), faces x0-2+p on lines y0-1+l
   Items<1, NFACE, NLC>::each([&](int, int p, int l) {
     const int f = x0 - 2 + p, j = y0 - 1 + l;
@@ -112,7 +120,7 @@ __device__ __forceinline__ void sweep_x_tile(TileCtx &cx, T *sm, const Maps &map
     cell_face_value(flux, pre_vol_of(donor, j), ratio, D1[bd], D1[bu], D1[bw], E1[bd], E1[bu], E1[bw], mass_flux, e_adv);
     s_mf[l * NFACE + p] = (double)mass_flux;
     s_ef[l * NFACE + p] = (double)mass_flux * (double)e_adv; // FP32: the exact product
-    if (p >= 2 && p < TILE_X + 2 && l >= 1) ((T *)out.cell.mass_flux)[gidx(pitch, f, j)] = mass_flux;
+    if (store_mf && p >= 2 && p < TILE_X + 2 && l >= 1) ((T *)out.cell.mass_flux)[gidx(pitch, f, j)] = mass_flux;
   });
   __syncthreads();
   // (B) the cell update (advec_cell.cpp:117-129) on cells x0-2+p, lines y0-1+l,
