@@ -62,13 +62,13 @@ template <typename T> struct Ops {
   static cudaError_t tile_halo(Chunk &dst, const Chunk &src, int side, const HaloJob &job, int depth);
   static cudaError_t field_summary(Chunk &c);
   // fused passes of the resident loop: ideal_gas + viscosity + calc_dt, and the Lagrangian step
-  static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold, bool write_ss = true);
+  static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold, bool write_ss = true, bool write_p = true);
   // the PdV predictor, accelerate, the PdV corrector and flux_calc in one
   // pass, every output folded (depths above zero); the predicted pressure
   // goes to p_out, with the pressure's outer halo ring (which the pass does
   // not write) copied there first when keep_ring is set
   static cudaError_t lagrange(Chunk &c, void *p_out, double dt, int p_fold, int acc_fold, int pdv_fold, int flux_fold, bool keep_ring,
-                              const int *store_ps = nullptr);
+                              const int *store_ps = nullptr, bool p_from_de = false);
 };
 
 extern template struct Ops<double>;

@@ -351,7 +351,7 @@ template <typename T> cudaError_t Ops<T>::tile_halo(Chunk &dst, const Chunk &src
   return launched(dst);
 }
 
-template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold, bool write_ss) {
+template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold, bool write_ss, bool write_p) {
   constexpr int TY = VISC_TY;
   using B = Box1<T, TY>;
   const size_t smem = (4 * B::BOXS + (sizeof(T) == sizeof(double) ? REST_MEMO_ELEMS : 0)) * sizeof(T);
@@ -361,7 +361,8 @@ template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k
   int per_sm = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt_ig_visc_dt<T>, 256, smem)) != cudaSuccess) return e;
   const int grid = std::min(nt, c.sms * std::max(per_sm, 1));
-  kt_ig_visc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {DENSITY0, ENERGY0, XVEL0, YVEL0}), (T *)c.base(PRESSURE),
+  kt_ig_visc_dt<T><<<grid, dim3(64, 4), smem, c.stream>>>(maps_of<B::BH>(c, {DENSITY0, ENERGY0, XVEL0, YVEL0}),
+                                                          write_p ? (T *)c.base(PRESSURE) : nullptr,
                                                           write_ss ? (T *)c.base(SOUNDSPEED) : nullptr, (T *)c.base(VISCOSITY), mesh<T>(c), (int)c.off, k,
                                                           gm1<T>(c), ig_fold, fold, tx, nt, c.d_dt_bits, c.d_err);
   return launched(c);
@@ -369,7 +370,7 @@ template <typename T> cudaError_t Ops<T>::ig_visc_dt(Chunk &c, const DtConsts &k
 
 template <typename T>
 cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int acc_fold, int pdv_fold, int flux_fold, bool keep_ring,
-                             const int *store_ps) {
+                             const int *store_ps, bool p_from_de) {
   if (p_fold <= 0 || acc_fold <= 0 || pdv_fold <= 0 || flux_fold <= 0) return cudaErrorInvalidValue;
   if (keep_ring) {
     RingPair rp{{c.base(PRESSURE), nullptr}, {p_out, nullptr}};
@@ -377,16 +378,23 @@ cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int a
     if (e != cudaSuccess) return e;
   }
   constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 12;
-  using L = LagLayout<T, TY>;
-  cudaError_t e = allow_smem(kt_lagrange<T, TY>, L::SMEM);
-  if (e != cudaSuccess) return e;
   // the nodes and faces reach one column and one row past the cells
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
   const LagOut<T> out{(T *)p_out, (T *)c.base(SOUNDSPEED), (T *)c.base(XVEL1), (T *)c.base(YVEL1), (T *)c.base(DENSITY1),
                       (T *)c.base(ENERGY1), (T *)c.base(VOL_FLUX_X), (T *)c.base(VOL_FLUX_Y), store_ps};
-  kt_lagrange<T, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, PRESSURE, VISCOSITY}), out,
-                                                            mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, gm1<T>(c),
-                                                            LagFolds{p_fold, acc_fold, pdv_fold, flux_fold}, c.d_err);
+  const LagFolds fd{p_fold, acc_fold, pdv_fold, flux_fold};
+  cudaError_t e;
+  if (p_from_de) { // the pressure formed from density0 and energy0 (they must agree: the caller's step has run ideal_gas on them)
+    using L = LagLayout<T, TY, true>;
+    if ((e = allow_smem(kt_lagrange<T, TY, true>, L::SMEM)) != cudaSuccess) return e;
+    kt_lagrange<T, TY, true><<<g, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, VISCOSITY}), out,
+                                                                    mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, gm1<T>(c), fd, c.d_err);
+  } else {
+    using L = LagLayout<T, TY>;
+    if ((e = allow_smem(kt_lagrange<T, TY>, L::SMEM)) != cudaSuccess) return e;
+    kt_lagrange<T, TY><<<g, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, PRESSURE, VISCOSITY}),
+                                                              out, mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, gm1<T>(c), fd, c.d_err);
+  }
   return launched(c);
 }
 

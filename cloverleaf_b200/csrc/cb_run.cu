@@ -171,9 +171,10 @@ template <typename T> struct Seq {
   bool fuse = false;
   // fused: the run's last-step flag on the device; the Lagrangian pass
   // stores the predicted pressure and soundspeed in that step only, the
-  // fused x sweep the mass flux of the tiles the edge strip does not read,
-  // and the fused ideal_gas pass no soundspeed (all rewritten unread
-  // otherwise)
+  // fused x sweep the mass flux of the tiles the edge strip does not read
+  // (all rewritten unread otherwise); the fused ideal_gas pass stores
+  // neither pressure nor soundspeed: the Lagrangian pass forms the pressure
+  // from density0 and energy0 as the ideal_gas pass would store it
   const int *last_flag = nullptr;
 
   Seq(Chunk &ch, bool e, bool f, const DtConsts &k) : c(ch), emit(e), fold(f), dk(k) { std::memcpy(fresh, ch.halo_fresh, sizeof fresh); }
@@ -219,7 +220,7 @@ template <typename T> struct Seq {
     // passes between them are none: density0 / energy0 and q are fresh),
     // the pressure written to its second buffer (see lagrange)
     if (fuse) swap_pressure();
-    if (emit) run(fuse ? Ops<T>::ig_visc_dt(c, dk, fi, fv, last_flag == nullptr) : Ops<T>::calc_dt(c, dk));
+    if (emit) run(fuse ? Ops<T>::ig_visc_dt(c, dk, fi, fv, last_flag == nullptr, last_flag == nullptr) : Ops<T>::calc_dt(c, dk));
     ++pos;
   }
   // Fused, the predicted pressure goes to the other of two buffers: the pass
@@ -234,7 +235,7 @@ template <typename T> struct Seq {
     const int ff = eff(dep(2));
     if (fuse) {
       // fused: the whole Lagrangian step in one pass
-      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), 0.0, fp, fa, fc, ff, false, last_flag));
+      if (emit) run(Ops<T>::lagrange(c, c.spare_base(4), 0.0, fp, fa, fc, ff, false, last_flag, last_flag != nullptr));
       swap_pressure();
     } else if (emit) {
       run(Ops<T>::pdv(c, 1, 0.0, 1, fp));

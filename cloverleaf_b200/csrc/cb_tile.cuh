@@ -502,9 +502,13 @@ __device__ __forceinline__ bool ig_visc_dt_tile(TileCtx &cx, T *sm, const MapSet
       // src/serial/ideal_gas.cpp:28-48 for the cell; pressure alone for its neighbours
       T p, ss;
       eos_value(D[b], E[b], gm1, p, ss);
-      p_out[g] = p;
-      if (c_out) c_out[g] = ss; // null in the resident loop: the step's Lagrangian pass rewrites it unread
-      if (ig_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), ig_fold, i, j, p);
+      // null in the resident loop: the step's Lagrangian pass rewrites the sound
+      // speed unread and forms the pressure from density0 and energy0 itself
+      if (p_out) {
+        p_out[g] = p;
+        if (ig_fold && near) fold_halo(p_out, m, halo_rule(PRESSURE), ig_fold, i, j, p);
+      }
+      if (c_out) c_out[g] = ss;
       const T dd = D[b];
       const T pl = gm1 * D[b - 1] * E[b - 1];
       const T pr = gm1 * D[b + 1] * E[b + 1];
@@ -807,13 +811,17 @@ __global__ void __launch_bounds__(256) kt_accelerate(const __grid_constant__ Map
 // swaps the two.
 // Staged: 0 xvel0, 1 yvel0, 2 density0, 3 energy0, 4 pressure, 5 viscosity,
 // rows y0 - 1 .. y0 + TY + 2.
-template <typename T, int TY> struct LagLayout {
+// PDE: the level-0 pressure formed from density0 and energy0 where it is read
+// (eos_value's product, the same bits as the ideal_gas pass stores) instead
+// of staged: five boxes.
+template <typename T, int TY, bool PDE = false> struct LagLayout {
+  static constexpr int NBOX = PDE ? 5 : 6;
   static constexpr int BH = TY + 4;
   static constexpr int BOXS = (BOX_X * BH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
   static constexpr int PCX = TILE_X + 2, PCY = TY + 2; // predicted pressure: cells x0 - 1 + p, y0 - 1 + l
   static constexpr int NNX = TILE_X + 1, NNY = TY + 1; // level-1 velocities: nodes x0 + p, y0 + l
   // + celldx of the box's columns and celldy of its rows (fill_widths)
-  static constexpr size_t SMEM = (size_t)(6 * BOXS + PCX * PCY + 2 * NNX * NNY + BOX_X + BH) * sizeof(T);
+  static constexpr size_t SMEM = (size_t)(NBOX * BOXS + PCX * PCY + 2 * NNX * NNY + BOX_X + BH) * sizeof(T);
   __device__ static constexpr int at(int i, int j, int x0, int y0) { return (j - y0 + 1) * BOX_X + (i - x0 + HALO); }
 };
 
@@ -857,14 +865,15 @@ struct LagFolds {
 // The tile (bx, by) with the block's staging context and shared memory
 // (L::SMEM bytes at sm); staged fields ms 0..5 as above.  Returns false when
 // the staging wait gave up.
-template <typename T, int TY, bool EDGE>
+template <typename T, int TY, bool EDGE, bool PDE = false>
 __device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &ms, const LagOut<T> &out, const Mesh<T> &m, int off, T dt,
                                               T gm1, const LagFolds &fd, int bx, int by) {
-  using L = LagLayout<T, TY>;
+  using L = LagLayout<T, TY, PDE>;
   const int x0 = 2 + bx * TILE_X, y0 = 2 + by * TY;
-  const T *U0 = sm, *V0 = sm + L::BOXS, *D0 = sm + 2 * L::BOXS, *E0 = sm + 3 * L::BOXS, *P = sm + 4 * L::BOXS, *Q = sm + 5 * L::BOXS;
-  T *sp = sm + 6 * L::BOXS, *su = sp + L::PCX * L::PCY, *sv = su + L::NNX * L::NNY, *gx = sv + L::NNX * L::NNY, *gy = gx + BOX_X;
-  stage_issue(cx, sm, ms, 6, L::BOXS, L::BH, off + x0 - HALO, y0 - 1);
+  const T *U0 = sm, *V0 = sm + L::BOXS, *D0 = sm + 2 * L::BOXS, *E0 = sm + 3 * L::BOXS, *P = sm + 4 * L::BOXS;
+  const T *Q = sm + (L::NBOX - 1) * L::BOXS;
+  T *sp = sm + L::NBOX * L::BOXS, *su = sp + L::PCX * L::PCY, *sv = su + L::NNX * L::NNY, *gx = sv + L::NNX * L::NNY, *gy = gx + BOX_X;
+  stage_issue(cx, sm, ms, L::NBOX, L::BOXS, L::BH, off + x0 - HALO, y0 - 1);
   fill_widths(m, x0, y0, 1, L::BH, 1, gx, gy, nullptr, nullptr); // gx[i - x0 + HALO] = celldx[i], gy[j - y0 + 1] = celldy[j]
   if (!stage_wait(cx)) return false;
   const int pitch = (int)m.pitch;
@@ -880,7 +889,7 @@ __device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &
     const T z = T(0);
     T d1, e1;
     pdv_value(true, dt, cdy, cdx, vol, U0[b], U0[b + BOX_X], U0[b + 1], U0[b + BOX_X + 1], V0[b], V0[b + 1], V0[b + BOX_X], V0[b + BOX_X + 1],
-              z, z, z, z, z, z, z, z, D0[b], E0[b], P[b], Q[b], d1, e1);
+              z, z, z, z, z, z, z, z, D0[b], E0[b], PDE ? gm1 * D0[b] * E0[b] : P[b], Q[b], d1, e1);
     sp[l * L::PCX + p] = gm1 * d1 * e1; // eos_value's pressure
     if (store_ps && p >= 1 && p <= TILE_X && l >= 1 && l <= TY && (!EDGE || (i == ic && j == jc))) { // one of the tile's own interior cells
       T pp, cc;
@@ -961,7 +970,7 @@ __device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &
 
 // Registers capped for four blocks per SM in FP64 and five in FP32 (the
 // shared memory's limits).
-template <typename T, int TY>
+template <typename T, int TY, bool PDE = false>
 __global__ void __launch_bounds__(256, sizeof(T) == sizeof(double) ? 4 : 5)
     kt_lagrange(const __grid_constant__ Maps maps, LagOut<T> out, Mesh<T> m, int off, T dt, const double *dtp, T gm1, LagFolds fd, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -969,10 +978,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == sizeof(double) ? 4 : 5)
   T *sm = reinterpret_cast<T *>(smraw);
   TileCtx cx = tile_ctx(&bar, err);
   const T d = dtp ? (T)*dtp : dt;
+  constexpr int NB = LagLayout<T, TY, PDE>::NBOX;
   if (edge_tile(m.nx, m.ny, 2 + blockIdx.x * TILE_X, 2 + blockIdx.y * TY, TY))
-    lagrange_tile<T, TY, true>(cx, sm, map_set(maps, 6), out, m, off, d, gm1, fd, blockIdx.x, blockIdx.y);
+    lagrange_tile<T, TY, true, PDE>(cx, sm, map_set(maps, NB), out, m, off, d, gm1, fd, blockIdx.x, blockIdx.y);
   else
-    lagrange_tile<T, TY, false>(cx, sm, map_set(maps, 6), out, m, off, d, gm1, fd, blockIdx.x, blockIdx.y);
+    lagrange_tile<T, TY, false, PDE>(cx, sm, map_set(maps, NB), out, m, off, d, gm1, fd, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
