@@ -111,7 +111,8 @@ extern "C" int cb_field_summary_noalloc(int nx, int ny, long long pitch, const d
   m.celldx_t = celldx;
   m.celldy_t = celldy;
   const int nt = (int)(tiles_x * tiles_y);
-  k_field_summary<double><<<nt, dim3(NOALLOC_TILE_X, NOALLOC_TILE_Y), 0, s>>>(F, m, gamma - 1.0, partials, counter, sums, (int)tiles_x, nt);
+  k_field_summary<double><<<nt, dim3(NOALLOC_TILE_X, NOALLOC_TILE_Y), 0, s>>>(F, m, gamma - 1.0, partials, counter, sums, (int)tiles_x, nt,
+                                                                          nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_last_error(CB_ECUDA, std::string("cb_field_summary_noalloc: launch: ") + cudaGetErrorString(e));
   return CB_OK;

@@ -60,7 +60,7 @@ template <typename T> struct Ops {
   // one strip of driver/update_tile_halo.cpp: dst's halo on `side` (CB_FACE_*) from the
   // interior of src, the neighbouring tile on that side; enqueued on dst's stream
   static cudaError_t tile_halo(Chunk &dst, const Chunk &src, int side, const HaloJob &job, int depth);
-  static cudaError_t field_summary(Chunk &c);
+  static cudaError_t field_summary(Chunk &c, const int *store_ps = nullptr);
   // fused passes of the resident loop: ideal_gas + viscosity + calc_dt, and the Lagrangian step
   static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold, bool write_ss = true, bool write_p = true);
   // the PdV predictor, accelerate, the PdV corrector and flux_calc in one

@@ -398,12 +398,12 @@ cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int a
   return launched(c);
 }
 
-template <typename T> cudaError_t Ops<T>::field_summary(Chunk &c) {
+template <typename T> cudaError_t Ops<T>::field_summary(Chunk &c, const int *store_ps) {
   dim3 b(32, 8);
   const int tx = (c.nx + 31) / 32, ty = (c.ny + 7) / 8;
   const int nt = tx * ty;
   k_field_summary<T><<<reduce_grid(c, nt), b, 0, c.stream>>>(fields<T>(c), mesh<T>(c), gm1<T>(c), c.d_partials, c.d_counter, c.d_sums,
-                                                             tx, nt);
+                                                             tx, nt, store_ps);
   return launched(c);
 }
 

@@ -410,13 +410,15 @@ __global__ void k_tile_halo(Fields<T> D, Mesh<T> md, Fields<T> S, Mesh<T> ms, Ha
 // The cell's ideal_gas (pressure and soundspeed written) and its terms of
 // the five sums, added to s.
 template <typename T>
-__device__ __forceinline__ void summary_cell(const Fields<T> &F, const Mesh<T> &m, T gm1, int i, int j, double s[5]) {
+__device__ __forceinline__ void summary_cell(const Fields<T> &F, const Mesh<T> &m, T gm1, int i, int j, double s[5], bool store_ps = true) {
   const long long id = m.at(i, j);
   const T d0 = F.f[DENSITY0][id], e0 = F.f[ENERGY0][id];
   T p, c;
   eos(d0, e0, gm1, p, c);
-  F.f[PRESSURE][id] = p;
-  F.f[SOUNDSPEED][id] = c;
+  if (store_ps) { // ideal_gas's stores (the resident loop keeps them for its last step only)
+    F.f[PRESSURE][id] = p;
+    F.f[SOUNDSPEED][id] = c;
+  }
   const T *u = F.f[XVEL0], *v = F.f[YVEL0];
   double vsqrd = 0.0;
   for (int kv = j; kv <= j + 1; ++kv)
@@ -435,13 +437,14 @@ __device__ __forceinline__ void summary_cell(const Fields<T> &F, const Mesh<T> &
 
 template <typename T>
 __global__ void k_field_summary(Fields<T> F, Mesh<T> m, T gm1, double *partials, unsigned int *counter, double *out,
-                                int tiles_x, int ntiles) {
+                                int tiles_x, int ntiles, const int *store_ps) {
   double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const bool st = !store_ps || *store_ps != 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int i = 2 + (t % tiles_x) * blockDim.x + threadIdx.x;
     const int j = 2 + (t / tiles_x) * blockDim.y + threadIdx.y;
     if (i >= m.nx + 2 || j >= m.ny + 2) continue;
-    summary_cell(F, m, gm1, i, j, s);
+    summary_cell(F, m, gm1, i, j, s, st);
   }
   // block reduction (fixed tree order)
   __shared__ double red[5][256];

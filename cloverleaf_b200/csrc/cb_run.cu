@@ -316,7 +316,7 @@ template <typename T> struct Seq {
   }
   // cb_field_summary
   void summary() {
-    if (emit) run(Ops<T>::field_summary(c));
+    if (emit) run(Ops<T>::field_summary(c, last_flag)); // its pressure and soundspeed are read by no later phase
     fresh[P] = 0;
     fresh[SS] = 0;
     ++pos;
