@@ -745,7 +745,9 @@ int cb_calc_dt(cb_chunk *c, const cb_dt_params *p, double *dt_min_val, int *cont
     CB_CUDA(cudaGetLastError());
     const int f1 = effective_fold(c, 1), f2 = effective_fold(c, 2);
     c->dt_dev = c->d_dt_ahead;
-    const cudaError_t le = dispatch(c, [&](auto ops) { return ops.lagrange(*c, c->spare_base(4), 0.0, f1, f2, f2, f2, true); });
+    // the pressure the fused pass just stored is eos_value's product of density0 and energy0,
+    // so the Lagrangian pass forms it from them instead of staging it (the same bits)
+    const cudaError_t le = dispatch(c, [&](auto ops) { return ops.lagrange(*c, c->spare_base(4), 0.0, f1, f2, f2, f2, true, nullptr, true); });
     c->dt_dev = nullptr;
     CB_CUDA(le);
     CB_CUDA(cudaEventSynchronize(c->ev_dt));
