@@ -794,11 +794,11 @@ def main():
     e2e = {"value": replicas_value(S * S, args.steps, world, ms_e2e), "unit": UNIT,
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
 
-    # roofline of the headline graph's dominant kernel, kt_lagrange (the fused
-    # Lagrangian pass): the graph's fused passes in a host loop (call fusion),
-    # a CUDA event pair around each group of calls on the chunk's stream; the
-    # flux_calc group is the Lagrangian pass (with the pressure's outer-ring
-    # copy, a few microseconds)
+    # roofline of kt_lagrange (the fused Lagrangian pass; the largest share of
+    # the step's launch list), with the advection passes beside it: the fused
+    # passes in a host loop (call fusion), a CUDA event pair around each group
+    # of calls on the chunk's stream; the flux_calc group is the Lagrangian
+    # pass (with the pressure's outer-ring copy, a few microseconds)
     lag_steps = min(args.steps, 20)
     msf, _, cf, phf, _ = run_form(FP64, S, args.warmup, lag_steps, with_phases=True, rank=rank, world=world, fuse_calls=True,
                                   tag_sweeps=True)
