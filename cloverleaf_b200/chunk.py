@@ -29,7 +29,7 @@ FACE_LEFT, FACE_RIGHT, FACE_BOTTOM, FACE_TOP = 1, 2, 4, 8
 
 # Every symbol include/cloverb200.h declares.
 EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "cb_create", "cb_destroy", "cb_set_gamma", "cb_set_option", "cb_get_extent",
-           "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk",
+           "cb_read_field", "cb_write_field", "cb_read_geom", "cb_write_geom", "cb_build_field", "cb_initialise_chunk", "cb_initialise_chunk_in",
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_set_dt_ahead", "cb_dt_ahead_stats", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_lagrangian", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
            "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_run", "cb_field_summary_noalloc",
@@ -94,6 +94,7 @@ def library() -> ctypes.CDLL:
         "cb_read_field": ([P, i, dp, sz, i], i), "cb_write_field": ([P, i, dp, sz, i], i),
         "cb_read_geom": ([P, i, dp, sz], i), "cb_write_geom": ([P, i, dp, sz], i),
         "cb_build_field": ([P], i), "cb_initialise_chunk": ([P, d, d, d, d], i),
+        "cb_initialise_chunk_in": ([P, d, d, d, d, i, i, i, i], i),
         "cb_generate_chunk": ([P, i, ctypes.POINTER(State)], i),
         "cb_ideal_gas": ([P, i, i], i), "cb_viscosity": ([P, i], i),
         "cb_calc_dt": ([P, ctypes.POINTER(DtParams), dp, ip, ip, ip, ip], i),
@@ -218,6 +219,10 @@ class Chunk:
     # ---- setup (driver/build_field.h, initialise_chunk.h, generate_chunk.h)
     def build_field(self): _check(self._L.cb_build_field(self._h))
     def initialise_chunk(self, xmin, ymin, xmax, ymax): _check(self._L.cb_initialise_chunk(self._h, xmin, ymin, xmax, ymax))
+
+    def initialise_chunk_in(self, xmin, ymin, xmax, ymax, x_cells: int, y_cells: int, left: int, bottom: int):
+        """The geometry of this chunk as cell (left, bottom) onward of an x_cells x y_cells grid."""
+        _check(self._L.cb_initialise_chunk_in(self._h, xmin, ymin, xmax, ymax, x_cells, y_cells, left, bottom))
 
     def generate_chunk(self, states: Sequence):
         arr = (State * len(states))()

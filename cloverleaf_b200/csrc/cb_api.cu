@@ -295,15 +295,18 @@ bool encode_buffer_maps(void *const *bufs, int nbuf, long long pitch, int ny, in
   return true;
 }
 
-// The 1-D geometry of src/serial/initialise_chunk.cpp:30-85 for a single
-// tile (t_left = t_bottom = 1), into g[NUM_GEOM] arrays of at least
-// max(nx, ny) + 5 entries.
-void chunk_geometry(int nx, int ny, double gxmin, double gymin, double gxmax, double gymax, double *const *g) {
+// The 1-D geometry of src/serial/initialise_chunk.cpp:30-85, into
+// g[NUM_GEOM] arrays of at least max(nx, ny) + 5 entries, for a chunk of
+// nx x ny cells whose first cell is cell (left, bottom) of a grid of
+// x_cells x y_cells over [gxmin, gxmax] x [gymin, gymax] (1-based global
+// indices; the chunk's own indices start at 1, as the reference's tile's).
+void chunk_geometry_at(int nx, int ny, double gxmin, double gymin, double gxmax, double gymax, int x_cells, int y_cells, int left, int bottom,
+                       double *const *g) {
   const int x_min = 1, y_min = 1, x_max = nx, y_max = ny;
-  double dx = (gxmax - gxmin) / (double)(nx);
-  double dy = (gymax - gymin) / (double)(ny);
-  double xmin = gxmin + dx * (double)(1 - 1);
-  double ymin = gymin + dy * (double)(1 - 1);
+  double dx = (gxmax - gxmin) / (double)(x_cells);
+  double dy = (gymax - gymin) / (double)(y_cells);
+  double xmin = gxmin + dx * (double)(left - 1);
+  double ymin = gymin + dy * (double)(bottom - 1);
   const int xrange = (x_max + 3) - (x_min - 2) + 1, yrange = (y_max + 3) - (y_min - 2) + 1;
   for (int j = 0; j < xrange; j++) {
     g[VERTEXX][j] = xmin + dx * (j - 1 - x_min);
@@ -322,6 +325,10 @@ void chunk_geometry(int nx, int ny, double gxmin, double gymin, double gxmax, do
     g[CELLY][k] = 0.5 * (g[VERTEXY][k] + g[VERTEXY][k + 1]);
     g[CELLDY][k] = dy;
   }
+}
+
+void chunk_geometry(int nx, int ny, double gxmin, double gymin, double gxmax, double gymax, double *const *g) {
+  chunk_geometry_at(nx, ny, gxmin, gymin, gxmax, gymax, nx, ny, 1, 1, g);
 }
 
 } // namespace cb
@@ -648,6 +655,17 @@ int cb_initialise_chunk(cb_chunk *c, double gxmin, double gymin, double gxmax, d
   CB_CHECK_CHUNK(c);
   if (!(gxmax > gxmin) || !(gymax > gymin)) return fail(CB_EINVAL, "cb_initialise_chunk: empty domain");
   chunk_geometry(c->nx, c->ny, gxmin, gymin, gxmax, gymax, c->geom_h);
+  CB_CUDA(upload_geom(c));
+  return CB_OK;
+}
+
+int cb_initialise_chunk_in(cb_chunk *c, double gxmin, double gymin, double gxmax, double gymax, int x_cells, int y_cells, int left,
+                           int bottom) {
+  CB_CHECK_CHUNK(c);
+  if (!(gxmax > gxmin) || !(gymax > gymin)) return fail(CB_EINVAL, "cb_initialise_chunk_in: empty domain");
+  if (x_cells < 1 || y_cells < 1 || left < 1 || bottom < 1 || left - 1 + c->nx > x_cells || bottom - 1 + c->ny > y_cells)
+    return fail(CB_EINVAL, "cb_initialise_chunk_in: the chunk does not lie inside the grid");
+  chunk_geometry_at(c->nx, c->ny, gxmin, gymin, gxmax, gymax, x_cells, y_cells, left, bottom, c->geom_h);
   CB_CUDA(upload_geom(c));
   return CB_OK;
 }

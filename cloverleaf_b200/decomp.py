@@ -16,6 +16,16 @@ reductions of the step, over torch.distributed (NCCL on GPUs, gloo on CPUs).
   arrays that extend one past the cells across the face).
 * dt_min() / summary_sum(): calc_dt's minimum over chunks (one all_reduce
   MIN of a double) and field_summary's five sums (one all_reduce SUM).
+* DecomposedChunk: one rank's chunk on its GPU with the calls a HydroRun
+  makes, so that HydroRun(DecomposedChunk(...), deck, fold=False) is the
+  reference driver's decomposed run: geometry as the reference forms a
+  chunk's (cb_initialise_chunk_in), the reflective fill on the physical faces
+  only (cb_set_external_faces), every update_halo an exchange of the internal
+  faces followed by that fill (driver/update_halo.cpp), the PdV predictor's
+  pressure halo likewise, calc_dt's minimum and the summary reduced over the
+  ranks.  The strips go through host memory (each exchanged field is read
+  back and written whole): a correctness path for small meshes, not a
+  performance one.
 
 Fields are 2-D arrays in the reference's index convention (x fastest, a
 2-deep halo: cells (ny+4, nx+4), nodes (ny+5, nx+5), x faces (ny+4, nx+5),
@@ -163,3 +173,50 @@ def summary_sum(local: Iterable[float], group=None) -> List[float]:
     t = torch.tensor([float(x) for x in local], dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return [float(x) for x in t.tolist()]
+
+
+class DecomposedChunk:
+    """One rank's chunk of a decomposed run (see the module docstring); the
+    other chunk calls go to the chunk as they are."""
+
+    def __init__(self, info: ChunkInfo, deck, precision: int = 0, device: int = 0, group=None):
+        from .chunk import FACE_BOTTOM, FACE_LEFT, FACE_RIGHT, FACE_TOP, Chunk
+        self.info, self.deck, self.group = info, deck, group
+        self.c = Chunk(info.nx, info.ny, precision=precision, gamma=deck.gamma, device=device)
+        faces = 0
+        for side, bit in ((LEFT, FACE_LEFT), (RIGHT, FACE_RIGHT), (BOTTOM, FACE_BOTTOM), (TOP, FACE_TOP)):
+            if info.neighbours[side] < 0:
+                faces |= bit
+        self.c.set_external_faces(faces)
+
+    def __getattr__(self, name):
+        return getattr(self.c, name)
+
+    def initialise_chunk(self, xmin, ymin, xmax, ymax):
+        d, i = self.deck, self.info
+        self.c.initialise_chunk_in(xmin, ymin, xmax, ymax, d.x_cells, d.y_cells, i.left, i.bottom)
+
+    def update_halo(self, fields, depth: int):
+        fids = sorted(set(int(f) for f in fields))
+        if any(n >= 0 for n in self.info.neighbours):
+            arrays = {f: self.c.read(f) for f in fids}
+            exchange(self.info, arrays, fids, depth, self.group)
+            for f in fids:
+                self.c.write(f, arrays[f])
+        self.c.update_halo(fids, depth)
+
+    def pdv(self, predict: bool, dt: float, full: bool = False, halo_depth: int = 0):
+        # the predictor's own pressure halo (src/serial/PdV.cpp:118-124) is an exchange too
+        self.c.pdv(predict, dt, full=full, halo_depth=0)
+        if full and halo_depth > 0:
+            self.update_halo([4], halo_depth)  # pressure
+
+    def calc_dt(self, *args, **kw):
+        dt, control, jldt, kldt, small = self.c.calc_dt(*args, **kw)
+        return dt_min(dt, self.group), control, jldt, kldt, small
+
+    def field_summary(self):
+        return tuple(summary_sum(self.c.field_summary(), self.group))
+
+    def close(self):
+        self.c.close()

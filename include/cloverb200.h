@@ -118,6 +118,12 @@ int cb_write_geom(cb_chunk *c, int geom, const double *host, size_t n);
 /* Setup: driver/build_field.h:24, driver/initialise_chunk.h:24, driver/generate_chunk.h:24. */
 int cb_build_field(cb_chunk *c);
 int cb_initialise_chunk(cb_chunk *c, double xmin, double ymin, double xmax, double ymax);
+/* src/serial/initialise_chunk.cpp:30-85 for one chunk of a decomposed grid:
+ * the chunk's first cell is cell (left, bottom) (1-based) of the x_cells x
+ * y_cells grid over [xmin, xmax] x [ymin, ymax]; dx, dy from the whole grid,
+ * the chunk's origin xmin + dx * (left - 1) as the reference forms it
+ * (driver/comms.cpp:64-156 gives left and bottom). */
+int cb_initialise_chunk_in(cb_chunk *c, double xmin, double ymin, double xmax, double ymax, int x_cells, int y_cells, int left, int bottom);
 int cb_generate_chunk(cb_chunk *c, int nstates, const cb_state *states);
 
 /* Hydro phases. */

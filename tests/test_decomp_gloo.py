@@ -139,3 +139,29 @@ def test_four_chunks_exchange_and_reduce_as_one_mesh():
         assert res[r]["dt"] == res[r]["dt_global"], (r, res[r]["dt"], res[r]["dt_global"])
         for a, b in zip(res[r]["sums"], res[r]["sums_global"]):
             assert abs(a - b) <= 1e-15 * abs(b), (r, a, b)
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("world", [2, 4])
+def test_decomposed_oracle_run_is_the_whole_mesh_run(world):
+    """The benchmark deck (64 x 48) decomposed over two (1 x 2) and four
+    (2 x 2) gloo ranks, each chunk held by the CPU oracle and driven by
+    HydroRun's call sequence (update_halo = exchange of the internal faces,
+    then the reflective fill of the physical ones): the dt of every step and
+    every captured field of each chunk equal, bit for bit, the whole mesh's
+    run; the summaries (sums reduced over the ranks) within 1e-13 of the
+    whole mesh's exactly rounded sums.  (In this deck the flow never crosses
+    a chunk edge against advec_cell's upwind clamp, so the decomposed run is
+    the whole mesh's run.)"""
+    from decomp_util import rank_body
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(rank_body, args=(world, port, out, "bm", False), nprocs=world, join=True)
+        res = dict(out)
+    for r in range(world):
+        assert res[r]["steps"][0] == res[r]["steps"][1], r
+        assert res[r]["dt"], r
+        assert res[r]["summary_steps"], r
+        assert res[r]["bad"] == [], (r, res[r]["bad"])
+        assert max(res[r]["sums"]) <= 1e-13, (r, res[r]["sums"])
