@@ -215,6 +215,8 @@ def format_deck(d: Deck) -> str:
         f" end_step={d.end_step}",
         f" summary_frequency={d.summary_frequency}",
     ]
+    if d.visit_frequency:
+        out.append(f" visit_frequency={d.visit_frequency}")
     if d.test_problem:
         out.append(f" test_problem {d.test_problem}")
     out.append("*endclover")

@@ -10,6 +10,9 @@ of decks and stores, per deck:
 and, for the dump deck, the reference's --dump output of driver/shared.cpp:96-189 as
   <name>.dump.sha256   one line per dump file: its name and the sha256 of its
                        text with the work_array blocks removed (dump_filter.py)
+and, for the visit deck, the files driver/visit.cpp:31-192 writes as
+  <name>.visit.sha256  one line per file (clover.visit and each .vtk): its name
+                       and the sha256 of its bytes
 
 Usage: python tests/golden/make_golden.py   (needs oracle/_ref/serial-capture and oracle/_ref/serial)
 """
@@ -89,8 +92,38 @@ def write_dump_fixture():
     print(name, len(files), "dump files")
 
 
+def visit_deck():
+    """The dump deck with visit output every second step (driver/hydro.cpp:95-96,
+    :112; driver/start.cpp:131): files at steps 0, 2 and 3."""
+    c = D.benchmark_deck(16, 3, ny=12)
+    c.states.append(D.State(density=2.0, energy=3.0, xvel=0.5, yvel=-0.25, geometry=D.GEOM_CIRC, xmin=6.0, ymin=6.0,
+                            radius=2.5, defined=True))
+    c.visit_frequency = 2
+    return "circ16x12x3v", D.format_deck(c)
+
+
+def write_visit_fixture():
+    name, text = visit_deck()
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "clover.in"), "w") as f:
+            f.write(text)
+        p = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "serial"), "--file", "clover.in"], cwd=tmp,
+                           capture_output=True, text=True, timeout=600)
+        if p.returncode != 0:
+            raise SystemExit(f"{name}: reference exited {p.returncode}")
+        files = sorted(fn for fn in os.listdir(tmp) if fn.endswith((".vtk", ".visit")))
+        with open(os.path.join(HERE, name + ".in"), "w") as f:
+            f.write(text)
+        with open(os.path.join(HERE, name + ".visit.sha256"), "w") as f:
+            for fn in files:
+                body = open(os.path.join(tmp, fn), "rb").read()
+                f.write(f"{fn} {hashlib.sha256(body).hexdigest()}\n")
+    print(name, len(files), "visit files")
+
+
 def main():
     write_dump_fixture()
+    write_visit_fixture()
     for name, (text, keep_fields) in decks().items():
         res = oracle.run_reference(text)
         if res["returncode"] != 0:

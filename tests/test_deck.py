@@ -35,9 +35,11 @@ def test_space_separated_values_and_unknown_keywords():
 
 
 def test_format_round_trip():
-    for name in SMALL_DECKS:
+    for name in SMALL_DECKS + ["circ16x12x3v"]:
         raw = D.parse_deck(deck_text(name), nudge=False)
         again = D.parse_deck(D.format_deck(raw), nudge=False)
         for a, b in zip(raw.states, again.states):
             assert a == b
-        assert (raw.x_cells, raw.y_cells, raw.end_step) == (again.x_cells, again.y_cells, again.end_step)
+        assert (raw.x_cells, raw.y_cells, raw.end_step, raw.visit_frequency) == \
+            (again.x_cells, again.y_cells, again.end_step, again.visit_frequency)
+    assert D.parse_deck(deck_text("circ16x12x3v")).visit_frequency == 2

@@ -125,3 +125,29 @@ def test_driver_dump_matches_reference():
             if name.startswith("work_array"):
                 continue
             assert np.array_equal(a0[name][2:-2, 2:-2], a1[name][2:-2, 2:-2]), (fn, name)
+
+
+def run_driver_visit(text, env_extra):
+    assert os.path.exists(EXE), "driver binary not built (make -C cloverleaf_b200/model)"
+    with tempfile.TemporaryDirectory() as tmp:
+        open(os.path.join(tmp, "clover.in"), "w").write(text)
+        env = dict(os.environ, **env_extra)
+        p = subprocess.run([EXE, "--file", "clover.in"], cwd=tmp, env=env, capture_output=True, text=True, timeout=600)
+        files = {fn: open(os.path.join(tmp, fn), "rb").read() for fn in os.listdir(tmp) if fn.endswith((".vtk", ".visit"))}
+    return p, files
+
+
+@pytest.mark.parametrize("env", [{"CLOVER_B200_FOLD": "0"}, {}], ids=["unfolded", "defaults"])
+def test_driver_visit_matches_reference(env):
+    """visit output (driver/visit.cpp:31-192, every second step and at the
+    end: ideal_gas, the pressure and velocity halos and viscosity run, then
+    the vertex coordinates, density, energy, pressure, viscosity and both
+    velocities are read through mirrored() and printed): clover.visit and
+    the three .vtk files equal the reference serial build's byte for byte,
+    with every update_halo run as called and with folding and call fusion on."""
+    gold = dict(line.split() for line in open(os.path.join(GOLDEN, "circ16x12x3v.visit.sha256")))
+    p, files = run_driver_visit(deck_text("circ16x12x3v"), env)
+    assert p.returncode == 0, p.stdout[-2000:]
+    assert sorted(files) == sorted(gold)
+    for fn, body in files.items():
+        assert hashlib.sha256(body).hexdigest() == gold[fn], fn
