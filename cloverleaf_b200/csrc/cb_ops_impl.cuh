@@ -377,7 +377,11 @@ cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int a
     cudaError_t e = copy_ring<T>(c, rp, 1, 1, c.nx + 2, 1, c.ny + 2, c.nx + 4, c.ny + 4);
     if (e != cudaSuccess) return e;
   }
-  constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 12;
+  // Tile rows: the pressure formed from density0 and energy0 (five staged
+  // boxes) leaves room for 12 rows at three blocks per SM in FP64 (4.90 ->
+  // 4.89 ms a fused step at 7680^2; 16 rows at two blocks: 5.07); with the
+  // pressure staged, 8 rows (four blocks per SM).  FP32: 12 rows both ways.
+  constexpr int TY = sizeof(T) == sizeof(double) ? 8 : 12, TYP = 12;
   // the nodes and faces reach one column and one row past the cells
   dim3 g((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TY - 1) / TY);
   const LagOut<T> out{(T *)p_out, (T *)c.base(SOUNDSPEED), (T *)c.base(XVEL1), (T *)c.base(YVEL1), (T *)c.base(DENSITY1),
@@ -385,10 +389,11 @@ cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int a
   const LagFolds fd{p_fold, acc_fold, pdv_fold, flux_fold};
   cudaError_t e;
   if (p_from_de) { // the pressure formed from density0 and energy0 (they must agree: the caller's step has run ideal_gas on them)
-    using L = LagLayout<T, TY, true>;
-    if ((e = allow_smem(kt_lagrange<T, TY, true>, L::SMEM)) != cudaSuccess) return e;
-    kt_lagrange<T, TY, true><<<g, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, VISCOSITY}), out,
-                                                                    mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, gm1<T>(c), fd, c.d_err);
+    using L = LagLayout<T, TYP, true>;
+    const dim3 gp((c.nx + 1 + TILE_X - 1) / TILE_X, (c.ny + 1 + TYP - 1) / TYP);
+    if ((e = allow_smem(kt_lagrange<T, TYP, true>, L::SMEM)) != cudaSuccess) return e;
+    kt_lagrange<T, TYP, true><<<gp, dim3(64, 4), L::SMEM, c.stream>>>(maps_of<L::BH>(c, {XVEL0, YVEL0, DENSITY0, ENERGY0, VISCOSITY}),
+                                                                      out, mesh<T>(c), (int)c.off, (T)dt, c.dt_dev, gm1<T>(c), fd, c.d_err);
   } else {
     using L = LagLayout<T, TY>;
     if ((e = allow_smem(kt_lagrange<T, TY>, L::SMEM)) != cudaSuccess) return e;

@@ -968,10 +968,10 @@ __device__ __forceinline__ bool lagrange_tile(TileCtx &cx, T *sm, const MapSet &
   return true;
 }
 
-// Registers capped for four blocks per SM in FP64 and five in FP32 (the
-// shared memory's limits).
+// Registers capped for the blocks per SM the shared memory allows: FP64 four
+// (8 rows) or three (12 rows), FP32 five.
 template <typename T, int TY, bool PDE = false>
-__global__ void __launch_bounds__(256, sizeof(T) == sizeof(double) ? 4 : 5)
+__global__ void __launch_bounds__(256, sizeof(T) == sizeof(double) ? (TY == 8 ? 4 : 3) : 5)
     kt_lagrange(const __grid_constant__ Maps maps, LagOut<T> out, Mesh<T> m, int off, T dt, const double *dtp, T gm1, LagFolds fd, int *err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ uint64_t bar;
