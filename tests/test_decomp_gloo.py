@@ -144,15 +144,16 @@ def test_four_chunks_exchange_and_reduce_as_one_mesh():
 @pytest.mark.timeout(300)
 @pytest.mark.parametrize("world", [2, 4])
 def test_decomposed_oracle_run_is_the_whole_mesh_run(world):
-    """The benchmark deck (64 x 48) decomposed over two (1 x 2) and four
+    """The benchmark deck (64 x 48) decomposed over two (2 x 1) and four
     (2 x 2) gloo ranks, each chunk held by the CPU oracle and driven by
     HydroRun's call sequence (update_halo = exchange of the internal faces,
     then the reflective fill of the physical ones): the dt of every step and
     every captured field of each chunk equal, bit for bit, the whole mesh's
     run; the summaries (sums reduced over the ranks) within 1e-13 of the
-    whole mesh's exactly rounded sums.  (In this deck the flow never crosses
-    a chunk edge against advec_cell's upwind clamp, so the decomposed run is
-    the whole mesh's run.)"""
+    whole mesh's exactly rounded sums.  (In this deck, split at column 32
+    and row 24, the flow never crosses a chunk edge against advec_cell's
+    upwind clamp, so the decomposed run is the whole mesh's run; split 3 x 1,
+    at columns 22 and 43, it does, and the runs part.)"""
     from decomp_util import rank_body
     port = _free_port()
     with mp.Manager() as mgr:

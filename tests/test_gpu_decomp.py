@@ -11,8 +11,8 @@ sums within 1e-13.
 Decks: the benchmark deck (64 x 48) and a deck whose flow crosses the
 chunk edges both ways (a moving circle, gamma 1.55; 56 x 40), so that
 each chunk's own upwind clamp at its right / top edge face
-(src/serial/advec_cell.cpp:77, :169) is exercised; over two (1 x 2) and
-four (2 x 2) ranks.  The ranks' kernels never wait on one another: the
+(src/serial/advec_cell.cpp:77, :169) is exercised; over two (2 x 1), three (3 x 1, ragged
+columns), four (2 x 2) and six (2 x 3, ragged rows in the circle deck) ranks.  The ranks' kernels never wait on one another: the
 exchange is a host-side gloo step between the calls.
 """
 import os
@@ -36,7 +36,7 @@ def _free_port():
 
 
 @pytest.mark.timeout(600)
-@pytest.mark.parametrize("world", [2, 4])
+@pytest.mark.parametrize("world", [2, 3, 4, 6])
 @pytest.mark.parametrize("deck_name", ["bm", "circle"])
 def test_decomposed_gpu_run_is_the_decomposed_oracle_run(deck_name, world):
     from decomp_util import rank_body
