@@ -33,7 +33,7 @@ EXPORTS = ["cb_version", "cb_last_error", "cb_device_count", "cb_device_name", "
            "cb_generate_chunk", "cb_ideal_gas", "cb_viscosity", "cb_calc_dt", "cb_set_dt_ahead", "cb_dt_ahead_stats", "cb_pdv", "cb_revert", "cb_accelerate",
            "cb_flux_calc", "cb_lagrangian", "cb_advec_cell", "cb_advec_mom", "cb_reset_field", "cb_update_halo", "cb_field_summary",
            "cb_synchronize", "cb_get_stream", "cb_launch_count", "cb_run", "cb_field_summary_noalloc",
-           "cb_set_external_faces", "cb_copy_tile_halo",
+           "cb_set_external_faces", "cb_copy_tile_halo", "cb_face_strip_size", "cb_pack_face", "cb_unpack_face",
            "cb_batch_create", "cb_batch_destroy", "cb_batch_set_schedule", "cb_batch_get_schedule", "cb_batch_autotune",
            "cb_batch_run", "cb_batch_synchronize", "cb_batch_deck_result", "cb_batch_read_summaries", "cb_batch_read_dt",
            "cb_batch_read_field", "cb_batch_get_stream", "cb_batch_launch_count",
@@ -110,6 +110,8 @@ def library() -> ctypes.CDLL:
         "cb_selftest_width_ratio": ([ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong)], i),
         "cb_selftest_wait_limits": ([d, ip, ip, dp, ip, ip, dp], i),
         "cb_set_external_faces": ([P, i], i), "cb_copy_tile_halo": ([P, P, i, ip, i], i),
+        "cb_face_strip_size": ([P, i, ip, i, ctypes.POINTER(sz)], i),
+        "cb_pack_face": ([P, i, ip, i, P, sz], i), "cb_unpack_face": ([P, i, ip, i, P, sz], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -283,6 +285,21 @@ class Chunk:
     def copy_tile_halo(self, src: "Chunk", side: int, fields: Iterable, depth: int):
         """This chunk's halo on `side` (one FACE_* value) from `src`, the tile on that side."""
         _check(self._L.cb_copy_tile_halo(self._h, src._h, int(side), _field_flags(fields), depth))
+
+    # ---- decomposed runs (driver/comms.cpp:clover_exchange, src/serial/pack_kernel.cpp)
+    def face_strip_size(self, side: int, fields: Iterable, depth: int) -> int:
+        """Elements (of the chunk's precision) of the face strip on `side` (one FACE_* value)."""
+        n = ctypes.c_size_t(0)
+        _check(self._L.cb_face_strip_size(self._h, int(side), _field_flags(fields), depth, ctypes.byref(n)))
+        return int(n.value)
+
+    def pack_face(self, side: int, fields: Iterable, depth: int, dev_ptr: int, capacity: int):
+        """The strip the neighbour on `side` needs, into the device buffer at dev_ptr (on the chunk's stream)."""
+        _check(self._L.cb_pack_face(self._h, int(side), _field_flags(fields), depth, ctypes.c_void_p(dev_ptr), capacity))
+
+    def unpack_face(self, side: int, fields: Iterable, depth: int, dev_ptr: int, capacity: int):
+        """This chunk's halo on `side` from the strip its neighbour there packed (on the chunk's stream)."""
+        _check(self._L.cb_unpack_face(self._h, int(side), _field_flags(fields), depth, ctypes.c_void_p(dev_ptr), capacity))
 
     def field_summary(self) -> Tuple[float, float, float, float, float]:
         out = (ctypes.c_double * 5)()

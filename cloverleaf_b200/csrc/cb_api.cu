@@ -1018,6 +1018,66 @@ int cb_copy_tile_halo(cb_chunk *dst, cb_chunk *src, int side, const int fields[1
   return CB_OK;
 }
 
+namespace {
+
+// The job of one face strip and its length in elements; CB_OK or an error.
+int strip_job(const char *who, cb_chunk *c, int side, const int fields[15], int depth, StripJob &job, size_t &elements) {
+  if (!fields) return fail(CB_EINVAL, std::string(who) + ": null fields");
+  if (side != CB_FACE_LEFT && side != CB_FACE_RIGHT && side != CB_FACE_BOTTOM && side != CB_FACE_TOP)
+    return fail(CB_EINVAL, std::string(who) + ": side must be one CB_FACE_* value");
+  if (int r = check_depth(depth, false)) return r;
+  const bool lr = side == CB_FACE_LEFT || side == CB_FACE_RIGHT;
+  job = StripJob{};
+  long long n = 0;
+  for (int f = 0; f < 15; ++f) {
+    if (fields[f] != 1) continue;
+    // the arrays one longer in x (nodes, x faces) or in y (nodes, y faces): driver/definitions.cpp:4-41
+    const bool node = f == XVEL0 || f == XVEL1 || f == YVEL0 || f == YVEL1;
+    const int xe = node || f == VOL_FLUX_X || f == MASS_FLUX_X, ye = node || f == VOL_FLUX_Y || f == MASS_FLUX_Y;
+    const int along_extra = lr ? ye : xe;
+    job.field[job.nfields] = f;
+    job.off[job.nfields] = n;
+    ++job.nfields;
+    n += (long long)((lr ? c->ny : c->nx) + 2 * depth + along_extra) * depth;
+  }
+  elements = (size_t)n;
+  return CB_OK;
+}
+
+} // namespace
+
+int cb_face_strip_size(cb_chunk *c, int side, const int fields[15], int depth, size_t *elements) {
+  CB_CHECK_CHUNK(c);
+  if (!elements) return fail(CB_EINVAL, "cb_face_strip_size: null elements");
+  StripJob job;
+  return strip_job("cb_face_strip_size", c, side, fields, depth, job, *elements);
+}
+
+int cb_pack_face(cb_chunk *c, int side, const int fields[15], int depth, void *dev_buf, size_t capacity) {
+  CB_CHECK_CHUNK(c);
+  StripJob job;
+  size_t n = 0;
+  if (int r = strip_job("cb_pack_face", c, side, fields, depth, job, n)) return r;
+  if (n > 0 && !dev_buf) return fail(CB_EINVAL, "cb_pack_face: null buffer");
+  if (capacity < n) return fail(CB_EINVAL, "cb_pack_face: buffer of " + std::to_string(capacity) + " elements, strip needs " + std::to_string(n));
+  CB_CUDA(run_pending(c));
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.face_strip(*c, side, job, depth, dev_buf, true); }));
+  return CB_OK;
+}
+
+int cb_unpack_face(cb_chunk *c, int side, const int fields[15], int depth, const void *dev_buf, size_t capacity) {
+  CB_CHECK_CHUNK(c);
+  StripJob job;
+  size_t n = 0;
+  if (int r = strip_job("cb_unpack_face", c, side, fields, depth, job, n)) return r;
+  if (n > 0 && !dev_buf) return fail(CB_EINVAL, "cb_unpack_face: null buffer");
+  if (capacity < n) return fail(CB_EINVAL, "cb_unpack_face: buffer of " + std::to_string(capacity) + " elements, strip needs " + std::to_string(n));
+  CB_CUDA(run_pending(c));
+  CB_CUDA(dispatch(c, [&](auto ops) { return ops.face_strip(*c, side, job, depth, const_cast<void *>(dev_buf), false); }));
+  for (int k = 0; k < job.nfields; ++k) c->halo_fresh[job.field[k]] = 0;
+  return CB_OK;
+}
+
 int cb_field_summary(cb_chunk *c, double out[5]) {
   CB_CHECK_CHUNK(c);
   if (!out) return fail(CB_EINVAL, "cb_field_summary: null out");

@@ -26,6 +26,14 @@ struct HaloJob {
   int field[15];
 };
 
+// The fields of one face strip (cb_pack_face / cb_unpack_face) and where
+// each starts in the strip buffer (elements).
+struct StripJob {
+  int nfields;
+  int field[15];
+  long long off[15];
+};
+
 template <typename T> struct Ops {
   static cudaError_t generate_chunk(Chunk &c, const DevState *d_states, int nstates);
   static cudaError_t ideal_gas(Chunk &c, int predict, int fold);
@@ -60,6 +68,10 @@ template <typename T> struct Ops {
   // one strip of driver/update_tile_halo.cpp: dst's halo on `side` (CB_FACE_*) from the
   // interior of src, the neighbouring tile on that side; enqueued on dst's stream
   static cudaError_t tile_halo(Chunk &dst, const Chunk &src, int side, const HaloJob &job, int depth);
+  // one face strip of driver/comms.cpp:clover_exchange between the chunk and
+  // a linear device buffer: pack = the strip the neighbour on `side` needs,
+  // unpack = the chunk's own halo on `side` from that neighbour's strip
+  static cudaError_t face_strip(Chunk &c, int side, const StripJob &job, int depth, void *buf, bool pack);
   static cudaError_t field_summary(Chunk &c, const int *store_ps = nullptr);
   // fused passes of the resident loop: ideal_gas + viscosity + calc_dt, and the Lagrangian step
   static cudaError_t ig_visc_dt(Chunk &c, const DtConsts &k, int ig_fold, int fold, bool write_ss = true, bool write_p = true);

@@ -403,6 +403,14 @@ cudaError_t Ops<T>::lagrange(Chunk &c, void *p_out, double dt, int p_fold, int a
   return launched(c);
 }
 
+template <typename T> cudaError_t Ops<T>::face_strip(Chunk &c, int side, const StripJob &job, int depth, void *buf, bool pack) {
+  if (job.nfields == 0) return cudaSuccess;
+  const int n = std::max(c.nx, c.ny) + 2 * depth + 1;
+  dim3 g((n * depth + 127) / 128, job.nfields);
+  k_face_strip<T><<<g, 128, 0, c.stream>>>(fields<T>(c), mesh<T>(c), job, side, depth, (T *)buf, pack ? 1 : 0);
+  return launched(c);
+}
+
 template <typename T> cudaError_t Ops<T>::field_summary(Chunk &c, const int *store_ps) {
   dim3 b(32, 8);
   const int tx = (c.nx + 31) / 32, ty = (c.ny + 7) / 8;

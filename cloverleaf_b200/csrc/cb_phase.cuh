@@ -402,6 +402,49 @@ __global__ void k_tile_halo(Fields<T> D, Mesh<T> md, Fields<T> S, Mesh<T> ms, Ha
 }
 
 // ---------------------------------------------------------------------------
+// Face strips of a decomposed run: driver/comms.cpp:clover_exchange with the
+// index rules of src/serial/pack_kernel.cpp (the same elements as
+// k_tile_halo's, between a chunk and a linear buffer).  Along the face the
+// strip runs over [2 - depth, n + depth + 1], one element further for the
+// arrays that extend one past the cells that way; across it, element k
+// (k = 0 nearest the face):
+//   pack, the strip for the neighbour on    left (2 + e + k, .)   right (nx + 1 - k, .)
+//                                           bottom (., 2 + e + k)  top (., ny + 1 - k)
+//   unpack, the chunk's own halo on         left (1 - k, .)       right (nx + 2 + e + k, .)
+//                                           bottom (., 1 - k)      top (., ny + 2 + e + k)
+// with e = 1 for the arrays one longer across the face.  Element (p, k) of
+// field slot s sits at buf[off[s] + k * n_along + p - (2 - depth)].  One
+// thread per element, blockIdx.y the field slot.
+template <typename T>
+__global__ void k_face_strip(Fields<T> F, Mesh<T> m, StripJob job, int side, int depth, T *buf, int pack) {
+  if ((int)blockIdx.y >= job.nfields) return;
+  const int f = job.field[blockIdx.y];
+  const Kind kd = kind_of(f);
+  const bool lr = side == 1 || side == 2;
+  const int along_extra = lr ? (kd == VERTEX || kd == YFACE) : (kd == VERTEX || kd == XFACE);
+  const int e = lr ? (kd == VERTEX || kd == XFACE) : (kd == VERTEX || kd == YFACE);
+  const int n_along = (lr ? m.ny : m.nx) + 2 * depth + along_extra;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_along * depth) return;
+  const int p = 2 - depth + t % n_along, k = t / n_along;
+  int across;
+  if (side == 1)
+    across = pack ? 2 + e + k : 1 - k;
+  else if (side == 2)
+    across = pack ? m.nx + 1 - k : m.nx + 2 + e + k;
+  else if (side == 4)
+    across = pack ? 2 + e + k : 1 - k;
+  else
+    across = pack ? m.ny + 1 - k : m.ny + 2 + e + k;
+  const long long id = lr ? m.at(across, p) : m.at(p, across);
+  T *b = buf + job.off[blockIdx.y] + t;
+  if (pack)
+    *b = F.f[f][id];
+  else
+    F.f[f][id] = *b;
+}
+
+// ---------------------------------------------------------------------------
 // field_summary: src/serial/field_summary.cpp:44-104 -- ideal_gas on level 0
 // (writing pressure and soundspeed as the reference does), then the five
 // sums.  Per-cell terms are formed exactly as the reference forms them; the

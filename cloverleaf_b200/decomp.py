@@ -23,9 +23,12 @@ reductions of the step, over torch.distributed (NCCL on GPUs, gloo on CPUs).
   only (cb_set_external_faces), every update_halo an exchange of the internal
   faces followed by that fill (driver/update_halo.cpp), the PdV predictor's
   pressure halo likewise, calc_dt's minimum and the summary reduced over the
-  ranks.  The strips go through host memory (each exchanged field is read
-  back and written whole): a correctness path for small meshes, not a
-  performance one.
+  ranks.  The strips stay on the device: the library packs each face's
+  strip into a linear device buffer (cb_pack_face), the buffers go to the
+  neighbours -- NCCL send/recv of the device buffers when the process group
+  is NCCL's, through host memory for gloo -- and the library unpacks what
+  arrives into the halo (cb_unpack_face).  exchange() is the same exchange
+  on host arrays (the oracle's chunks in the tests).
 
 Fields are 2-D arrays in the reference's index convention (x fastest, a
 2-deep halo: cells (ny+4, nx+4), nodes (ny+5, nx+5), x faces (ny+4, nx+5),
@@ -42,6 +45,7 @@ import numpy as np
 EXTRA = {0: (0, 0), 1: (0, 0), 2: (0, 0), 3: (0, 0), 4: (0, 0), 5: (0, 0), 6: (0, 0), 7: (1, 1), 8: (1, 1), 9: (1, 1),
          10: (1, 1), 11: (1, 0), 12: (0, 1), 13: (1, 0), 14: (0, 1)}
 LEFT, RIGHT, BOTTOM, TOP = 0, 1, 2, 3  # driver/definitions.h:57 (chunk_left .. chunk_top)
+_FACE_BIT = {LEFT: 1, RIGHT: 2, BOTTOM: 4, TOP: 8}  # the library's CB_FACE_* bits
 
 
 @dataclasses.dataclass
@@ -181,7 +185,8 @@ class DecomposedChunk:
 
     def __init__(self, info: ChunkInfo, deck, precision: int = 0, device: int = 0, group=None):
         from .chunk import FACE_BOTTOM, FACE_LEFT, FACE_RIGHT, FACE_TOP, Chunk
-        self.info, self.deck, self.group = info, deck, group
+        self.info, self.deck, self.group, self.device = info, deck, group, device
+        self._bufs = {}
         self.c = Chunk(info.nx, info.ny, precision=precision, gamma=deck.gamma, device=device)
         faces = 0
         for side, bit in ((LEFT, FACE_LEFT), (RIGHT, FACE_RIGHT), (BOTTOM, FACE_BOTTOM), (TOP, FACE_TOP)):
@@ -199,11 +204,61 @@ class DecomposedChunk:
     def update_halo(self, fields, depth: int):
         fids = sorted(set(int(f) for f in fields))
         if any(n >= 0 for n in self.info.neighbours):
-            arrays = {f: self.c.read(f) for f in fids}
-            exchange(self.info, arrays, fids, depth, self.group)
-            for f in fids:
-                self.c.write(f, arrays[f])
+            self._exchange_strips(fids, depth)
         self.c.update_halo(fids, depth)
+
+    def _strip_buffers(self, side: int, fids: List[int], depth: int):
+        """The send and receive device buffers of one face strip, kept for the
+        chunk's life (the library's stream uses them after this call returns)."""
+        import torch
+        key = (side, tuple(fids), depth)
+        if key not in self._bufs:
+            from .chunk import FP64
+            n = self.c.face_strip_size(_FACE_BIT[side], fids, depth)
+            dtype = torch.float64 if self.c.precision == FP64 else torch.float32
+            dev = torch.device("cuda", self.device)
+            self._bufs[key] = (torch.empty(n, dtype=dtype, device=dev), torch.empty(n, dtype=dtype, device=dev), n)
+        return self._bufs[key]
+
+    def _exchange_strips(self, fids: List[int], depth: int):
+        """clover_exchange on the device: left / right strips, then bottom / top."""
+        import torch
+        import torch.distributed as dist
+        stream = torch.cuda.ExternalStream(self.c.stream(), device=torch.device("cuda", self.device))
+        nccl = dist.get_backend(self.group) == "nccl"
+        for pair in ((LEFT, RIGHT), (BOTTOM, TOP)):
+            sides = [s for s in pair if self.info.neighbours[s] >= 0]
+            if not sides:
+                continue
+            bufs = {s: self._strip_buffers(s, fids, depth) for s in sides}
+            for s in sides:
+                snd, _, n = bufs[s]
+                self.c.pack_face(_FACE_BIT[s], fids, depth, snd.data_ptr(), n)
+            if nccl:  # device buffers straight to the neighbours, ordered on the chunk's stream
+                with torch.cuda.stream(stream):
+                    ops = []
+                    for s in sides:
+                        snd, rcv, _ = bufs[s]
+                        ops.append(dist.P2POp(dist.isend, snd, self.info.neighbours[s], group=self.group))
+                        ops.append(dist.P2POp(dist.irecv, rcv, self.info.neighbours[s], group=self.group))
+                    for w in dist.batch_isend_irecv(ops):
+                        w.wait()
+            else:  # gloo: the strips through host memory
+                self.c.synchronize()
+                reqs, host = [], {}
+                for s in sides:
+                    snd, _, n = bufs[s]
+                    host[s] = torch.empty(n, dtype=snd.dtype)
+                    reqs.append(dist.isend(snd.cpu(), self.info.neighbours[s], group=self.group))
+                    reqs.append(dist.irecv(host[s], self.info.neighbours[s], group=self.group))
+                for r in reqs:
+                    r.wait()
+                with torch.cuda.stream(stream):
+                    for s in sides:
+                        bufs[s][1].copy_(host[s])
+            for s in sides:
+                _, rcv, n = bufs[s]
+                self.c.unpack_face(_FACE_BIT[s], fids, depth, rcv.data_ptr(), n)
 
     def pdv(self, predict: bool, dt: float, full: bool = False, halo_depth: int = 0):
         # the predictor's own pressure halo (src/serial/PdV.cpp:118-124) is an exchange too

@@ -199,6 +199,26 @@ int cb_field_summary(cb_chunk *c, double out[5]);
  * work already enqueued for both chunks and before any work enqueued later. */
 int cb_set_external_faces(cb_chunk *c, int faces);
 int cb_copy_tile_halo(cb_chunk *dst, cb_chunk *src, int side, const int fields[15], int depth);
+
+/* Chunks of a decomposed run in different processes (one per GPU): the face
+ * strips of driver/comms.cpp:clover_exchange (the pack / unpack index rules
+ * of src/serial/pack_kernel.cpp:27-300) between a chunk and a linear device
+ * buffer, for the caller to move between ranks (NCCL send/recv of device
+ * buffers, or any other transport).  cb_pack_face writes the strip the
+ * neighbour on `side` (one CB_FACE_* value) needs, `depth` deep, of the listed
+ * fields (fields[f] == 1) to dev_buf; cb_unpack_face fills the chunk's own
+ * halo on `side` from the strip that neighbour packed for it.  The strip is
+ * cb_face_strip_size elements of the chunk's precision: per listed field in
+ * field order, depth rows across the face of the field's extent along it
+ * (interior + 2 * depth, + 1 for the arrays one longer that way), the row
+ * nearest the face first.  Both enqueue on the chunk's stream (cb_get_stream)
+ * after its earlier work; neighbours along a face share its extent.  A
+ * caller's update_halo is then: left/right strips, then bottom/top (so the
+ * corners arrive), then cb_update_halo for the physical faces
+ * (cb_set_external_faces). */
+int cb_face_strip_size(cb_chunk *c, int side, const int fields[15], int depth, size_t *elements);
+int cb_pack_face(cb_chunk *c, int side, const int fields[15], int depth, void *dev_buf, size_t capacity);
+int cb_unpack_face(cb_chunk *c, int side, const int fields[15], int depth, const void *dev_buf, size_t capacity);
 /* Waits for everything enqueued on the chunk. */
 int cb_synchronize(cb_chunk *c);
 /* The CUDA stream (a cudaStream_t) the chunk's work is enqueued on, for
