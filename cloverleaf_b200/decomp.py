@@ -226,6 +226,8 @@ class DecomposedChunk:
         import torch.distributed as dist
         stream = torch.cuda.ExternalStream(self.c.stream(), device=torch.device("cuda", self.device))
         nccl = dist.get_backend(self.group) == "nccl"
+        if nccl:
+            torch.cuda.set_device(self.device)  # NCCL's point-to-point calls run on the current device
         for pair in ((LEFT, RIGHT), (BOTTOM, TOP)):
             sides = [s for s in pair if self.info.neighbours[s] >= 0]
             if not sides:
