@@ -3,8 +3,8 @@ through the C ABI, in the reference driver's call order, and print the
 field summaries.
 
   python -m cloverleaf_b200.run --deck clover.in
-  python -m cloverleaf_b200.run --bm 4608 --steps 2 [--precision fp32] [--no-fold] [--lagrangian | --fuse-calls |
-                                                      --resident [--fuse]]
+  python -m cloverleaf_b200.run --bm 4608 --steps 2 [--precision fp32] [--no-fold] [--lagrangian |
+                                                      --fuse-calls [--dt-ahead] | --resident [--fuse]]
   python -m cloverleaf_b200.run --ensemble 512 [--precision fp32] [--runs 3]
 """
 from __future__ import annotations
@@ -32,6 +32,8 @@ def main(argv=None):
                     help="host loop with one cb_lagrangian call in place of PdV, accelerate, PdV and flux_calc")
     ap.add_argument("--fuse-calls", action="store_true",
                     help="host loop with the chunk's call fusion on (the fused passes, one launch each)")
+    ap.add_argument("--dt-ahead", action="store_true",
+                    help="with --fuse-calls: the Lagrangian pass run ahead from calc_dt (cb_set_dt_ahead)")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--runs", type=int, default=1, help="ensemble runs after one warm-up run")
     ap.add_argument("--cells-per-cta", type=int, default=0, help="ensemble schedule: cells per CTA (0: the default schedule)")
@@ -42,7 +44,8 @@ def main(argv=None):
 
     dk = read_deck(args.deck) if args.deck else nudged(benchmark_deck(args.bm, end_step=args.steps or 87))
     c = Chunk(dk.x_cells, dk.y_cells, precision=FP32 if args.precision == "fp32" else FP64, device=args.device)
-    run = HydroRun(c, dk, fold=not args.no_fold, lagrangian=args.lagrangian, fuse_calls=args.fuse_calls)
+    run = HydroRun(c, dk, fold=not args.no_fold, lagrangian=args.lagrangian, fuse_calls=args.fuse_calls,
+                   dt_ahead=args.fuse_calls and args.dt_ahead)
     t = time.time()
     if args.resident:
         run.start()
