@@ -175,13 +175,15 @@ def compare(info, mine, ref, ref_is_whole):
     return bad
 
 
-def rank_body(rank, world, port, out, deck_name, on_gpu):
+def rank_body(rank, world, port, out, deck_name, on_gpu, mode="plain"):
     """One rank of a decomposed run of deck `deck_name` ("bm" or "circle").
 
     on_gpu False: the chunk is held by the oracle and the run is compared with
     the whole mesh's oracle run.  on_gpu True: the chunk is held by the
     library (DecomposedChunk on cuda:0) and the run is compared with the same
-    decomposed run on oracle chunks.  Every captured field of the chunk, the
+    decomposed run on oracle chunks; mode "fold" passes HydroRun's halo depths
+    to the calls and "fuse" turns the chunk's call fusion on as well (a chunk
+    with an internal face folds no halo, so both must give the same run).  Every captured field of the chunk, the
     step count and the dt of every step must agree to the bit; the final
     summary's sums within 1e-13 (relative) of the reference run's."""
     import datetime
@@ -200,7 +202,7 @@ def rank_body(rank, world, port, out, deck_name, on_gpu):
     if on_gpu:
         ref, ref_r = c, r
         c = DC.DecomposedChunk(info, dk)
-        r = HydroRun(c, dk, fold=False)
+        r = HydroRun(c, dk, fold=mode != "plain", fuse_calls=mode == "fuse")
         r.run()
         res = {"steps": (r.step, ref_r.step), "dt": r.dt_trace == ref_r.dt_trace,
                "bad": compare(info, c, ref, False),

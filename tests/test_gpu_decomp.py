@@ -56,12 +56,32 @@ def test_decomposed_gpu_run_is_the_decomposed_oracle_run(deck_name, world):
         out = mgr.dict()
         mp.spawn(rank_body, args=(world, port, out, deck_name, True), nprocs=world, join=True)
         res = dict(out)
+    _check(res, world)
+
+
+def _check(res, world):
     for r in range(world):
         assert res[r]["steps"][0] == res[r]["steps"][1], (r, res[r]["steps"])
         assert res[r]["dt"], r
         assert res[r]["summary_steps"], r
         assert res[r]["bad"] == [], (r, res[r]["bad"])
         assert max(res[r]["sums"]) <= 1e-13, (r, res[r]["sums"])
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("mode", ["fold", "fuse"])
+def test_decomposed_run_with_folds_and_call_fusion(mode):
+    """The circle deck on four ranks with HydroRun's halo depths passed to the
+    calls, and with the chunk's call fusion on: with internal faces the
+    chunks fold no halo and run the held-back calls as made, so the run is
+    the decomposed oracle run, bit for bit."""
+    from decomp_util import rank_body
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(rank_body, args=(4, port, out, "circle", True, mode), nprocs=4, join=True)
+        res = dict(out)
+    _check(res, 4)
 
 
 def _info(nx, ny):
