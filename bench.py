@@ -241,10 +241,10 @@ def run_form(precision, cells, warmup, steps, forced_dt=None, with_phases=False,
 
 
 def resident_form(precision, cells, warmup, steps, rank=0, world=1, fuse=True):
-    """Sets up a chunk, runs `warmup` steps as one device-resident graph, then
-    times `steps` steps as another (cb_run; the graph's capture and
-    instantiation inside the timed region); returns (ms, run, chunk, launches
-    in the timed region)."""
+    """Sets up a chunk, runs `warmup` steps as one device-resident graph
+    (cb_run), then times `steps` steps as another cb_run call, which launches
+    again the graph the warm-up call captured and instantiated (the chunk keeps
+    it); returns (ms, run, chunk, launches in the timed region)."""
     import torch
     from cloverleaf_b200 import Chunk, HydroRun
     dk = bench_deck(cells)

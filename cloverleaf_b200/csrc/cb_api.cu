@@ -496,6 +496,7 @@ int cb_destroy(cb_chunk *c) {
   if (!c) return CB_OK;
   select_device(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  run_cache_free(*c);
   release(c);
   delete c;
   return CB_OK;

@@ -110,6 +110,10 @@ struct Chunk {
   // When set, the phases that take dt (PdV, accelerate, flux_calc) read it
   // from this device address instead of their argument (cb_run's graph).
   const double *dt_dev = nullptr;
+  // cb_run's instantiated graph of the last run and its device buffers,
+  // launched again by a run that finds the chunk as it was captured for
+  // (cb_run.cu); freed by run_cache_free.
+  void *run_cache = nullptr;
 
   // folding writes reflected halos, so it needs every face on the physical boundary
   bool can_fold() const { return fold_enabled && nx >= 8 && ny >= 8 && external_faces == 15; }
@@ -117,6 +121,9 @@ struct Chunk {
   void *spare_base(int s) const { return (char *)buf[sbuf[s]] + off * esize; }
   template <int H> const CUtensorMap *map(int f) const { return &tmap[fbuf[f]][box_slot<H>()]; }
 };
+
+// Frees cb_run's kept graph (cb_run.cu).
+void run_cache_free(Chunk &c);
 
 } // namespace cb
 

@@ -13,6 +13,12 @@
 // driver/hydro.cpp:87-111) and set the conditions from the device.  The
 // host waits once, at the end.
 //
+// The run's entry state and constants live in device memory (RunParams),
+// written before each launch, so the instantiated graph is kept by the
+// chunk and launched again by the next cb_run that finds the chunk as the
+// graph was captured for (RunKey: the buffer map, the halo freshness, the
+// options and the constants its launches carry).
+//
 // The update_halo calls of the sequence follow the chunk's halo freshness
 // exactly as cb_update_halo does.  The body is captured from the state the
 // freshness settles in after the first steps; a pass that the first step
@@ -28,6 +34,8 @@
 #include <cstddef>
 #include <cstring>
 #include <initializer_list>
+#include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -65,17 +73,25 @@ struct RunConsts {
   int end_step, summary_frequency, last_step, step0, max_records;
 };
 
+// What a launch of the run's graph starts from: the constants and the entry
+// state, copied to the device before each launch.
+struct RunParams {
+  RunConsts k;
+  double time, dtold;
+  int step, advect_x;
+};
+
 constexpr int RUN_KERNELS_PER_STEP = 3; // k_run_begin, k_run_dt, k_run_end
 
-__global__ void k_run_init(RunState *s, int step, double time, double dtold, int advect_x) {
-  s->dt = dtold;
-  s->dtold = dtold;
-  s->time = time;
-  s->step = step;
+__global__ void k_run_init(RunState *s, const RunParams *p) {
+  s->dt = p->dtold;
+  s->dtold = p->dtold;
+  s->time = p->time;
+  s->step = p->step;
   s->nsum = 0;
   s->sum_runs = 0;
   s->small = 0;
-  s->advect_x = advect_x;
+  s->advect_x = p->advect_x;
   s->records_due = 0;
 }
 
@@ -87,8 +103,9 @@ __global__ void k_run_begin(RunState *s, unsigned long long *dt_bits) {
 
 // dt of the step from calc_dt's minimum (driver/timestep.cpp:75-96), kept on
 // the device for the phases that read it; the advection branch of the step.
-__global__ void k_run_dt(RunState *s, const unsigned long long *dt_bits, RunConsts k, double *dt_dev, double *trace,
+__global__ void k_run_dt(RunState *s, const unsigned long long *dt_bits, const RunParams *p, double *dt_dev, double *trace,
                          cudaGraphConditionalHandle hadv) {
+  const RunConsts &k = p->k;
   const double dtlp = __longlong_as_double((long long)*dt_bits);
   double dt = g_big;
   if (dtlp <= dt) dt = dtlp;
@@ -107,7 +124,8 @@ __global__ void k_run_dt(RunState *s, const unsigned long long *dt_bits, RunCons
 
 // End of a step (driver/hydro.cpp:87-111): direction toggle, time, the end
 // test, the summaries due, and whether the loop goes on.
-__global__ void k_run_end(RunState *s, RunConsts k, cudaGraphConditionalHandle hsum, cudaGraphConditionalHandle hloop) {
+__global__ void k_run_end(RunState *s, const RunParams *p, cudaGraphConditionalHandle hsum, cudaGraphConditionalHandle hloop) {
+  const RunConsts &k = p->k;
   s->advect_x = !s->advect_x;
   s->time += s->dt;
   const bool complete = s->time + g_small > k.end_time || s->step >= k.end_step;
@@ -124,7 +142,8 @@ __global__ void k_run_end(RunState *s, RunConsts k, cudaGraphConditionalHandle h
 
 // The summary record(s) of the step: step, time and the five sums
 // (the report line of driver/field_summary.cpp).
-__global__ void k_run_record(RunState *s, const double *sums, double *records, RunConsts k) {
+__global__ void k_run_record(RunState *s, const double *sums, double *records, const RunParams *p) {
+  const RunConsts &k = p->k;
   for (int r = 0; r < s->records_due; ++r) {
     if (s->nsum < k.max_records) {
       double *rec = records + 7 * (size_t)s->nsum;
@@ -359,15 +378,30 @@ cudaError_t add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGr
   return cudaSuccess;
 }
 
-// Device buffers of one run.
+// Device buffers of a run's graph: its scalar state, parameters, dt, and
+// room for trace_cap dt values and rec_cap summary records.
 struct RunBufs {
   RunState *st = nullptr;
+  RunParams *par = nullptr;
   double *dt_dev = nullptr, *trace = nullptr, *records = nullptr;
+  int trace_cap = 0, rec_cap = 0;
   ~RunBufs() {
     cudaFree(st);
+    cudaFree(par);
     cudaFree(dt_dev);
     cudaFree(trace);
     cudaFree(records);
+  }
+  cudaError_t alloc(int ntrace, int nrec) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&st, sizeof(RunState))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&par, sizeof(RunParams))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&dt_dev, sizeof(double))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&trace, sizeof(double) * (size_t)ntrace)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&records, sizeof(double) * 7 * (size_t)nrec)) != cudaSuccess) return e;
+    trace_cap = ntrace;
+    rec_cap = nrec;
+    return cudaSuccess;
   }
 };
 
@@ -376,12 +410,39 @@ struct Counts {
   long long body = 0, adv[2] = {0, 0}, sum = 0;
 };
 
+// Everything a captured run bakes into its launches besides the device
+// buffers it owns: a graph is launched again only for an equal key.
+struct RunKey {
+  const void *buf[NUM_BUF];
+  const void *geom[NUM_GEOM], *geom_t[NUM_GEOM];
+  const void *rgeom;
+  int fbuf[15], sbuf[NUM_SPARE], fresh[15];
+  int precision, fold, fuse, can_fold;
+  double gamma, dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;
+};
+
+// The instantiated graph of a chunk's last run (Chunk::run_cache).
+struct RunCache {
+  RunKey key;
+  RunBufs rb;
+  Counts n;
+  bool fuse = false;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  RunParams *h_par = nullptr; // pinned: the parameters of the next launch
+  ~RunCache() {
+    if (x) cudaGraphExecDestroy(x);
+    if (g) cudaGraphDestroy(g);
+    if (h_par) cudaFreeHost(h_par);
+  }
+};
+
 // Captures the loop into *g: init, then WHILE { step }.  Every capture this
 // function began has ended when it returns; *g is set only once the
 // top-level capture has ended, and the caller owns it from then on.
 template <typename T>
-cudaError_t capture_run(Chunk &c, Seq<T> &q, const RunBufs &rb, const RunConsts &k, const cb_run_state &in, cudaStream_t s0,
-                        cudaStream_t s1, cudaGraph_t *g, Counts &n, std::string &why) {
+cudaError_t capture_run(Chunk &c, Seq<T> &q, const RunBufs &rb, cudaStream_t s0, cudaStream_t s1, cudaGraph_t *g, Counts &n,
+                        std::string &why) {
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
   bool top_open = false;
   auto abandon = [&](cudaError_t err) {
@@ -398,7 +459,7 @@ cudaError_t capture_run(Chunk &c, Seq<T> &q, const RunBufs &rb, const RunConsts 
   cudaError_t e;
   if ((e = cudaStreamBeginCapture(s0, mode)) != cudaSuccess) return abandon(e);
   top_open = true;
-  k_run_init<<<1, 1, 0, s0>>>(rb.st, in.step, in.time, in.dtold, in.advect_x ? 1 : 0);
+  k_run_init<<<1, 1, 0, s0>>>(rb.st, rb.par);
   if ((e = cudaGetLastError()) != cudaSuccess) return abandon(e);
   cudaGraph_t top = nullptr;
   {
@@ -424,7 +485,7 @@ cudaError_t capture_run(Chunk &c, Seq<T> &q, const RunBufs &rb, const RunConsts 
   k_run_begin<<<1, 1, 0, s0>>>(rb.st, c.d_dt_bits);
   q.run(cudaGetLastError());
   q.timestep_front();
-  k_run_dt<<<1, 1, 0, s0>>>(rb.st, c.d_dt_bits, k, rb.dt_dev, rb.trace, hadv);
+  k_run_dt<<<1, 1, 0, s0>>>(rb.st, c.d_dt_bits, rb.par, rb.dt_dev, rb.trace, hadv);
   q.run(cudaGetLastError());
   q.lagrange();
   if (q.err != cudaSuccess) return abandon(q.err);
@@ -457,7 +518,7 @@ cudaError_t capture_run(Chunk &c, Seq<T> &q, const RunBufs &rb, const RunConsts 
     }
   }
   q.reset();
-  k_run_end<<<1, 1, 0, s0>>>(rb.st, k, hsum, hloop);
+  k_run_end<<<1, 1, 0, s0>>>(rb.st, rb.par, hsum, hloop);
   q.run(cudaGetLastError());
   if (q.err != cudaSuccess) return abandon(q.err);
   cudaGraph_t sum;
@@ -471,7 +532,7 @@ cudaError_t capture_run(Chunk &c, Seq<T> &q, const RunBufs &rb, const RunConsts 
   const long long ls = c.launches;
   if ((e = cudaStreamBeginCaptureToGraph(s0, sum, nullptr, nullptr, 0, mode)) != cudaSuccess) return abandon(e);
   q.summary();
-  k_run_record<<<1, 1, 0, s0>>>(rb.st, c.d_sums, rb.records, k);
+  k_run_record<<<1, 1, 0, s0>>>(rb.st, c.d_sums, rb.records, rb.par);
   q.run(cudaGetLastError());
   {
     cudaGraph_t got = nullptr;
@@ -523,73 +584,108 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
     }
   }
 
-  // device buffers of the run
-  RunBufs rb;
-  cudaError_t e;
+  // what the captured graph bakes in: a kept graph with the same key is launched again
   const int max_records = std::max(max_summaries, 0);
-  if ((e = cudaMalloc(&rb.st, sizeof(RunState))) != cudaSuccess) return cuda_fail(e, "cb_run");
-  if ((e = cudaMalloc(&rb.dt_dev, sizeof(double))) != cudaSuccess) return cuda_fail(e, "cb_run");
-  if ((e = cudaMalloc(&rb.trace, sizeof(double) * (size_t)max_steps)) != cudaSuccess) return cuda_fail(e, "cb_run");
-  if ((e = cudaMalloc(&rb.records, sizeof(double) * 7 * (size_t)std::max(max_records, 1))) != cudaSuccess) return cuda_fail(e, "cb_run");
-
-  RunConsts k{};
-  k.dtmin = p->dtmin;
-  k.dtmax = p->dtmax;
-  k.dtrise = p->dtrise;
-  k.end_time = p->end_time;
-  k.end_step = p->end_step;
-  k.summary_frequency = p->summary_frequency;
-  k.step0 = state->step;
-  k.last_step = state->step + max_steps;
-  k.max_records = max_records;
-
-  // the loop's graph, its body captured from the settled freshness
-  cudaStream_t s0 = nullptr, s1 = nullptr;
-  if ((e = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "cb_run");
-  if ((e = cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking)) != cudaSuccess) {
-    cudaStreamDestroy(s0);
-    return cuda_fail(e, "cb_run");
+  RunKey key;
+  std::memset(&key, 0, sizeof key);
+  for (int b = 0; b < NUM_BUF; ++b) key.buf[b] = c->buf[b];
+  for (int g = 0; g < NUM_GEOM; ++g) {
+    key.geom[g] = c->geom_d[g];
+    key.geom_t[g] = c->geom_t[g];
   }
-  Seq<T> q(*c, true, fold, dk);
-  q.fuse = p->fuse != 0 && fold && c->can_fold();
-  if (q.fuse) q.last_flag = reinterpret_cast<const int *>(reinterpret_cast<const char *>(rb.st) + offsetof(RunState, last));
-  std::memcpy(q.fresh, settled[3], sizeof q.fresh);
-  const cudaStream_t user = c->stream;
-  const long long launches0 = c->launches;
-  c->dt_dev = rb.dt_dev;
-  cudaGraph_t g = nullptr;
-  Counts n;
-  std::string why;
-  e = capture_run<T>(*c, q, rb, k, *state, s0, s1, &g, n, why);
-  c->dt_dev = nullptr;
-  c->stream = user;
-  c->launches = launches0;
-  std::memcpy(c->fbuf, fbuf0, sizeof fbuf0); // (a capture that stopped midway may leave a sweep's swap undone)
-  std::memcpy(c->sbuf, sbuf0, sizeof sbuf0);
-  cudaGraphExec_t x = nullptr;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
-  long long restore_launches = 0;
-  if (e == cudaSuccess) {
-    for (int d = 0; d < 2 && e == cudaSuccess; ++d)
-      if (pro[d].nfields) e = Ops<T>::update_halo(*c, pro[d], d + 1);
-    if (e == cudaSuccess) e = cudaGraphLaunch(x, c->stream);
-    if (e == cudaSuccess && q.fuse) {
-      // the fused second sweeps left energy1 / xvel1 / yvel1 stale: rebuild
-      // them as the phase-by-phase step leaves them (the last first sweep's
-      // momentum output, in the spares, gives the velocities' halo ring)
-      const long long l = c->launches;
-      e = Ops<T>::restore_level1(*c, c->spare_base(2), c->spare_base(3));
-      restore_launches = c->launches - l;
-      c->launches = l;
+  key.rgeom = c->rgeom_d;
+  std::memcpy(key.fbuf, fbuf0, sizeof key.fbuf);
+  std::memcpy(key.sbuf, sbuf0, sizeof key.sbuf);
+  std::memcpy(key.fresh, settled[3], sizeof key.fresh);
+  key.precision = c->precision;
+  key.fold = fold ? 1 : 0;
+  key.fuse = p->fuse != 0 ? 1 : 0;
+  key.can_fold = c->can_fold() ? 1 : 0;
+  key.gamma = c->gamma;
+  key.dtc_safe = dk.dtc_safe;
+  key.dtu_safe = dk.dtu_safe;
+  key.dtv_safe = dk.dtv_safe;
+  key.dtdiv_safe = dk.dtdiv_safe;
+  RunCache *rc = static_cast<RunCache *>(c->run_cache);
+  if (rc && (std::memcmp(&rc->key, &key, sizeof key) != 0 || rc->rb.trace_cap < max_steps || rc->rb.rec_cap < std::max(max_records, 1))) {
+    run_cache_free(*c);
+    rc = nullptr;
+  }
+  cudaError_t e;
+  if (!rc) {
+    // the loop's graph, its body captured from the settled freshness
+    std::unique_ptr<RunCache> nc(new (std::nothrow) RunCache);
+    if (!nc) return fail(CB_ECUDA, "cb_run: out of host memory");
+    nc->key = key;
+    if ((e = nc->rb.alloc(std::max(max_steps, 1024), std::max(max_records, 256))) != cudaSuccess) return cuda_fail(e, "cb_run");
+    if ((e = cudaMallocHost(&nc->h_par, sizeof(RunParams))) != cudaSuccess) return cuda_fail(e, "cb_run");
+    cudaStream_t s0 = nullptr, s1 = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "cb_run");
+    if ((e = cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking)) != cudaSuccess) {
+      cudaStreamDestroy(s0);
+      return cuda_fail(e, "cb_run");
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    Seq<T> q(*c, true, fold, dk);
+    q.fuse = p->fuse != 0 && fold && c->can_fold();
+    if (q.fuse) q.last_flag = reinterpret_cast<const int *>(reinterpret_cast<const char *>(nc->rb.st) + offsetof(RunState, last));
+    std::memcpy(q.fresh, settled[3], sizeof q.fresh);
+    const cudaStream_t user = c->stream;
+    const long long launches0 = c->launches;
+    c->dt_dev = nc->rb.dt_dev;
+    std::string why;
+    e = capture_run<T>(*c, q, nc->rb, s0, s1, &nc->g, nc->n, why);
+    c->dt_dev = nullptr;
+    c->stream = user;
+    c->launches = launches0;
+    std::memcpy(c->fbuf, fbuf0, sizeof fbuf0); // (a capture that stopped midway may leave a sweep's swap undone)
+    std::memcpy(c->sbuf, sbuf0, sizeof sbuf0);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&nc->x, nc->g, 0);
+    cudaStreamDestroy(s0);
+    cudaStreamDestroy(s1);
+    if (e != cudaSuccess) {
+      if (!why.empty()) return fail(CB_ESTATE, "cb_run: " + why);
+      return cuda_fail(e, "cb_run");
+    }
+    nc->fuse = q.fuse;
+    rc = nc.release();
+    c->run_cache = rc;
   }
-  if (x) cudaGraphExecDestroy(x);
-  if (g) cudaGraphDestroy(g);
-  cudaStreamDestroy(s0);
-  cudaStreamDestroy(s1);
+  const RunBufs &rb = rc->rb;
+  const Counts &n = rc->n;
+
+  // this launch's constants and entry state
+  RunParams &hp = *rc->h_par;
+  hp.k = RunConsts{};
+  hp.k.dtmin = p->dtmin;
+  hp.k.dtmax = p->dtmax;
+  hp.k.dtrise = p->dtrise;
+  hp.k.end_time = p->end_time;
+  hp.k.end_step = p->end_step;
+  hp.k.summary_frequency = p->summary_frequency;
+  hp.k.step0 = state->step;
+  hp.k.last_step = state->step + max_steps;
+  hp.k.max_records = max_records;
+  hp.time = state->time;
+  hp.dtold = state->dtold;
+  hp.step = state->step;
+  hp.advect_x = x0 ? 1 : 0;
+  long long restore_launches = 0;
+  e = cudaMemcpyAsync(rb.par, &hp, sizeof hp, cudaMemcpyHostToDevice, c->stream);
+  for (int d = 0; d < 2 && e == cudaSuccess; ++d)
+    if (pro[d].nfields) e = Ops<T>::update_halo(*c, pro[d], d + 1);
+  if (e == cudaSuccess) e = cudaGraphLaunch(rc->x, c->stream);
+  if (e == cudaSuccess && rc->fuse) {
+    // the fused second sweeps left energy1 / xvel1 / yvel1 stale: rebuild
+    // them as the phase-by-phase step leaves them (the last first sweep's
+    // momentum output, in the spares, gives the velocities' halo ring)
+    const long long l = c->launches;
+    e = Ops<T>::restore_level1(*c, c->spare_base(2), c->spare_base(3));
+    restore_launches = c->launches - l;
+    c->launches = l;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
-    if (!why.empty()) return fail(CB_ESTATE, "cb_run: " + why);
+    run_cache_free(*c);
     return cuda_fail(e, "cb_run");
   }
 
@@ -619,6 +715,17 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
   if (h.small) return fail(CB_ESTATE, "cb_run: small timestep " + std::to_string(h.dt) + " at step " + std::to_string(h.step));
   return CB_OK;
 }
+
+} // namespace
+
+namespace cb {
+void run_cache_free(Chunk &c) {
+  delete static_cast<RunCache *>(c.run_cache);
+  c.run_cache = nullptr;
+}
+} // namespace cb
+
+namespace {
 
 cudaError_t select_device(const cb_chunk *c) {
   int cur = -1;

@@ -214,3 +214,39 @@ def test_run_fused_launch_count():
         r.run_steps_on_device(fuse=fuse)
         counts.append(c.launch_count() - n0)
     assert counts[1] == counts[0] - 7 * 12 + 4
+
+
+@pytest.mark.parametrize("fuse", [False, True], ids=["unfused", "fused"])
+def test_kept_graph_follows_the_chunk(fuse):
+    """cb_run keeps its instantiated graph for the next run on the chunk and
+    launches it again only when the chunk is as the graph was captured for:
+    runs of a few steps each, with gamma changed between two of them (the
+    pressure's factor is baked into the launches) and a phase-by-phase step
+    in between (which moves the double-buffered fields to other buffers),
+    end bit-identical to the host-driven loop making the same changes."""
+    dk = deck_b()
+
+    def host_then(r, c, steps):
+        for _ in range(steps):
+            r.hydro_step()
+
+    c1 = Chunk(dk.x_cells, dk.y_cells, gamma=dk.gamma)
+    r1 = HydroRun(c1, dk)
+    r1.start()
+    host_then(r1, c1, 6)
+    c1.set_gamma(1.62)
+    host_then(r1, c1, 7)
+
+    c2 = Chunk(dk.x_cells, dk.y_cells, gamma=dk.gamma)
+    r2 = HydroRun(c2, dk)
+    r2.start()
+    r2.hydro_step()  # a settled halo state for the graph
+    r2.run_steps_on_device(max_steps=3, fuse=fuse)
+    r2.run_steps_on_device(max_steps=6, fuse=fuse)  # the kept graph again
+    c2.set_gamma(1.62)
+    r2.run_steps_on_device(max_steps=9, fuse=fuse)  # captured anew: gamma changed
+    r2.hydro_step()  # the double-buffered fields now live in other buffers
+    r2.run_steps_on_device(max_steps=13, fuse=fuse)  # captured anew: another buffer map
+    assert_same(c1, r1, c2, r2)
+    c1.close()
+    c2.close()
