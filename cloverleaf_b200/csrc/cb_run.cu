@@ -417,7 +417,7 @@ struct RunKey {
   const void *geom[NUM_GEOM], *geom_t[NUM_GEOM];
   const void *rgeom;
   int fbuf[15], sbuf[NUM_SPARE], fresh[15];
-  int precision, fold, fuse, can_fold;
+  int precision, fold, fuse, can_fold, faces;
   double gamma, dtc_safe, dtu_safe, dtv_safe, dtdiv_safe;
 };
 
@@ -601,6 +601,7 @@ int run_impl(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_s
   key.fold = fold ? 1 : 0;
   key.fuse = p->fuse != 0 ? 1 : 0;
   key.can_fold = c->can_fold() ? 1 : 0;
+  key.faces = c->external_faces; // the reflective fill's faces
   key.gamma = c->gamma;
   key.dtc_safe = dk.dtc_safe;
   key.dtu_safe = dk.dtu_safe;

@@ -278,7 +278,7 @@ typedef struct {
  * a few device buffers) until it is destroyed: the next cb_run on it
  * launches that graph again, without capturing, when the chunk is as the
  * graph was captured for -- the same buffers and buffer map, halo state,
- * gamma, fold / fuse and safety factors -- and max_steps and max_summaries
+ * physical faces, gamma, fold / fuse and safety factors -- and max_steps and max_summaries
  * fit the kept buffers; otherwise it captures anew. */
 int cb_run(cb_chunk *c, const cb_run_params *p, cb_run_state *state, int max_steps, double *dt_trace, double *summaries,
            int max_summaries, int *nsummaries);
