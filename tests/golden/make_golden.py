@@ -14,7 +14,8 @@ and, for the visit deck, the files driver/visit.cpp:31-192 writes as
   <name>.visit.sha256  one line per file (clover.visit and each .vtk): its name
                        and the sha256 of its bytes
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref/serial-capture and oracle/_ref/serial)
+Usage: python tests/golden/make_golden.py [deck names]   (needs oracle/_ref/serial-capture and
+oracle/_ref/serial, and the reference checkout for the InputDecks decks)
 """
 import hashlib
 import os
@@ -49,6 +50,26 @@ DEFAULT_DECK = """*clover
 """
 
 
+# The reference checkout: CLOVER_REFERENCE, else the directory beside this repository.
+REFERENCE = os.environ.get("CLOVER_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
+
+# The reference's own shock-tube and QA decks (InputDecks/), read from the
+# reference checkout and written back in this package's deck format: name ->
+# (file, keep the final fields).  The two larger runs keep summaries only.
+REFERENCE_DECKS = {"sodx10x2": ("clover_sodx.in", True), "sody2x10": ("clover_sody.in", True),
+                   "sodxy10x10": ("clover_sodxy.in", True), "sodbig200": ("clover_sodbig.in", False),
+                   "qa1024": ("clover_qa.in", False)}
+
+
+def reference_decks():
+    out = {}
+    for name, (fn, keep) in REFERENCE_DECKS.items():
+        with open(os.path.join(REFERENCE, "InputDecks", fn)) as f:
+            raw = D.parse_deck(f.read(), nudge=False)
+        out[name] = (D.format_deck(raw), keep)
+    return out
+
+
 def decks():
     out = {"default10x2": (DEFAULT_DECK, True)}
     out["bm32x87"] = (D.format_deck(D.benchmark_deck(32, 87)), True)
@@ -61,6 +82,7 @@ def decks():
     out["circ24x20x70"] = (D.format_deck(c), True)
     # the reference benchmark at 960^2, 87 steps (test_problem 2): summaries only
     out["bm960x87"] = (D.format_deck(D.benchmark_deck(960, 87, test_problem=2)), False)
+    out.update(reference_decks())
     return out
 
 
@@ -121,10 +143,13 @@ def write_visit_fixture():
     print(name, len(files), "visit files")
 
 
-def main():
-    write_dump_fixture()
-    write_visit_fixture()
+def main(only=None):
+    if only is None:
+        write_dump_fixture()
+        write_visit_fixture()
     for name, (text, keep_fields) in decks().items():
+        if only is not None and name not in only:
+            continue
         res = oracle.run_reference(text)
         if res["returncode"] != 0:
             raise SystemExit(f"{name}: reference exited {res['returncode']}")
@@ -144,4 +169,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)  # names: only those decks

@@ -4,7 +4,9 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-SMALL_DECKS = ["default10x2", "bm32x87", "bm40x24x120", "circ24x20x70"]
+SMALL_DECKS = ["default10x2", "bm32x87", "bm40x24x120", "circ24x20x70", "sodx10x2", "sody2x10", "sodxy10x10"]
+# the reference's own larger decks (InputDecks/clover_sodbig.in, clover_qa.in): summaries only
+SUMMARY_DECKS = ["sodbig200", "qa1024"]
 # (field id, kind) of the arrays a fields.bin holds
 CAPTURED = [(0, "cell"), (2, "cell"), (4, "cell"), (5, "cell"), (6, "cell"), (7, "node"), (9, "node"),
             (11, "xface"), (12, "yface")]

@@ -4,6 +4,10 @@
   (cloverleaf_b200.HydroRun) on the golden decks: every final per-cell field
   bit-identical to the reference serial build's, every summary within 1e-12
   relative (small decks: the reference's sequential sum has ~1e-15 rounding).
+* The golden decks include the reference's own Sod shock tubes
+  (InputDecks/clover_sod*.in, 10 x 2, 2 x 10, 10 x 10); its 200^2 Sod deck and
+  its 1024^2 QA deck are checked through their summaries, the oracle's final
+  fields and the fused device-resident graph.
 * Halo folding on and off give bit-identical runs.
 * Config 1 (960^2, 87 steps, test_problem 2): the driver's PASS criterion,
   per-cell bit parity against the oracle, and the summaries against the
@@ -18,7 +22,7 @@ import pytest
 import oracle
 from cloverleaf_b200 import Chunk, HydroRun
 from cloverleaf_b200 import deck as D
-from golden_util import CAPTURED, SMALL_DECKS, deck_text, fields, interior, rel, summaries
+from golden_util import CAPTURED, SMALL_DECKS, SUMMARY_DECKS, deck_text, fields, interior, rel, summaries
 
 pytestmark = pytest.mark.gpu
 
@@ -89,3 +93,41 @@ def test_config1_960_pass_and_parity():
     last = run.summaries[-1]
     for a, b in zip((last.vol, last.mass, last.ie, last.ke, last.press), ex):
         assert rel(a, b) <= 1e-13, (a, b)
+
+
+@pytest.mark.parametrize("name", SUMMARY_DECKS)
+def test_reference_decks(name):
+    """The reference's own Sod deck (200^2 to t = 30, 1,330 steps) and QA deck
+    (1024^2, a domain centred on the origin): the phase-by-phase run's
+    summaries within 5e-11 of the reference's printed ones (its sequential
+    sums carry their own rounding), its final fields bit for bit the
+    oracle's, its last sums within 1e-13 of the exactly rounded sums; the
+    fused device-resident graph ends with the same fields to the bit."""
+    dk = D.parse_deck(deck_text(name))
+    c, run = gpu_run(dk)
+    gold = summaries(name)
+    assert [(s.step, s.time) for s in run.summaries] == [(g[0], g[1]) for g in gold]
+    for s, g in zip(run.summaries, gold):
+        for a, b in zip((s.vol, s.mass, s.ie, s.ke, s.press), g[2:]):
+            assert rel(a, b) <= 5e-11, (name, s.step, a, b)
+    o = oracle.OracleChunk(dk.x_cells, dk.y_cells)
+    o.run(dk, max_summaries=4096)
+    for fid, kind in CAPTURED:
+        got = interior(c.read(fid), dk.x_cells, dk.y_cells, kind)
+        ref = interior(o.field(fid), dk.x_cells, dk.y_cells, kind)
+        assert np.array_equal(got, ref), (name, fid)
+    ex = o.field_summary(exact=True)
+    last = run.summaries[-1]
+    for a, b in zip((last.vol, last.mass, last.ie, last.ke, last.press), ex):
+        assert rel(a, b) <= 1e-13, (name, a, b)
+    o.close()
+    g = Chunk(dk.x_cells, dk.y_cells)
+    r2 = HydroRun(g, dk)
+    r2.start()
+    r2.run_steps_on_device(fuse=True)
+    assert r2.step == run.step and r2.dt_trace == run.dt_trace
+    for fid, kind in CAPTURED:
+        assert np.array_equal(interior(g.read(fid), dk.x_cells, dk.y_cells, kind),
+                              interior(c.read(fid), dk.x_cells, dk.y_cells, kind)), (name, fid)
+    g.close()
+    c.close()

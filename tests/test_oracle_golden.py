@@ -3,7 +3,9 @@
 The golden fixtures were produced by the reference driver + serial model
 compiled from the reference sources (tests/golden/make_golden.py).  The
 oracle must reproduce them bit for bit: every summary value and every final
-per-cell field.  The 960^2 deck also checks the reference's hard-coded
+per-cell field; the decks include the reference's own Sod shock tubes
+(InputDecks/clover_sod*.in: 10 x 2, 2 x 10, 10 x 10 and 200 x 200) and its
+QA deck (clover_qa.in, 1024^2).  The 960^2 deck also checks the reference's hard-coded
 expected kinetic energy (driver/report.cpp:79-80, test_problem 2).
 """
 import numpy as np
@@ -11,7 +13,7 @@ import pytest
 
 import oracle
 from cloverleaf_b200 import deck as D
-from golden_util import CAPTURED, SMALL_DECKS, deck_text, fields, interior, summaries
+from golden_util import CAPTURED, SMALL_DECKS, SUMMARY_DECKS, deck_text, fields, interior, summaries
 
 
 @pytest.mark.parametrize("name", SMALL_DECKS)
@@ -38,6 +40,16 @@ def test_oracle_config1_960_pass():
     ke = recs[-1][5]
     qa_diff = abs(100.0 * (ke / 1.19316898756307) - 100.0)  # driver/report.cpp:79-80, :102
     assert qa_diff < 0.001
+
+
+@pytest.mark.parametrize("name", SUMMARY_DECKS)
+def test_oracle_reference_decks_summaries(name):
+    """The reference's Sod deck on 200^2 to t = 30 (1,330 steps) and its QA deck
+    on 1024^2 over a domain centred on the origin: every summary bit for bit."""
+    dk = D.parse_deck(deck_text(name))
+    c = oracle.OracleChunk(dk.x_cells, dk.y_cells)
+    recs, steps, _ = c.run(dk, max_summaries=4096)
+    assert recs == summaries(name)
 
 
 def test_default_deck_test_problem_1():
