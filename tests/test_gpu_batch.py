@@ -248,3 +248,33 @@ def test_autotune_picks_the_fastest(decks):
         b.run()
         b.synchronize()
         assert all(b.result(k).status == B.DECK_DONE for k in range(len(decks)))
+
+
+def test_batch_runs_the_golden_decks_as_the_reference_does():
+    """One batch of the golden decks the reference build ran (the reference's
+    own Sod decks InputDecks/clover_sodxy.in, 10 x 10, and clover_sodbig.in,
+    200^2 over 1,330 steps, with the benchmark and moving-circle decks):
+    every final field the fixtures hold bit for bit the reference's, every
+    summary at the reference's steps and times with sums within 1e-12 of
+    its printed ones (its sums are sequential, the batch's a reduction)."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from cloverleaf_b200 import deck as D
+    from golden_util import CAPTURED, GOLDEN, deck_text, fields, interior, rel, summaries
+    names = ["sodxy10x10", "bm32x87", "bm40x24x120", "circ24x20x70", "sodbig200"]
+    decks = [D.parse_deck(deck_text(n)) for n in names]
+    with Batch(decks, FP64) as b:
+        b.run()
+        b.synchronize()
+        for k, (name, dk) in enumerate(zip(names, decks)):
+            gold = summaries(name)
+            got = b.summaries(k)
+            assert [(s.step, s.time) for s in got] == [(g[0], g[1]) for g in gold], name
+            for s, g in zip(got, gold):
+                for x, y in zip((s.vol, s.mass, s.ie, s.ke, s.press), g[2:]):
+                    assert rel(x, y) <= 1e-12, (name, s.step, x, y)
+            if os.path.exists(os.path.join(GOLDEN, name + ".fields.bin")):
+                gf = fields(name)
+                for fid, kind in CAPTURED:
+                    assert np.array_equal(interior(b.read(k, fid), dk.x_cells, dk.y_cells, kind), gf[fid]), (name, fid)
