@@ -78,3 +78,35 @@ def test_fp32_summary_sums_are_fp64():
     # volume of [0,10]^2 from FP32 cell widths: exact in FP64 accumulation to ~1e-6
     assert abs(s[0] - 100.0) <= 1e-4
     c32.close()
+
+
+@pytest.mark.parametrize("name", ["sodx10x2", "sody2x10", "sodxy10x10", "qa1024"])
+def test_fp32_on_the_reference_decks(name):
+    """The FP32 form on the reference's own short decks (the Sod shock tubes
+    InputDecks/clover_sodx.in, clover_sody.in, clover_sodxy.in to t = 3, and
+    clover_qa.in, 1024^2 to t = 3), through the fused device-resident graph:
+    the same step count and summary steps as the reference build, every sum
+    within 1e-5 of its printed FP64 sums, and the final density within 1e-5
+    (L1, relative) of its fields where the fixtures hold them.  (Over long
+    runs the FP32 dt sequence parts from FP64's: clover_sodbig.in, 200^2 to
+    t = 30, ends three steps early in FP32.)"""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from cloverleaf_b200 import deck as D
+    from golden_util import GOLDEN, deck_text, fields, interior, rel, summaries
+    dk = D.parse_deck(deck_text(name))
+    c = Chunk(dk.x_cells, dk.y_cells, precision=FP32)
+    r = HydroRun(c, dk)
+    r.start()
+    r.run_steps_on_device(fuse=True)
+    gold = summaries(name)
+    assert [s.step for s in r.summaries] == [g[0] for g in gold]
+    for s, g in zip(r.summaries, gold):
+        for a, b in zip((s.vol, s.mass, s.ie, s.ke, s.press), g[2:]):
+            assert rel(a, b) <= 1e-5, (name, s.step, a, b)
+    if os.path.exists(os.path.join(GOLDEN, name + ".fields.bin")):
+        x = interior(c.read(0), dk.x_cells, dk.y_cells, "cell")
+        y = fields(name)[0]
+        assert np.abs(x - y).sum() / np.abs(y).sum() <= 1e-5
+    c.close()
