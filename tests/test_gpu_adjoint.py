@@ -148,3 +148,30 @@ def test_torch_autograd_harness():
     assert np.allclose(en.grad.numpy(), 2.0 * ge, rtol=1e-12, atol=0.0)
     assert abs(g.grad.item() - 2.0 * gg) <= 1e-12 * abs(gg)
     adj.close()
+
+
+@pytest.mark.parametrize("name,steps", [("sodxy10x10", 75), ("sodbig200", 300)])
+def test_dot_product_on_the_reference_sod_decks(name, steps):
+    """The dot-product test on the reference's own Sod decks
+    (InputDecks/clover_sodxy.in to its end at t = 3, 75 steps;
+    clover_sodbig.in, 200^2, over 300 steps), from the decks' own initial
+    state: the reverse sweep's gradient against the tangent-linear run, to
+    1e-10 relative, through the shocks and their reflections."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from cloverleaf_b200 import deck as D
+    from golden_util import deck_text
+    dk = D.parse_deck(deck_text(name))
+    dk.end_step = steps
+    adj = Adjoint(dk)
+    ke = adj.forward(steps)
+    gr, ge, gg = adj.gradient()
+    rng = np.random.default_rng(11)
+    dr, de, dg = rng.standard_normal(gr.shape), rng.standard_normal(ge.shape), float(rng.standard_normal())
+    _, dke = adj.tangent(dr, de, dg)
+    lhs = float((gr * dr).sum() + (ge * de).sum() + gg * dg)
+    scale = float(np.abs(gr * dr).sum() + np.abs(ge * de).sum() + abs(gg * dg))
+    assert scale > 0.0 and ke > 0.0
+    assert abs(lhs - dke) <= 1e-10 * scale, (name, lhs, dke, scale)
+    adj.close()
