@@ -6,7 +6,7 @@ dt and the summary's sums reduced over the ranks), driven by HydroRun's call
 sequence.  Checked, rank by rank, against the same decomposed run on oracle
 chunks (tests/decomp_util.py): every captured field of every chunk, the step
 count and the dt of every step bit-identical in FP64; the final summary's
-sums within 1e-13.
+sums within 1e-13 of the oracle chunks' exactly rounded sums.
 
 Decks: the benchmark deck (64 x 48) and a deck whose flow crosses the
 chunk edges both ways (a moving circle, gamma 1.55; 56 x 40), so that
@@ -80,6 +80,22 @@ def test_decomposed_run_with_folds_and_call_fusion(mode):
     with mp.Manager() as mgr:
         out = mgr.dict()
         mp.spawn(rank_body, args=(4, port, out, "circle", True, mode), nprocs=4, join=True)
+        res = dict(out)
+    _check(res, 4)
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("deck_name", ["sodxy10x10", "sodbig200"])
+def test_decomposed_run_of_the_reference_sod_decks(deck_name):
+    """The reference's own Sod decks decomposed over four ranks (2 x 2:
+    chunks of 5 x 5 cells, below the size at which the library folds halos,
+    and of 100 x 100 over 200 steps): the GPU run is the decomposed oracle
+    run, bit for bit."""
+    from decomp_util import rank_body
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(rank_body, args=(4, port, out, deck_name, True), nprocs=4, join=True)
         res = dict(out)
     _check(res, 4)
 
